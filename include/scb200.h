@@ -1,0 +1,164 @@
+/* scb200.h -- C ABI of the B200 SuperConga self-consistency engine.
+ *
+ * One handle is one self-consistency context: the grain, the Fermi surface,
+ * the Ozaki energies and all iteration state live on one GPU.  Host buffers use
+ * the reference's planar layout (GridData.h:276-291): every field is an N0 x N0
+ * row-major plane (index y*N0 + x); a complex field is its real plane followed
+ * by its imaginary plane; order-parameter components are ordered as the
+ * reference driver adds them (dx2-y2, dxy, g, s; src/simulation.cu:213-290).
+ * The induced vector potential is in the reference's internal units, i.e.
+ * multiplied by lambda^2 (src/simulation.cu:368-373).
+ *
+ * Every function returns 0 on success and a negative status on error; the
+ * message is available from sc_last_error().  Nothing here exits or throws.
+ * A handle is not thread-safe; all its work is issued on one CUDA stream.
+ */
+#ifndef SCB200_H_
+#define SCB200_H_
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct sc_ctx sc_ctx;
+
+#define SC_OK 0
+#define SC_ERR_ARG -1     /* invalid argument or configuration */
+#define SC_ERR_CUDA -2    /* CUDA runtime error (allocation, launch) */
+#define SC_ERR_STATE -3   /* call not valid in the current state */
+
+#define SC_MODE_FP64 0    /* complex FP64 end to end */
+#define SC_MODE_MIXED 1   /* FP32 Riccati stepping, FP64 accumulation */
+
+/* Creates a context from a reference JSON configuration (the file
+ * simulation_f64 reads; src/simulation.cu:64-463 builds the same objects).
+ * Replaces: the Context, Parameters, GeometryGroup, IntegrationIteratorOzaki,
+ * OrderParameter, compute-object and RiccatiSolverConfined set-up of
+ * src/simulation.cu:95-463 and Context::initialize (include/conga/Context.h:285-375).
+ * The order parameter starts at zero; set it with sc_set_state. */
+int sc_create(const char *config_json, int mode, sc_ctx **out);
+
+/* Frees the context and all its device memory. */
+int sc_destroy(sc_ctx *ctx);
+
+/* Last error message of ctx (or of the last failed sc_create if ctx is NULL). */
+const char *sc_last_error(const sc_ctx *ctx);
+
+/* Lattice sizes: N0 (reference grid), N1 (trajectory frame), Fermi angles,
+ * Ozaki energies, order-parameter components
+ * (Parameters.h:48-50, IntegrationIteratorOzaki.h:207-210). */
+int sc_get_dims(const sc_ctx *ctx, int *n0, int *n1, int *n_angles, int *n_energies,
+                int *n_comp);
+
+/* In-grain Riccati site-updates per iteration: 2 * Ne * sum_angles #{label > 0}. */
+int sc_site_updates(const sc_ctx *ctx, long long *per_iteration);
+
+/* Sets x = (order parameter [Nc][2][N0][N0], vector potential [2][N0][N0]),
+ * host buffers.  a may be NULL (zero).  The order parameter is zeroed outside
+ * the grain as OrderParameter::initialize does (OrderParameter.h:180-199).
+ * Replaces the load_path injection of src/simulation.cu:300-377. */
+int sc_set_state(sc_ctx *ctx, const double *delta, const double *a_internal);
+
+/* Reads x back (host buffers, same layout). */
+int sc_get_state(sc_ctx *ctx, double *delta, double *a_internal);
+
+/* Runs n self-consistency iterations (Context::compute, Context.h:391-447):
+ * accelerator step (from the second iteration on), Riccati sweep and Green
+ * accumulation for all angles, boundary condition, vector potential.  On
+ * return *residual holds Context::getResidual and *converged
+ * Context::isPartiallyConverged of the last iteration.  Either may be NULL. */
+int sc_compute(sc_ctx *ctx, int n, double *residual, int *converged);
+
+/* Runs n burn-in iterations (Context::burnIn, Context.h:377-389): boundary
+ * coherence functions only.  *residual is the boundary residual. */
+int sc_burn_in(sc_ctx *ctx, int n, double *residual, int *converged);
+
+/* g(x) of the last iteration: new order parameter [Nc][2][N0][N0], current
+ * density [2][N0][N0] (ComputeCurrent::getResult), new vector potential
+ * [2][N0][N0] (internal units).  Any pointer may be NULL. */
+int sc_get_results(sc_ctx *ctx, double *delta_new, double *j, double *a_new);
+
+/* out[0..10]: free energy, free energy per area, magnetic free energy,
+ * magnetic free energy per area, residuals of order parameter, current, free
+ * energy, vector potential and boundary, total residual, grain lattice sites
+ * (ComputeFreeEnergy.h:281-414, Context.h:462-483). */
+int sc_get_scalars(sc_ctx *ctx, double *out);
+
+/* Sets the CUDA stream (cudaStream_t) all work of ctx is issued on. */
+int sc_set_stream(sc_ctx *ctx, void *stream);
+
+/* Device-pointer variants of sc_set_state / sc_get_state for callers whose
+ * data already lives on the context's GPU (same layouts, FP64). */
+int sc_set_state_device(sc_ctx *ctx, const double *d_delta, const double *d_a_internal);
+int sc_get_state_device(sc_ctx *ctx, double *d_delta, double *d_a_internal);
+
+/* ---- probes used by the parity tests ------------------------------------ */
+
+/* Frame geometry of one angle: labels [N1*N1] (0 out, 1 in, 2 entry, 3 exit)
+ * and the trajectory box {x0, x1, y0, y1}
+ * (GeometryGroup::create(-theta), BoundaryStorage.h:265-350). */
+int sc_get_frame_labels(const sc_ctx *ctx, int angle, signed char *labels, int *box);
+
+/* Reference-frame domain [N0*N0] (GeometryGroup::createDomain). */
+int sc_get_domain(const sc_ctx *ctx, signed char *domain);
+
+/* Sizes of the sparse boundary storage: in/out for gamma, in/out for
+ * gammaTilde (BoundaryStorage.h:440-490). */
+int sc_boundary_sizes(const sc_ctx *ctx, int *sizes);
+
+/* Boundary coherence values, interleaved (re, im), count*Ne complex values.
+ * which: 0 in-gamma, 1 out-gamma, 2 in-gammaTilde, 3 out-gammaTilde. */
+int sc_get_boundary(sc_ctx *ctx, int which, double *values);
+int sc_set_boundary(sc_ctx *ctx, int which, const double *values);
+
+/* Sets the boundary initial condition (homogeneous solutions at the exit
+ * nodes followed by the boundary condition),
+ * IntegrationIteratorOzaki::setBoundaryInitialCondition
+ * (IntegrationIteratorOzaki.h:244-300). */
+int sc_boundary_initial(sc_ctx *ctx);
+
+/* Frame Green sums of one angle for the current state and boundary values
+ * (before the boundary extension): F = sum_n r_n (f + f~*) [2][N1][N1],
+ * Re G [N1][N1], Re I [N1][N1] (GreensFunctionStatic.h:125-157,
+ * ComputeFreeEnergy.h:106-160).  Updates the out-going boundary values of that
+ * angle as the sweep does. */
+int sc_angle_greens(sc_ctx *ctx, int angle, double *f, double *g_re, double *i_re);
+
+/* Vector potential of a current density [2][N0][N0] through the separable
+ * Poisson filters (ComputeVectorPotential::solve, ComputeVectorPotential.h:727-745),
+ * internal units. */
+int sc_poisson(sc_ctx *ctx, const double *j, double *a_out);
+
+/* Number of this library's kernel launches issued by ctx so far. */
+int sc_launch_count(const sc_ctx *ctx, long long *count);
+
+/* ---- host-only setup probes (no GPU needed) ------------------------------ */
+
+/* The static tables of a configuration, built without touching CUDA: lattice
+ * sizes, Ozaki energies, frame labels, boundary-storage sizes and Poisson
+ * filters (the set-up part of Context::initialize, Context.h:285-375). */
+typedef struct sc_setup sc_setup;
+int sc_setup_create(const char *config_json, sc_setup **out);
+const char *sc_setup_last_error(void);
+int sc_setup_destroy(sc_setup *s);
+int sc_setup_dims(const sc_setup *s, int *n0, int *n1, int *n_angles, int *n_energies,
+                  int *n_comp);
+/* Imaginary parts of the Ozaki energies and their residues
+ * (IntegrationIteratorOzaki.h:108-200). */
+int sc_setup_energies(const sc_setup *s, double *e_im, double *residues);
+int sc_setup_frame(const sc_setup *s, int angle, signed char *labels, int *box);
+int sc_setup_domain(const sc_setup *s, signed char *domain);
+int sc_setup_boundary_sizes(const sc_setup *s, int *sizes);
+/* Separable Poisson filters [n][2*N0-1], their signs and the common scale
+ * (ComputeVectorPotential.h:212-416).  Call with NULL arrays to get n first. */
+int sc_setup_filters(const sc_setup *s, int *n_filters, double *filters, int *positive,
+                     double *scale);
+int sc_setup_site_updates(const sc_setup *s, long long *per_iteration);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SCB200_H_ */

@@ -1,0 +1,11 @@
+"""superconga_b200 -- Blackwell-native SuperConga self-consistency hot path.
+
+The engine (libscb200.so, C ABI in include/scb200.h) runs the Riccati sweep,
+Green accumulation, specular boundary condition, vector-potential Poisson
+solve and accelerators as CUDA kernels for sm_100a.  ``Context`` is the Python
+face of one engine handle.
+"""
+from .engine import Context, Dims, Setup  # noqa: F401
+from ._lib import EngineError, LIB_PATH, load  # noqa: F401
+
+__all__ = ["Context", "Dims", "Setup", "EngineError", "LIB_PATH", "load"]

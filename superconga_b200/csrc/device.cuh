@@ -1,0 +1,138 @@
+// Device-side building blocks of the B200 self-consistency path: complex
+// arithmetic, the midpoint Riccati step, the local Green functions and the
+// bilinear lookups into the reference grid.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace scb {
+
+constexpr int MAX_COMP = 4;
+
+template <typename R>
+struct Cx {
+  R re, im;
+};
+
+// Per-angle constants of one trajectory frame.
+struct AngleParams {
+  double cD, sD;  // order parameter into the frame (float trig, promoted)
+  double cA, sA;  // induced vector potential into the frame
+  double cB, sB;  // frame back to the reference grid
+  double cE, sE;  // external vector potential coordinates (double trig)
+  double vx, vy;  // Fermi velocity
+  double w;       // Fermi-surface integrand factor
+  double sx, sy;  // vx * w, vy * w
+  double eta[MAX_COMP];  // basis function of every component at this angle
+};
+
+template <typename R>
+__device__ __forceinline__ Cx<R> cmul(Cx<R> a, Cx<R> b) {
+  return Cx<R>{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+
+// Principal square root, branch cut on the negative real axis.
+template <typename R>
+__device__ __forceinline__ Cx<R> csqrt_dev(R x, R y) {
+  const R m = sqrt(x * x + y * y);
+  if (x >= R(0)) {
+    const R t = sqrt(R(0.5) * (m + x));
+    if (t == R(0)) return Cx<R>{R(0), y};
+    return Cx<R>{t, y / (R(2) * t)};
+  }
+  const R t = sqrt(R(0.5) * (m - x));
+  return Cx<R>{fabs(y) / (R(2) * t), copysign(t, y)};
+}
+
+// Midpoint Riccati step, riccati::computeStep (RiccatiSolutions.h:65-94):
+//   a = i h/4 conj(D), b = 2 a g0 + i h e - 1, c = (a g0 + i h e + 1) g0 + i h D,
+//   g1 = 2 c / (-b + sqrt(b^2 - 4 a c)).
+// The products with the purely imaginary step are written out (they are exact).
+template <typename R>
+__device__ __forceinline__ Cx<R> riccati_step(R dre, R dim, R ere, R eim, Cx<R> g, R h) {
+  const R q = R(0.25) * h;
+  const Cx<R> a{q * dim, q * dre};
+  const R ser = -h * eim, sei = h * ere;  // (i h) * e
+  const Cx<R> ag = cmul(a, g);
+  const Cx<R> b{R(2) * ag.re + ser - R(1), R(2) * ag.im + sei};
+  const Cx<R> t{ag.re + ser + R(1), ag.im + sei};
+  const Cx<R> tg = cmul(t, g);
+  const Cx<R> c{tg.re - h * dim, tg.im + h * dre};
+  const Cx<R> bb = cmul(b, b);
+  const Cx<R> ac = cmul(a, c);
+  const Cx<R> disc = csqrt_dev<R>(bb.re - R(4) * ac.re, bb.im - R(4) * ac.im);
+  const R den_re = disc.re - b.re, den_im = disc.im - b.im;
+  const R inv = R(1) / (den_re * den_re + den_im * den_im);
+  const R c2r = R(2) * c.re, c2i = R(2) * c.im;
+  return Cx<R>{(c2r * den_re + c2i * den_im) * inv, (c2i * den_re - c2r * den_im) * inv};
+}
+
+// Homogeneous solutions, riccati::computeHomogeneous (RiccatiSolutions.h:36-54).
+template <typename R>
+__device__ __forceinline__ void riccati_homogeneous(R dre, R dim, R ere, R eim, Cx<R> &g,
+                                                    Cx<R> &gt) {
+  const R nd = dre * dre + dim * dim;
+  const R e2re = ere * ere - eim * eim, e2im = ere * eim + eim * ere;
+  const Cx<R> om = csqrt_dev<R>(nd - e2re, -e2im);
+  const R dr = ere - om.im, di = eim + om.re;  // energy + i * Omega
+  const R inv = R(1) / (dr * dr + di * di);
+  const Cx<R> invd{dr * inv, -di * inv};
+  g = cmul(Cx<R>{-dre, -dim}, invd);
+  gt = cmul(Cx<R>{dre, -dim}, invd);
+}
+
+// Local Green functions of one energy (LocalGreens.h:32-70) and the free-energy
+// kernel (ComputeFreeEnergy.h:95-103): returns f + f~* in F, Re g and Im I.
+template <typename R>
+__device__ __forceinline__ void local_greens(Cx<R> g, Cx<R> gt, R dre, R dim, Cx<R> &F,
+                                             R &g_re, R &i_im) {
+  const Cx<R> p = cmul(g, gt);
+  const R den_re = R(1) + p.re, den_im = p.im;
+  const R inv = R(1) / (den_re * den_re + den_im * den_im);
+  // (1 - p) / (1 + p)
+  const R nr = R(1) - p.re, ni = -p.im;
+  const R q_im = (ni * den_re - nr * den_im) * inv;
+  g_re = q_im;  // g = -i (1 - p) / (1 + p)
+  // 2 / (1 + p) and factor = i * 2 / (1 + p)
+  const R t2r = R(2) * den_re * inv, t2i = -R(2) * den_im * inv;
+  const Cx<R> fac{-t2i, t2r};
+  const Cx<R> fg = cmul(fac, g);
+  const Cx<R> fgt = cmul(fac, gt);
+  F = Cx<R>{-fg.re + fgt.re, -fg.im - fgt.im};
+  // I = conj(D) g - D g~
+  i_im = (dre * g.im - dim * g.re) - (dre * gt.im + dim * gt.re);
+}
+
+// Bilinear lookup of insertRotatedGrid(_Additive)_kernel
+// (GridFunctions_GPU.h:436-546): coordinates of site (x, y) of an n_out grid in
+// an n_in grid rotated by the angle whose (cos, sin) of minus the angle are
+// (c, s).  Returns false when the reference leaves the site untouched.
+struct Bilinear {
+  int i00;  // index of the lower-left corner in the input grid
+  double xf, yf;
+};
+__device__ __forceinline__ bool rotated_lookup(int x, int y, int n_out, int n_in, double c,
+                                               double s, Bilinear &b) {
+  const double xt = (double)(n_in - n_out) / 2.0;
+  const double sh = (double)(n_in - 1) / 2.0;
+  const double X = (double)x + xt - sh, Y = (double)y + xt - sh;
+  const double xr = X * c - Y * s + sh;
+  const double yr = X * s + Y * c + sh;
+  const int xi = (int)xr, yi = (int)yr;
+  if (xi >= 0 && xi + 1 < n_in && yi >= 0 && yi + 1 < n_in) {
+    b.i00 = yi * n_in + xi;
+    b.xf = xr - (double)xi;
+    b.yf = yr - (double)yi;
+    return true;
+  }
+  return false;
+}
+__device__ __forceinline__ double bilerp(double v00, double v01, double v10, double v11,
+                                         double xf, double yf) {
+  const double x1 = (1.0 - xf) * v00 + xf * v01;
+  const double x2 = (1.0 - xf) * v10 + xf * v11;
+  return (1.0 - yf) * x1 + yf * x2;
+}
+
+}  // namespace scb

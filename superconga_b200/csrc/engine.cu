@@ -1,0 +1,1831 @@
+// B200 engine of the SuperConga self-consistency hot path, behind the C ABI of
+// include/scb200.h.
+//
+// One iteration (Context::compute, include/conga/Context.h:391-447) is a short
+// sequence of launches on the context's stream:
+//   accelerate        x <- F(x, g(x))                      (iterations >= 2)
+//   extend_reference  order parameter extended past the grain (domain_ops.h)
+//   per angle chunk:
+//     sweep           gammaTilde down every trajectory column (stored), gamma up,
+//                     Green sums over the Ozaki energies -> frame buffers;
+//                     outgoing boundary values written in sparse order
+//     halo            frame extension next to the boundary (domain_ops.h:11-69)
+//     rotate_back     frame -> reference grid, accumulated angle by angle
+//   finalize          Delta, j, free energy, residuals (ComputeOrderParameter.h,
+//                     ComputeCurrent.h, ComputeFreeEnergy.h)
+//   boundary          specular reflection through precomputed gather tables
+//   poisson           separable Toeplitz filters (ComputeVectorPotential.h)
+// All static data (geometry in every frame, sparse indices, gather tables) is
+// built once by setup.cpp and stays resident in HBM.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/scb200.h"
+#include "device.cuh"
+#include "setup.hpp"
+
+using namespace scb;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+#define CUDA_TRY(expr)                                                          \
+  do {                                                                          \
+    cudaError_t _e = (expr);                                                    \
+    if (_e != cudaSuccess)                                                      \
+      throw EngineError(SC_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(_e)); \
+  } while (0)
+
+struct EngineError {
+  int code;
+  std::string msg;
+  EngineError(int c, std::string m) : code(c), msg(std::move(m)) {}
+};
+
+constexpr int REDUCE_THREADS = 256;
+constexpr int NQ = 48;  // partial-sum slots of the finalize reduction
+
+// ------------------------------------------------------------------ kernels --
+
+// Reference-grid extension of the order parameter (domain_ops.h:11-69):
+// out = in everywhere, except label-0 sites next to the grain, which get the
+// mean of their nearest grain sites.
+__global__ void k_extend_reference(int n_fields, int nn, int n_sites, const int *__restrict__ site,
+                                   const int *__restrict__ off, const int *__restrict__ src,
+                                   const double *__restrict__ in, double *__restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int f = blockIdx.y;
+  if (k >= n_sites || f >= n_fields) return;
+  const double *v = in + (size_t)f * nn;
+  const int b = off[k], e = off[k + 1];
+  double acc = v[src[b]];
+  for (int i = b + 1; i < e; ++i) acc = __dadd_rn(acc, v[src[i]]);
+  out[(size_t)f * nn + site[k]] = __ddiv_rn(acc, (double)(e - b));
+}
+
+template <typename R>
+struct SweepArgs {
+  int n0, n1, ne, nc, groups, log_groups, ept, n_items;
+  int burn_in, has_vp, has_ext, gauge;
+  int slot_base;
+  double h, lam_scale, flux_b, q, area;
+  const int4 *items;  // (angle, x, first row, last row)
+  const AngleParams *ang;
+  const uint8_t *labels;
+  const int *idx_in_g, *idx_out_g, *idx_in_gt, *idx_out_gt;
+  const double *dist_in_g, *dist_out_g, *dist_in_gt, *dist_out_gt;
+  const Cx<R> *bin_g, *bin_gt;
+  Cx<R> *bout_g, *bout_gt;
+  const double *dext;  // [c][2][n0*n0]
+  const double *avec;  // [2][n0*n0]
+  const double *e_im, *res;
+  Cx<R> *scratch;   // [row][energy][item]
+  double *scratch2; // [row][3][item]: Re D, Im D, energy shift
+  double2 *fg, *gi; // frame buffers [slot][n1*n1]: (Re F, Im F), (Re G, Re I)
+};
+
+// Gauges, include/conga/riccati/energy_shift/Gauges.h:25-62.
+__device__ __forceinline__ void gauge_potential(int gauge, double b, double area, double x,
+                                                double y, double &ax, double &ay) {
+  if (gauge == GAUGE_LANDAU) {
+    ax = 0.0;
+    ay = x * b;
+  } else if (gauge == GAUGE_SYMMETRIC) {
+    const double f = 0.5 * b;
+    ax = -y * f;
+    ay = x * f;
+  } else {
+    const double r2 = fmax(x * x + y * y, 1e-7);
+    const double f = b * area / (2.0 * M_PI * r2);
+    ax = -y * f;
+    ay = x * f;
+  }
+}
+
+// Order parameter (OrderParameter::getRotatedGrid) and Doppler shift
+// (computeEnergyShift, RiccatiSolver.h:127-176) at frame site (x, y).
+template <typename R>
+__device__ __forceinline__ void frame_fields(const SweepArgs<R> &A, const AngleParams &P, int x,
+                                             int y, double &dre, double &dim, double &es) {
+  const int n0 = A.n0;
+  const size_t nn0 = (size_t)n0 * n0;
+  Bilinear b;
+  dre = 0.0;
+  dim = 0.0;
+  if (rotated_lookup(x, y, A.n1, n0, P.cD, P.sD, b)) {
+    double c_re[4] = {0, 0, 0, 0}, c_im[4] = {0, 0, 0, 0};
+    const int off[4] = {b.i00, b.i00 + 1, b.i00 + n0, b.i00 + n0 + 1};
+    for (int c = 0; c < A.nc; ++c) {
+      const double *pr = A.dext + (size_t)(2 * c) * nn0;
+      const double *pi = pr + nn0;
+      const double et = P.eta[c];
+      for (int k = 0; k < 4; ++k) {
+        c_re[k] += __ldg(pr + off[k]) * et;
+        c_im[k] += __ldg(pi + off[k]) * et;
+      }
+    }
+    dre = bilerp(c_re[0], c_re[1], c_re[2], c_re[3], b.xf, b.yf);
+    dim = bilerp(c_im[0], c_im[1], c_im[2], c_im[3], b.xf, b.yf);
+  }
+  es = 0.0;
+  if (A.has_vp || A.has_ext) {
+    double ax = 0.0, ay = 0.0;
+    const double off = -0.5 * (double)(A.n1 - 1);
+    const double xp = ((double)x + off) * A.h, yp = ((double)y + off) * A.h;
+    const double xr = xp * P.cE - yp * P.sE, yr = xp * P.sE + yp * P.cE;
+    gauge_potential(A.gauge, A.flux_b, A.area, xr, yr, ax, ay);
+    if (A.has_vp) {
+      double rx = 0.0, ry = 0.0;
+      Bilinear ba;
+      if (rotated_lookup(x, y, A.n1, n0, P.cA, P.sA, ba)) {
+        const double *px = A.avec, *py = A.avec + nn0;
+        rx = bilerp(__ldg(px + ba.i00), __ldg(px + ba.i00 + 1), __ldg(px + ba.i00 + n0),
+                    __ldg(px + ba.i00 + n0 + 1), ba.xf, ba.yf);
+        ry = bilerp(__ldg(py + ba.i00), __ldg(py + ba.i00 + 1), __ldg(py + ba.i00 + n0),
+                    __ldg(py + ba.i00 + n0 + 1), ba.xf, ba.yf);
+      }
+      rx *= A.lam_scale;
+      ry *= A.lam_scale;
+      es = A.q * (P.vx * (rx + ax) + P.vy * (ry + ay));
+    } else {
+      es = A.q * (P.vx * ax + P.vy * ay);
+    }
+  }
+}
+
+template <typename R, int EMAX>
+__device__ __forceinline__ void group_sum(double &v, int groups, unsigned mask) {
+  for (int o = groups >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
+}
+
+// The fused Riccati sweep of one chunk of angles.  G = 2^log_groups threads
+// share one trajectory column (angle, x); thread g integrates Ozaki energies
+// [g*ept, g*ept + ept).  gammaTilde runs down the column first and is kept in
+// scratch; gamma then runs up and the Green sums over all energies are formed
+// site by site (RiccatiSolverConfined.h:129-312, GreensFunctionStatic.h:92-157,
+// ComputeFreeEnergy.h:106-160).  Energies and the frame order parameter are
+// computed in FP64; the coherence functions in R.
+template <typename R, int EMAX>
+__global__ void __launch_bounds__(128) k_sweep(const SweepArgs<R> A) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int item = tid >> A.log_groups;
+  const int g = tid & (A.groups - 1);
+  const int lane = threadIdx.x & 31;
+  const unsigned gmask = ((A.groups == 32) ? 0xffffffffu : ((1u << A.groups) - 1u))
+                         << (lane & ~(A.groups - 1));
+  if (item >= A.n_items) return;  // whole groups leave together (groups divide the warp)
+  const int4 it = A.items[item];
+  const int a = it.x, x = it.y, lo = it.z, hi = it.w;
+  const AngleParams P = A.ang[a];
+  const int n1 = A.n1, ne = A.ne;
+  const size_t nn1 = (size_t)n1 * n1;
+  const uint8_t *lab = A.labels + (size_t)a * nn1;
+  const size_t ni = (size_t)A.n_items;
+  const R h = (R)A.h;
+  const int e0 = g * A.ept;
+  int ecount = ne - e0;
+  if (ecount > A.ept) ecount = A.ept;
+  if (ecount < 0) ecount = 0;
+
+  R eim[EMAX];
+#pragma unroll
+  for (int j = 0; j < EMAX; ++j) eim[j] = (j < ecount) ? (R)A.e_im[e0 + j] : R(1);
+
+  Cx<R> coh[EMAX];
+  // ------------------------------------------------------ gammaTilde, down --
+  {
+    const int ain = (size_t)a * n1 + x;
+    const int in_base = A.idx_in_gt[ain], out_base = A.idx_out_gt[ain];
+    int nin = 0, nout = 0;
+    R pdre = 0, pdim = 0, pes = 0;
+#pragma unroll
+    for (int j = 0; j < EMAX; ++j) coh[j] = Cx<R>{R(0), R(0)};
+    for (int y = hi; y >= lo; --y) {
+      const int r = y - lo;
+      const uint8_t l = lab[(size_t)y * n1 + x];
+      double ddre, ddim, des;
+      frame_fields(A, P, x, y, ddre, ddim, des);
+      if (!A.burn_in) {  // every lane of the group writes the same values
+        double *s2 = A.scratch2 + (size_t)r * 3 * ni + item;
+        s2[0] = ddre;
+        s2[ni] = ddim;
+        s2[2 * ni] = des;
+      }
+      // gammaTilde uses -conj(Delta) (RiccatiSolverConfined.h:74-79).
+      const R dre = (R)(-ddre), dim = (R)ddim, es = (R)des;
+      if (l == 1) {
+        const R mre = (dre + pdre) * R(0.5), mim = (dim + pdim) * R(0.5), mes = (es + pes) * R(0.5);
+#pragma unroll
+        for (int j = 0; j < EMAX; ++j)
+          if (j < A.ept) coh[j] = riccati_step<R>(mre, mim, mes, eim[j], coh[j], h);
+      } else if (l == 3) {  // entry of gammaTilde
+        const R st = (R)A.dist_in_gt[in_base + nin] * h;
+        const Cx<R> *bin = A.bin_gt + (size_t)(in_base + nin) * ne + e0;
+#pragma unroll
+        for (int j = 0; j < EMAX; ++j)
+          if (j < A.ept) coh[j] = riccati_step<R>(dre, dim, es, eim[j], j < ecount ? bin[j] : Cx<R>{R(0), R(0)}, st);
+        nin++;
+      } else if (l == 2) {  // exit of gammaTilde
+        const R mre = (dre + pdre) * R(0.5), mim = (dim + pdim) * R(0.5), mes = (es + pes) * R(0.5);
+        const R st = (R)A.dist_out_gt[out_base + nout] * h;
+        Cx<R> *bout = A.bout_gt + (size_t)(out_base + nout) * ne + e0;
+#pragma unroll
+        for (int j = 0; j < EMAX; ++j)
+          if (j < A.ept) {
+            coh[j] = riccati_step<R>(mre, mim, mes, eim[j], coh[j], h);
+            const Cx<R> bv = riccati_step<R>(dre, dim, es, eim[j], coh[j], st);
+            if (j < ecount) bout[j] = bv;
+          }
+        nout++;
+      } else {
+#pragma unroll
+        for (int j = 0; j < EMAX; ++j) coh[j] = Cx<R>{R(0), R(0)};
+      }
+      if (!A.burn_in) {
+        Cx<R> *sc = A.scratch + (size_t)r * ne * ni + (size_t)e0 * ni + item;
+#pragma unroll
+        for (int j = 0; j < EMAX; ++j)
+          if (j < ecount) sc[(size_t)j * ni] = coh[j];
+      }
+      pdre = dre;
+      pdim = dim;
+      pes = es;
+    }
+  }
+  // ----------------------------------------------------------- gamma, up --
+  {
+    const int ain = (size_t)a * n1 + x;
+    const int in_base = A.idx_in_g[ain], out_base = A.idx_out_g[ain];
+    int nin = 0, nout = 0;
+    R pdre = 0, pdim = 0, pes = 0;
+#pragma unroll
+    for (int j = 0; j < EMAX; ++j) coh[j] = Cx<R>{R(0), R(0)};
+    double2 *fg = A.fg + (size_t)(a - A.slot_base) * nn1;
+    double2 *gi = A.gi + (size_t)(a - A.slot_base) * nn1;
+    for (int y = lo; y <= hi; ++y) {
+      const int r = y - lo;
+      const uint8_t l = lab[(size_t)y * n1 + x];
+      double ddre, ddim, des;
+      if (A.burn_in) {
+        frame_fields(A, P, x, y, ddre, ddim, des);
+      } else {
+        const double *s2 = A.scratch2 + (size_t)r * 3 * ni + item;
+        ddre = s2[0];
+        ddim = s2[ni];
+        des = s2[2 * ni];
+      }
+      const R dre = (R)ddre, dim = (R)ddim, es = (R)des;
+      if (l == 1) {
+        const R mre = (dre + pdre) * R(0.5), mim = (dim + pdim) * R(0.5), mes = (es + pes) * R(0.5);
+#pragma unroll
+        for (int j = 0; j < EMAX; ++j)
+          if (j < A.ept) coh[j] = riccati_step<R>(mre, mim, mes, eim[j], coh[j], h);
+      } else if (l == 2) {  // entry of gamma
+        const R st = (R)A.dist_in_g[in_base + nin] * h;
+        const Cx<R> *bin = A.bin_g + (size_t)(in_base + nin) * ne + e0;
+#pragma unroll
+        for (int j = 0; j < EMAX; ++j)
+          if (j < A.ept) coh[j] = riccati_step<R>(dre, dim, es, eim[j], j < ecount ? bin[j] : Cx<R>{R(0), R(0)}, st);
+        nin++;
+      } else if (l == 3) {  // exit of gamma
+        const R mre = (dre + pdre) * R(0.5), mim = (dim + pdim) * R(0.5), mes = (es + pes) * R(0.5);
+        const R st = (R)A.dist_out_g[out_base + nout] * h;
+        Cx<R> *bout = A.bout_g + (size_t)(out_base + nout) * ne + e0;
+#pragma unroll
+        for (int j = 0; j < EMAX; ++j)
+          if (j < A.ept) {
+            coh[j] = riccati_step<R>(mre, mim, mes, eim[j], coh[j], h);
+            const Cx<R> bv = riccati_step<R>(dre, dim, es, eim[j], coh[j], st);
+            if (j < ecount) bout[j] = bv;
+          }
+        nout++;
+      } else {
+#pragma unroll
+        for (int j = 0; j < EMAX; ++j) coh[j] = Cx<R>{R(0), R(0)};
+      }
+      pdre = dre;
+      pdim = dim;
+      pes = es;
+      if (A.burn_in) continue;
+      double sfr = 0.0, sfi = 0.0, sg = 0.0, si = 0.0;
+      if (l != 0) {
+        const Cx<R> *sc = A.scratch + (size_t)r * ne * ni + (size_t)e0 * ni + item;
+#pragma unroll
+        for (int j = 0; j < EMAX; ++j)
+          if (j < ecount) {
+            const Cx<R> gt = sc[(size_t)j * ni];
+            Cx<R> F;
+            R gre, iim;
+            local_greens<R>(coh[j], gt, dre, dim, F, gre, iim);
+            const double rr = A.res[e0 + j];
+            sfr += rr * (double)F.re;
+            sfi += rr * (double)F.im;
+            sg += rr * (double)gre;
+            si += rr * (double)iim;
+          }
+      }
+      if (A.groups > 1) {
+        group_sum<R, EMAX>(sfr, A.groups, gmask);
+        group_sum<R, EMAX>(sfi, A.groups, gmask);
+        group_sum<R, EMAX>(sg, A.groups, gmask);
+        group_sum<R, EMAX>(si, A.groups, gmask);
+      }
+      if (g == 0) {
+        const size_t fi = (size_t)y * n1 + x;
+        fg[fi] = make_double2(sfr, sfi);
+        gi[fi] = make_double2(sg, -si);
+      }
+    }
+  }
+}
+
+// Frame extension next to the boundary for the angles of one chunk
+// (ComputeOrderParameter.h:180-181, ComputeCurrent.h:149-150,
+// ComputeFreeEnergy.h:265-266, all through domain_ops.h:11-69).
+__global__ void k_halo(int n_entries, int entry0, int n1, const int *__restrict__ entry_angle,
+                       int slot_base, const int *__restrict__ site, const int *__restrict__ off,
+                       const int *__restrict__ src, double2 *fg, double2 *gi) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n_entries) return;
+  const int e = entry0 + k;
+  const size_t base = (size_t)(entry_angle[e] - slot_base) * n1 * n1;
+  const int b = off[e], en = off[e + 1];
+  double2 f = fg[base + src[b]], q = gi[base + src[b]];
+  for (int i = b + 1; i < en; ++i) {
+    const double2 f2 = fg[base + src[i]], q2 = gi[base + src[i]];
+    f.x = __dadd_rn(f.x, f2.x);
+    f.y = __dadd_rn(f.y, f2.y);
+    q.x = __dadd_rn(q.x, q2.x);
+    q.y = __dadd_rn(q.y, q2.y);
+  }
+  const double cnt = (double)(en - b);
+  fg[base + site[e]] = make_double2(__ddiv_rn(f.x, cnt), __ddiv_rn(f.y, cnt));
+  gi[base + site[e]] = make_double2(__ddiv_rn(q.x, cnt), __ddiv_rn(q.y, cnt));
+}
+
+// Rotation of the frame Green sums back to the reference grid, accumulated in
+// angle order (ComputeOrderParameter.h:174-210, ComputeCurrent.h:142-173,
+// ComputeFreeEnergy.h:260-279).
+__global__ void __launch_bounds__(256) k_rotate_back(int n0, int n1, int nc, int a_begin,
+                                                     int a_end, const AngleParams *__restrict__ ang,
+                                                     const double2 *__restrict__ fg,
+                                                     const double2 *__restrict__ gi,
+                                                     double *acc_d, double *acc_j, double *acc_fe) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= n0 || y >= n0) return;
+  const size_t nn0 = (size_t)n0 * n0, nn1 = (size_t)n1 * n1;
+  const size_t i = (size_t)y * n0 + x;
+  double dr[MAX_COMP], di[MAX_COMP];
+  for (int c = 0; c < nc; ++c) {
+    dr[c] = acc_d[(size_t)(2 * c) * nn0 + i];
+    di[c] = acc_d[(size_t)(2 * c + 1) * nn0 + i];
+  }
+  double jx = acc_j[i], jy = acc_j[nn0 + i], fe = acc_fe[i];
+  for (int a = a_begin; a < a_end; ++a) {
+    const AngleParams &P = ang[a];
+    Bilinear b;
+    if (!rotated_lookup(x, y, n0, n1, P.cB, P.sB, b)) continue;
+    const size_t base = (size_t)(a - a_begin) * nn1 + b.i00;
+    const double2 f00 = fg[base], f01 = fg[base + 1], f10 = fg[base + n1], f11 = fg[base + n1 + 1];
+    const double2 q00 = gi[base], q01 = gi[base + 1], q10 = gi[base + n1], q11 = gi[base + n1 + 1];
+    const double fre = bilerp(f00.x, f01.x, f10.x, f11.x, b.xf, b.yf);
+    const double fim = bilerp(f00.y, f01.y, f10.y, f11.y, b.xf, b.yf);
+    for (int c = 0; c < nc; ++c) {
+      const double et = P.eta[c];
+      dr[c] += (fre * et) * P.w;
+      di[c] += (fim * et) * P.w;
+    }
+    jx += bilerp(q00.x * P.sx, q01.x * P.sx, q10.x * P.sx, q11.x * P.sx, b.xf, b.yf);
+    jy += bilerp(q00.x * P.sy, q01.x * P.sy, q10.x * P.sy, q11.x * P.sy, b.xf, b.yf);
+    fe += bilerp(q00.y * P.w, q01.y * P.w, q10.y * P.w, q11.y * P.w, b.xf, b.yf);
+  }
+  for (int c = 0; c < nc; ++c) {
+    acc_d[(size_t)(2 * c) * nn0 + i] = dr[c];
+    acc_d[(size_t)(2 * c + 1) * nn0 + i] = di[c];
+  }
+  acc_j[i] = jx;
+  acc_j[nn0 + i] = jy;
+  acc_fe[i] = fe;
+}
+
+// Residual partial sums of one (old, new) pair: sum d^2, sum old^2, sum |d|,
+// sum |old|, max |d|, max |old| (ComputeResidual.h:54-106).
+struct Res6 {
+  double s[6];
+};
+__device__ __forceinline__ void res_add(double *q, double o, double n) {
+  const double d = o - n;
+  q[0] += d * d;
+  q[1] += o * o;
+  q[2] += fabs(d);
+  q[3] += fabs(o);
+  q[4] = fmax(q[4], fabs(d));
+  q[5] = fmax(q[5], fabs(o));
+}
+
+// Block reduction of NQ slots: slots listed in max_mask are max-reduced.
+__device__ void block_reduce(double *q, int nq, unsigned long long max_mask, double *out) {
+  __shared__ double sh[REDUCE_THREADS];
+  for (int k = 0; k < nq; ++k) {
+    sh[threadIdx.x] = q[k];
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+      if ((int)threadIdx.x < s) {
+        const double o = sh[threadIdx.x + s];
+        sh[threadIdx.x] = ((max_mask >> k) & 1ull) ? fmax(sh[threadIdx.x], o) : sh[threadIdx.x] + o;
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) out[k] = sh[0];
+    __syncthreads();
+  }
+}
+
+// Slot layout of the finalize reduction.
+//   [6c .. 6c+5]  order-parameter residual of component c (c < 4)
+//   [24 .. 29]    current-density residual
+//   30            sum of the free-energy kernel inside the grain
+//   31 .. 34      sum |Delta_c|^2 inside the grain
+//   35            sum B^2 over the lattice
+//   36, 37        sum of the new current density (x, y)
+constexpr unsigned long long FIN_MAX_MASK =
+    (0x30ull) | (0x30ull << 6) | (0x30ull << 12) | (0x30ull << 18) | (0x30ull << 24);
+
+// ComputeOrderParameter / ComputeCurrent / ComputeFreeEnergy
+// ::computePropertyFromGreens, element-wise part and partial sums.
+__global__ void __launch_bounds__(REDUCE_THREADS) k_finalize(
+    int n0, int nc, double h, double jfactor, int has_vp, const uint8_t *__restrict__ dom,
+    const double *__restrict__ coupling, const double *__restrict__ acc_d,
+    const double *__restrict__ acc_j, const double *__restrict__ acc_fe,
+    const double *__restrict__ delta, const double *__restrict__ avec, double *delta_new,
+    double *j_real, double *partial) {
+  const size_t nn = (size_t)n0 * n0;
+  double q[NQ];
+  for (int k = 0; k < NQ; ++k) q[k] = 0.0;
+  const double inv_h = 1.0 / h;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nn;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const bool in = dom[i] != 0;
+    for (int c = 0; c < nc; ++c) {
+      const double lc = coupling[c];
+      for (int p = 0; p < 2; ++p) {
+        const size_t k = (size_t)(2 * c + p) * nn + i;
+        const double nv = in ? acc_d[k] * lc : 0.0;
+        delta_new[k] = nv;
+        res_add(&q[6 * c], delta[k], nv);
+      }
+      if (in) {
+        const double o_re = delta[(size_t)(2 * c) * nn + i], o_im = delta[(size_t)(2 * c + 1) * nn + i];
+        q[31 + c] += o_re * o_re + o_im * o_im;
+      }
+    }
+    for (int d = 0; d < 2; ++d) {
+      const size_t k = (size_t)d * nn + i;
+      const double nv = in ? acc_j[k] * jfactor : 0.0;
+      res_add(&q[24], j_real[k], nv);
+      j_real[k] = nv;
+      q[36 + d] += nv;
+    }
+    if (in) q[30] += acc_fe[i];
+    if (has_vp) {
+      // curl_kernel, GridFunctions_GPU.h:326-352.
+      const int x = (int)(i % n0), y = (int)(i / n0);
+      const int xn = min(x + 1, n0 - 1), xp = max(x - 1, 0);
+      const int yn = min(y + 1, n0 - 1), yp = max(y - 1, 0);
+      const double *ax = avec, *ay = avec + nn;
+      const double dAydx = (ay[(size_t)y * n0 + xn] - ay[(size_t)y * n0 + xp]) / (double)(xn - xp);
+      const double dAxdy = (ax[(size_t)yn * n0 + x] - ax[(size_t)yp * n0 + x]) / (double)(yn - yp);
+      const double bz = (dAydx - dAxdy) * inv_h;
+      q[35] += bz * bz;
+    }
+  }
+  block_reduce(q, NQ, FIN_MAX_MASK, partial + (size_t)blockIdx.x * NQ);
+}
+
+// Residual partials of a boundary gather (in-place update) or of any (old, new)
+// pair of arrays.
+__global__ void __launch_bounds__(REDUCE_THREADS) k_residual(size_t n, const double *__restrict__ o,
+                                                             const double *__restrict__ nw,
+                                                             double *partial) {
+  double q[6] = {0, 0, 0, 0, 0, 0};
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    res_add(q, o[i], nw[i]);
+  block_reduce(q, 6, 0x30ull, partial + (size_t)blockIdx.x * 6);
+}
+
+// Specular boundary condition through the precomputed gather table
+// (BoundaryConditionSpecular.h:245-358): in[k] = sum_s w_s out[src_s] / wsum.
+// The old value is read before it is replaced so the residual comes for free.
+template <typename R>
+__global__ void __launch_bounds__(REDUCE_THREADS) k_boundary(int n_in, int ne,
+                                                             const int *__restrict__ src,
+                                                             const double *__restrict__ w,
+                                                             const double *__restrict__ wsum,
+                                                             const Cx<R> *__restrict__ out,
+                                                             Cx<R> *in, double *partial) {
+  double q[6] = {0, 0, 0, 0, 0, 0};
+  const size_t total = (size_t)n_in * ne;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const int k = (int)(t / ne), e = (int)(t % ne);
+    double re = 0.0, im = 0.0;
+    for (int s = 0; s < 4; ++s) {
+      const int sidx = src[4 * k + s];
+      if (sidx < 0) continue;
+      const Cx<R> v = out[(size_t)sidx * ne + e];
+      const double ws = w[4 * k + s];
+      re = __dadd_rn(re, __dmul_rn((double)v.re, ws));
+      im = __dadd_rn(im, __dmul_rn((double)v.im, ws));
+    }
+    const double W = wsum[k];
+    Cx<R> nv{R(0), R(0)};
+    if (W > 0.0) nv = Cx<R>{(R)__ddiv_rn(re, W), (R)__ddiv_rn(im, W)};
+    const Cx<R> ov = in[t];
+    res_add(q, (double)ov.re, (double)nv.re);
+    res_add(q, (double)ov.im, (double)nv.im);
+    in[t] = nv;
+  }
+  block_reduce(q, 6, 0x30ull, partial + (size_t)blockIdx.x * 6);
+}
+
+// Initial boundary values: homogeneous solutions at every exit node
+// (computeGammaFunctionInitialBoundaryTemplate_kernel,
+// RiccatiSolverConfined.h:400-468).
+template <typename R>
+__global__ void k_boundary_initial(int n_out, int ne, int is_g, const int *__restrict__ node_a,
+                                   const int *__restrict__ node_x, const int *__restrict__ node_y,
+                                   SweepArgs<R> A, Cx<R> *bout) {
+  const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (t >= (size_t)n_out * ne) return;
+  const int k = (int)(t / ne), e = (int)(t % ne);
+  const AngleParams P = A.ang[node_a[k]];
+  double dre, dim, es;
+  frame_fields(A, P, node_x[k], node_y[k], dre, dim, es);
+  Cx<R> g, gt;
+  riccati_homogeneous<R>((R)dre, (R)dim, (R)es, (R)A.e_im[e], g, gt);
+  bout[t] = is_g ? g : gt;
+}
+
+// Subtracts the mean of each current component (ComputeVectorPotential.h:575-591).
+__global__ void k_subtract_mean(int n0, const double *__restrict__ j, const double *__restrict__ scal,
+                                int mean_slot, double *s) {
+  const size_t nn = (size_t)n0 * n0;
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= 2 * nn) return;
+  const int d = (int)(i / nn);
+  s[i] = j[i] - scal[mean_slot + d];
+}
+
+// One Toeplitz correlation pass of the separable Poisson solve for every
+// filter (cvp_internal::crossCorrelate1DTranspose, ComputeVectorPotential.h:437-499):
+//   out[k][d][x][y] = sum_i filt_k[i + n - 1 - y] * src[k or 0][d][i][x].
+// Tiled 32 x 32 in (x, y), 32 source rows at a time through shared memory.
+constexpr int PT = 32;
+__global__ void __launch_bounds__(PT * 8) k_toeplitz(int n, int nk, const double *__restrict__ filt,
+                                                     const double *__restrict__ src, size_t src_kstride,
+                                                     double *__restrict__ dst) {
+  __shared__ double s_src[PT][PT + 1];
+  __shared__ double s_f[2 * PT];
+  const int k = blockIdx.z / 2, d = blockIdx.z % 2;
+  const int x0 = blockIdx.x * PT, y0 = blockIdx.y * PT;
+  const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+  const size_t nn = (size_t)n * n;
+  const double *S = src + (size_t)k * src_kstride + (size_t)d * nn;
+  const double *F = filt + (size_t)k * (2 * n - 1);
+  double acc[4] = {0, 0, 0, 0};
+  for (int i0 = 0; i0 < n; i0 += PT) {
+    for (int r = ty; r < PT; r += 8) {
+      const int i = i0 + r, xx = x0 + tx;
+      s_src[r][tx] = (i < n && xx < n) ? S[(size_t)i * n + xx] : 0.0;
+    }
+    // filter window: f[i + n - 1 - y] for i in [i0, i0+32), y in [y0, y0+32)
+    const int t = ty * 32 + tx;
+    if (t < 2 * PT) {
+      const int fi = i0 + n - 1 - y0 - (PT - 1) + t;
+      s_f[t] = (fi >= 0 && fi < 2 * n - 1) ? F[fi] : 0.0;
+    }
+    __syncthreads();
+    for (int r = 0; r < PT; ++r) {
+      const double sv = s_src[r][tx];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int yl = ty + 8 * u;
+        acc[u] += s_f[r - yl + PT - 1] * sv;
+      }
+    }
+    __syncthreads();
+  }
+  const int xx = x0 + tx;
+  if (xx < n) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int yy = y0 + ty + 8 * u;
+      if (yy < n) dst[(size_t)k * 2 * nn + (size_t)n * (d * n + xx) + yy] = acc[u];
+    }
+  }
+}
+
+// A = -h^2 scale * sum_k (+/-) T1_k, accumulated in filter order
+// (ComputeVectorPotential.h:671-724).
+__global__ void k_poisson_sum(int n, int nk, const int *__restrict__ pos, const double *__restrict__ t1,
+                              double factor, double *a) {
+  const size_t nn2 = 2 * (size_t)n * n;
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= nn2) return;
+  double v = 0.0;
+  for (int k = 0; k < nk; ++k) {
+    const double t = t1[(size_t)k * nn2 + i];
+    v = pos[k] ? v + t : v - t;
+  }
+  a[i] = v * factor;
+}
+
+// Scalars of one iteration, reduced from the block partials in a fixed order.
+struct Scalars {
+  double fe, fe_area, fe_mag, fe_mag_area;
+  double res_op, res_j, res_fe, res_vp, res_bc, residual;
+  double n_grain;
+  double j_mean[2];
+  double fe_area_prev;
+  int first_j, first_fe;
+  int conv_op, conv_j, conv_fe;
+};
+
+__device__ double residual_from(const double *t, size_t n_elem, int norm) {
+  double numer, denom, eps = 1e-4;
+  if (norm == NORM_L1) {
+    numer = t[2];
+    denom = t[3];
+    eps *= (double)n_elem;
+  } else if (norm == NORM_L2) {
+    numer = sqrt(t[0]);
+    denom = sqrt(t[1]);
+    eps *= (double)n_elem;
+  } else {
+    numer = fmax(t[4], 2.2250738585072014e-308);
+    denom = fmax(t[5], 2.2250738585072014e-308);
+  }
+  return numer / fmax(denom, eps);
+}
+
+__device__ void reduce_partials(const double *partial, int nblocks, int nq, int k, bool is_max,
+                                double *out) {
+  __shared__ double sh[256];
+  double v = is_max ? 0.0 : 0.0;
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
+    const double p = partial[(size_t)b * nq + k];
+    v = is_max ? fmax(v, p) : v + p;
+  }
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) {
+      const double o = sh[threadIdx.x + s];
+      sh[threadIdx.x] = is_max ? fmax(sh[threadIdx.x], o) : sh[threadIdx.x] + o;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = sh[0];
+  __syncthreads();
+}
+
+struct FinalizeConsts {
+  int nc, norm, n_grain, has_vp;
+  size_t n_elem_field;  // 2 * n0 * n0
+  double temperature, h, lambda, conv, sum_inv;
+  double log_t_tc[MAX_COMP];
+};
+
+// Free energy and the order-parameter / current residuals
+// (ComputeFreeEnergy.h:281-414, ComputeOrderParameter.h:234-254,
+// ComputeCurrent.h:184-211).
+__global__ void k_scalars_a(FinalizeConsts C, const double *partial, int nblocks, Scalars *S) {
+  __shared__ double t[NQ];
+  for (int k = 0; k < NQ; ++k)
+    reduce_partials(partial, nblocks, NQ, k, (FIN_MAX_MASK >> k) & 1ull, &t[k]);
+  if (threadIdx.x != 0) return;
+  double rop = 0.0;
+  for (int c = 0; c < C.nc; ++c) rop = fmax(rop, residual_from(&t[6 * c], C.n_elem_field, C.norm));
+  S->res_op = rop;
+  S->conv_op = rop < C.conv;
+  const double rj = residual_from(&t[24], C.n_elem_field, C.norm);
+  S->res_j = S->first_j ? C.conv * 0.1 : rj;
+  S->conv_j = S->res_j < C.conv;
+  S->first_j = 0;
+  double nonmag = C.temperature * t[30];
+  for (int c = 0; c < C.nc; ++c) nonmag += t[31 + c] * (C.log_t_tc[c] + C.sum_inv);
+  double mag = 0.0;
+  if (C.has_vp) mag += (0.5 / (C.lambda * C.lambda)) * t[35];
+  const double la = C.h * C.h;
+  const double fe_area = (nonmag + mag) / (double)C.n_grain;
+  const double actual = fabs(S->fe_area_prev - fe_area) / fmax(fabs(S->fe_area_prev), 1e-4);
+  S->res_fe = S->first_fe ? C.conv * 0.1 : actual;
+  S->conv_fe = S->res_fe < C.conv;
+  S->first_fe = 0;
+  S->fe = (nonmag + mag) * la;
+  S->fe_mag = mag * la;
+  S->fe_area = fe_area;
+  S->fe_mag_area = mag / (double)C.n_grain;
+  S->fe_area_prev = fe_area;
+  S->n_grain = (double)C.n_grain;
+  S->j_mean[0] = t[36] / (double)C.n_grain;
+  S->j_mean[1] = t[37] / (double)C.n_grain;
+}
+
+// Boundary and vector-potential residuals, total residual (Context.h:462-483).
+__global__ void k_scalars_b(int norm, size_t n_elem_g, size_t n_elem_gt, size_t n_elem_vp,
+                            int do_bc, int do_vp, int compute_mode, const double *p_bg, int nb_g,
+                            const double *p_bgt, int nb_gt, const double *p_vp, int nb_vp, Scalars *S) {
+  __shared__ double t[18];
+  for (int k = 0; k < 6; ++k) {
+    const bool mx = k >= 4;
+    if (do_bc) {
+      reduce_partials(p_bg, nb_g, 6, k, mx, &t[k]);
+      reduce_partials(p_bgt, nb_gt, 6, k, mx, &t[6 + k]);
+    }
+    if (do_vp) reduce_partials(p_vp, nb_vp, 6, k, mx, &t[12 + k]);
+  }
+  if (threadIdx.x != 0) return;
+  if (do_bc) S->res_bc = fmax(residual_from(&t[0], n_elem_g, norm), residual_from(&t[6], n_elem_gt, norm));
+  if (do_vp) S->res_vp = residual_from(&t[12], n_elem_vp, norm);
+  double r = S->res_vp;
+  r = fmax(S->res_bc, r);
+  if (compute_mode) {
+    r = fmax(r, S->res_op);
+    r = fmax(r, S->res_j);
+    r = fmax(r, S->res_fe);
+  }
+  S->residual = r;
+}
+
+// ---------------------------------------------------------- accelerators --
+// Per-field sums for CongAcc (CongAcc.h:371-385) and Barzilai-Borwein
+// (BarzilaiBorwein.h:214-229): slots [3f] sum d^2, [3f+1] sum m^2, [3f+2] sum d m,
+// where d = g - x and m is the running mean (CongAcc) or the previous d (BB).
+__global__ void __launch_bounds__(REDUCE_THREADS) k_acc_sums(int nf, size_t nn, const double *__restrict__ x,
+                                                             const double *__restrict__ gx,
+                                                             const double *__restrict__ m,
+                                                             double *partial) {
+  const int f = blockIdx.y;
+  double q[3] = {0, 0, 0};
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nn;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const size_t k = (size_t)f * nn + i;
+    const double d = gx[k] - x[k], mv = m[k];
+    q[0] += d * d;
+    q[1] += mv * mv;
+    q[2] += d * mv;
+  }
+  block_reduce(q, 3, 0, partial + ((size_t)f * gridDim.x + blockIdx.x) * 3);
+}
+
+struct AccState {
+  double step[16];
+  double inertia[16];
+  double bb_step;
+  int bb_iter;
+  int initialized;
+};
+
+// CongAcc::computeInertia (CongAcc.h:300-356).
+__device__ double congacc_inertia(double dn, double mn, double dot, double mincos) {
+  double ea = dot / (dn * mn) - mincos, xa = 1.0;
+  double eb = 1.0 - mincos, xb = 0.0;
+  double x = 0.5 * (xa + xb);
+  auto sgn = [](double v) { return (0.0 < v) - (v < 0.0); };
+  for (int it = 0; it < 200; ++it) {
+    const double y = 1.0 - x;
+    const double numer = x * dot + y * dn * dn;
+    const double denom = dn * sqrt(x * x * mn * mn + 2.0 * x * y * dot + y * y * dn * dn);
+    const double err = numer / denom - mincos;
+    const bool conv = fabs(err) < 0.01;
+    if (sgn(err) == sgn(ea)) {
+      ea = err;
+      xa = x;
+    } else {
+      eb = err;
+      xb = x;
+    }
+    if (sgn(ea) == sgn(eb)) break;
+    x = 0.5 * (xa + xb);
+    if (conv) break;
+  }
+  return x;
+}
+
+struct AccConsts {
+  int kind, nf;
+  double step_size, factor, mincos, smax, smin, drag;
+};
+
+// Scalar part of CongAcc::computeInternal (CongAcc.h:371-408) and
+// BarzilaiBorwein::computeInternal (BarzilaiBorwein.h:211-232).
+__global__ void k_acc_scalars(AccConsts C, const double *partial, int nblocks, AccState *st) {
+  __shared__ double t[48];
+  const int nf = C.nf;
+  for (int f = 0; f < nf; ++f)
+    for (int k = 0; k < 3; ++k)
+      reduce_partials(partial + (size_t)f * nblocks * 3, nblocks, 3, k, false, &t[3 * f + k]);
+  if (threadIdx.x != 0) return;
+  if (!st->initialized) {
+    for (int f = 0; f < nf; ++f) {
+      st->step[f] = C.step_size;
+      st->inertia[f] = 0.0;
+    }
+    st->bb_step = C.step_size;
+    st->bb_iter = 0;
+    st->initialized = 1;
+  }
+  if (C.kind == ACC_CONGACC) {
+    for (int f = 0; f < nf; ++f) {
+      const double d = sqrt(t[3 * f]), m = sqrt(t[3 * f + 1]);
+      const double den = d * m;
+      if (den > 0.0) {
+        const double dot = t[3 * f + 2];
+        const double cs = dot / den;
+        st->step[f] *= pow(C.factor, cs);
+        if (cs < C.mincos) st->inertia[f] = congacc_inertia(d, m, dot, C.mincos);
+      }
+      st->step[f] = fmin(fmax(st->step[f], C.smin), C.smax);
+    }
+  } else if (C.kind == ACC_BB) {
+    if (st->bb_iter > 0) {
+      // t: d^2 (= |d|^2), m^2 (= |dprev|^2), d.m (= d . dprev)
+      double dd = 0.0, pp = 0.0, dp = 0.0;
+      for (int f = 0; f < nf; ++f) {
+        dd += t[3 * f];
+        pp += t[3 * f + 1];
+        dp += t[3 * f + 2];
+      }
+      const double dot = fabs(dp - pp);             // |dprev . (d - dprev)|
+      const double ss = dd - 2.0 * dp + pp;         // |d - dprev|^2
+      const double scale = (st->bb_iter % 2 == 0) ? dot / ss : pp / dot;
+      st->bb_step *= scale;
+    }
+    st->bb_step = fmin(fmax(st->bb_step, C.smin), C.smax);
+    st->bb_iter++;
+  }
+}
+
+// Element-wise accelerator update: CongAcc (CongAcc.h:271-297), Picard
+// (Picard.h:133-138), Polyak (Polyak.h:214-239), Barzilai-Borwein
+// (BarzilaiBorwein.h:234-237).
+__global__ void k_acc_update(AccConsts C, size_t nn, const double *__restrict__ gx, double *x,
+                             double *m, const AccState *st) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= (size_t)C.nf * nn) return;
+  const int f = (int)(i / nn);
+  const double d = gx[i] - x[i];
+  if (C.kind == ACC_CONGACC) {
+    const double in = st->inertia[f];
+    const double mean = m[i] * in + d * (1.0 - in);
+    m[i] = mean;
+    x[i] += st->step[f] * mean;
+  } else if (C.kind == ACC_PICARD) {
+    x[i] += d * C.step_size;
+  } else if (C.kind == ACC_POLYAK) {
+    const double v = m[i] * (1.0 - C.drag) + d * C.step_size;
+    m[i] = v;
+    x[i] += v;
+  } else {  // Barzilai-Borwein: m holds the previous difference
+    m[i] = d;
+    x[i] += d * st->bb_step;
+  }
+}
+
+// Zero outside the reference domain (GeometryGroup::zeroValuesOutsideDomainRef).
+__global__ void k_mask(int n_fields, size_t nn, const uint8_t *__restrict__ dom, double *v) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= (size_t)n_fields * nn) return;
+  if (dom[i % nn] == 0) v[i] = 0.0;
+}
+
+template <typename R>
+__global__ void k_to_interleaved(size_t n, const Cx<R> *__restrict__ in, double *out) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  out[2 * i] = (double)in[i].re;
+  out[2 * i + 1] = (double)in[i].im;
+}
+template <typename R>
+__global__ void k_from_interleaved(size_t n, const double *__restrict__ in, Cx<R> *out) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  out[i] = Cx<R>{(R)in[2 * i], (R)in[2 * i + 1]};
+}
+
+// --------------------------------------------------------------- helpers --
+template <typename T>
+struct DevArray {
+  T *p = nullptr;
+  size_t n = 0;
+  DevArray() = default;
+  DevArray(const DevArray &) = delete;
+  DevArray &operator=(const DevArray &) = delete;
+  ~DevArray() { free(); }
+  void alloc(size_t count) {
+    free();
+    n = count;
+    if (count) CUDA_TRY(cudaMalloc(&p, count * sizeof(T)));
+  }
+  void upload(const std::vector<T> &v, cudaStream_t s) {
+    alloc(v.size());
+    if (n) CUDA_TRY(cudaMemcpyAsync(p, v.data(), n * sizeof(T), cudaMemcpyHostToDevice, s));
+  }
+  void zero(cudaStream_t s) {
+    if (n) CUDA_TRY(cudaMemsetAsync(p, 0, n * sizeof(T), s));
+  }
+  void free() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+struct Chunk {
+  int a_begin, a_end;   // angles [a_begin, a_end)
+  int item_begin, item_end;
+  int kmax;             // longest column of the chunk
+};
+
+}  // namespace
+
+// ------------------------------------------------------------------- context
+struct sc_ctx {
+  HostSetup S;
+  int mode = SC_MODE_FP64;
+  cudaStream_t stream = nullptr;      // stream all work is issued on
+  cudaStream_t own_stream = nullptr;  // the stream this context created
+  std::string err;
+  long long launches = 0;
+  int device = 0;
+
+  // static data
+  DevArray<AngleParams> ang;
+  DevArray<uint8_t> labels, dom;
+  DevArray<int> idx_in_g, idx_out_g, idx_in_gt, idx_out_gt;
+  DevArray<double> dist_in_g, dist_out_g, dist_in_gt, dist_out_gt;
+  DevArray<int> bc_src_g, bc_src_gt;
+  DevArray<double> bc_w_g, bc_w_gt, bc_ws_g, bc_ws_gt;
+  DevArray<int> halo_site, halo_off, halo_src, halo_angle;
+  DevArray<int> rext_site, rext_off, rext_src;
+  DevArray<int4> items;
+  DevArray<double> e_im, res, coupling;
+  DevArray<double> filters;
+  DevArray<int> filter_pos;
+  DevArray<int> onode_a_g, onode_x_g, onode_y_g, onode_a_gt, onode_x_gt, onode_y_gt;
+  std::vector<Chunk> chunks;
+  int groups = 1, log_groups = 0, ept = 1;
+
+  // state: x = [delta | avec], g = [delta_new | a_new]
+  DevArray<double> xstate, gstate, dext, j_real;
+  DevArray<double> acc_d, acc_j, acc_fe;
+  DevArray<double> bnd;      // boundary storage (4 arrays), R-typed, viewed through pointers
+  size_t bnd_off[4] = {0, 0, 0, 0};
+  DevArray<double> scratch, scratch2, fg, gi;
+  DevArray<double> partial_fin, partial_bg, partial_bgt, partial_vp, partial_acc;
+  DevArray<double> pois_s, pois_t0, pois_t1;
+  DevArray<double> acc_m;
+  DevArray<AccState> acc_state;
+  DevArray<Scalars> scalars;
+  DevArray<double> tmp_io;
+  int nb_fin = 0, nb_bnd = 0, nb_vp = 0, nb_acc = 0;
+
+  bool boundary_initialized = false, first_compute = true;
+  Scalars host_scalars{};
+
+  size_t nn0() const { return (size_t)S.n0 * S.n0; }
+  size_t esize() const { return mode == SC_MODE_FP64 ? sizeof(Cx<double>) : sizeof(Cx<float>); }
+  void *bnd_ptr(int which) const { return (char *)bnd.p + bnd_off[which]; }
+  int n_bnd(int which) const {
+    return which == 0 ? S.n_in_g : which == 1 ? S.n_out_g : which == 2 ? S.n_in_gt : S.n_out_gt;
+  }
+  bool has_vp() const { return S.lambda > 0.0; }
+  int n_fields() const { return 2 * S.nc + (has_vp() ? 2 : 0); }
+};
+
+namespace {
+
+void check_launch(sc_ctx *c) {
+  c->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) throw EngineError(SC_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+}
+
+unsigned grid1(size_t n, int threads) { return (unsigned)std::max<size_t>(1, (n + threads - 1) / threads); }
+
+template <typename R>
+SweepArgs<R> sweep_args(sc_ctx *c, const Chunk *ch, int burn_in) {
+  const HostSetup &S = c->S;
+  SweepArgs<R> A{};
+  A.n0 = S.n0;
+  A.n1 = S.n1;
+  A.ne = S.ne;
+  A.nc = S.nc;
+  A.groups = c->groups;
+  A.log_groups = c->log_groups;
+  A.ept = c->ept;
+  A.n_items = ch ? ch->item_end - ch->item_begin : 0;
+  A.burn_in = burn_in;
+  A.has_vp = c->has_vp();
+  A.flux_b = M_PI * S.flux_quanta / S.area;
+  A.has_ext = std::fabs(A.flux_b) > 0.0;
+  A.gauge = S.gauge;
+  A.slot_base = ch ? ch->a_begin : 0;
+  A.h = S.h;
+  A.lam_scale = c->has_vp() ? 1.0 / (S.lambda * S.lambda) : 0.0;
+  A.q = (double)S.charge_sign;
+  A.area = S.area;
+  A.items = ch ? c->items.p + ch->item_begin : nullptr;
+  A.ang = c->ang.p;
+  A.labels = c->labels.p;
+  A.idx_in_g = c->idx_in_g.p;
+  A.idx_out_g = c->idx_out_g.p;
+  A.idx_in_gt = c->idx_in_gt.p;
+  A.idx_out_gt = c->idx_out_gt.p;
+  A.dist_in_g = c->dist_in_g.p;
+  A.dist_out_g = c->dist_out_g.p;
+  A.dist_in_gt = c->dist_in_gt.p;
+  A.dist_out_gt = c->dist_out_gt.p;
+  A.bin_g = (const Cx<R> *)c->bnd_ptr(0);
+  A.bout_g = (Cx<R> *)c->bnd_ptr(1);
+  A.bin_gt = (const Cx<R> *)c->bnd_ptr(2);
+  A.bout_gt = (Cx<R> *)c->bnd_ptr(3);
+  A.dext = c->dext.p;
+  A.avec = c->xstate.p + (size_t)2 * S.nc * c->nn0();
+  A.e_im = c->e_im.p;
+  A.res = c->res.p;
+  A.scratch = (Cx<R> *)c->scratch.p;
+  A.scratch2 = c->scratch2.p;
+  A.fg = (double2 *)c->fg.p;
+  A.gi = (double2 *)c->gi.p;
+  return A;
+}
+
+template <typename R>
+void launch_sweep(sc_ctx *c, const Chunk &ch, int burn_in) {
+  SweepArgs<R> A = sweep_args<R>(c, &ch, burn_in);
+  const size_t threads = (size_t)A.n_items * c->groups;
+  if (!threads) return;
+  const unsigned blocks = grid1(threads, 128);
+  if (c->ept <= 4) k_sweep<R, 4><<<blocks, 128, 0, c->stream>>>(A);
+  else if (c->ept <= 8) k_sweep<R, 8><<<blocks, 128, 0, c->stream>>>(A);
+  else k_sweep<R, 16><<<blocks, 128, 0, c->stream>>>(A);
+  check_launch(c);
+}
+
+void extend_reference(sc_ctx *c) {
+  const HostSetup &S = c->S;
+  const size_t bytes = (size_t)2 * S.nc * c->nn0() * sizeof(double);
+  CUDA_TRY(cudaMemcpyAsync(c->dext.p, c->xstate.p, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  const int ns = (int)S.rext_site.size();
+  if (ns) {
+    dim3 grid(grid1(ns, 128), 2 * S.nc);
+    k_extend_reference<<<grid, 128, 0, c->stream>>>(2 * S.nc, (int)c->nn0(), ns, c->rext_site.p,
+                                                    c->rext_off.p, c->rext_src.p, c->xstate.p, c->dext.p);
+    check_launch(c);
+  }
+}
+
+template <typename R>
+void boundary_condition(sc_ctx *c) {
+  const HostSetup &S = c->S;
+  k_boundary<R><<<c->nb_bnd, REDUCE_THREADS, 0, c->stream>>>(
+      S.n_in_g, S.ne, c->bc_src_g.p, c->bc_w_g.p, c->bc_ws_g.p, (const Cx<R> *)c->bnd_ptr(1),
+      (Cx<R> *)c->bnd_ptr(0), c->partial_bg.p);
+  check_launch(c);
+  k_boundary<R><<<c->nb_bnd, REDUCE_THREADS, 0, c->stream>>>(
+      S.n_in_gt, S.ne, c->bc_src_gt.p, c->bc_w_gt.p, c->bc_ws_gt.p, (const Cx<R> *)c->bnd_ptr(3),
+      (Cx<R> *)c->bnd_ptr(2), c->partial_bgt.p);
+  check_launch(c);
+}
+
+template <typename R>
+void boundary_initial(sc_ctx *c) {
+  const HostSetup &S = c->S;
+  extend_reference(c);
+  SweepArgs<R> A = sweep_args<R>(c, nullptr, 1);
+  const size_t ng = (size_t)S.n_out_g * S.ne, ngt = (size_t)S.n_out_gt * S.ne;
+  if (ng) {
+    k_boundary_initial<R><<<grid1(ng, 128), 128, 0, c->stream>>>(
+        S.n_out_g, S.ne, 1, c->onode_a_g.p, c->onode_x_g.p, c->onode_y_g.p, A, (Cx<R> *)c->bnd_ptr(1));
+    check_launch(c);
+  }
+  if (ngt) {
+    k_boundary_initial<R><<<grid1(ngt, 128), 128, 0, c->stream>>>(
+        S.n_out_gt, S.ne, 0, c->onode_a_gt.p, c->onode_x_gt.p, c->onode_y_gt.p, A,
+        (Cx<R> *)c->bnd_ptr(3));
+    check_launch(c);
+  }
+  boundary_condition<R>(c);
+  c->boundary_initialized = true;
+}
+
+void launch_scalars_b(sc_ctx *c, int do_bc, int do_vp, int compute_mode) {
+  const HostSetup &S = c->S;
+  k_scalars_b<<<1, 256, 0, c->stream>>>(S.norm, (size_t)2 * S.n_in_g * S.ne,
+                                         (size_t)2 * S.n_in_gt * S.ne, 2 * c->nn0(), do_bc, do_vp,
+                                         compute_mode, c->partial_bg.p, c->nb_bnd, c->partial_bgt.p,
+                                         c->nb_bnd, c->partial_vp.p, c->nb_vp, c->scalars.p);
+  check_launch(c);
+}
+
+void poisson(sc_ctx *c, const double *j, double *a_out, int mean_from_scalars) {
+  const HostSetup &S = c->S;
+  const int n = S.n0, nk = S.n_filters;
+  const size_t nn2 = 2 * c->nn0();
+  if (mean_from_scalars) {
+    k_subtract_mean<<<grid1(nn2, 256), 256, 0, c->stream>>>(
+        n, j, (const double *)c->scalars.p, (int)(offsetof(Scalars, j_mean) / sizeof(double)),
+        c->pois_s.p);
+    check_launch(c);
+  } else {
+    CUDA_TRY(cudaMemcpyAsync(c->pois_s.p, j, nn2 * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  }
+  dim3 blk(PT, 8);
+  dim3 grid((n + PT - 1) / PT, (n + PT - 1) / PT, 2 * nk);
+  k_toeplitz<<<grid, blk, 0, c->stream>>>(n, nk, c->filters.p, c->pois_s.p, 0, c->pois_t0.p);
+  check_launch(c);
+  k_toeplitz<<<grid, blk, 0, c->stream>>>(n, nk, c->filters.p, c->pois_t0.p, nn2, c->pois_t1.p);
+  check_launch(c);
+  const double factor = -1.0 * (S.h * S.h) * S.vp_scale;
+  k_poisson_sum<<<grid1(nn2, 256), 256, 0, c->stream>>>(n, nk, c->filter_pos.p, c->pois_t1.p, factor, a_out);
+  check_launch(c);
+}
+
+void accelerate(sc_ctx *c) {
+  const HostSetup &S = c->S;
+  AccConsts C{};
+  C.kind = S.acc.kind;
+  C.nf = c->n_fields();
+  C.step_size = S.acc.step_size;
+  C.factor = S.acc.step_size_factor;
+  C.mincos = S.acc.cos_similarity_min;
+  C.smax = S.acc.step_size_max;
+  C.smin = S.acc.step_size_min;
+  C.drag = S.acc.drag;
+  const size_t nn = c->nn0();
+  if (C.kind == ACC_CONGACC || C.kind == ACC_BB) {
+    dim3 grid(c->nb_acc, C.nf);
+    k_acc_sums<<<grid, REDUCE_THREADS, 0, c->stream>>>(C.nf, nn, c->xstate.p, c->gstate.p, c->acc_m.p,
+                                                        c->partial_acc.p);
+    check_launch(c);
+    k_acc_scalars<<<1, 256, 0, c->stream>>>(C, c->partial_acc.p, c->nb_acc, c->acc_state.p);
+    check_launch(c);
+  }
+  k_acc_update<<<grid1((size_t)C.nf * nn, 256), 256, 0, c->stream>>>(C, nn, c->gstate.p, c->xstate.p,
+                                                                       c->acc_m.p, c->acc_state.p);
+  check_launch(c);
+}
+
+template <typename R>
+void run_chunks(sc_ctx *c, int burn_in) {
+  const HostSetup &S = c->S;
+  const size_t nn1 = (size_t)S.n1 * S.n1;
+  for (const Chunk &ch : c->chunks) {
+    const int nslots = ch.a_end - ch.a_begin;
+    if (!burn_in) {
+      CUDA_TRY(cudaMemsetAsync(c->fg.p, 0, (size_t)nslots * nn1 * sizeof(double2), c->stream));
+      CUDA_TRY(cudaMemsetAsync(c->gi.p, 0, (size_t)nslots * nn1 * sizeof(double2), c->stream));
+    }
+    launch_sweep<R>(c, ch, burn_in);
+    if (burn_in) continue;
+    const int h0 = S.halo_angle_off[ch.a_begin], h1 = S.halo_angle_off[ch.a_end];
+    if (h1 > h0) {
+      k_halo<<<grid1(h1 - h0, 128), 128, 0, c->stream>>>(h1 - h0, h0, S.n1, c->halo_angle.p, ch.a_begin,
+                                                          c->halo_site.p, c->halo_off.p, c->halo_src.p,
+                                                          (double2 *)c->fg.p, (double2 *)c->gi.p);
+      check_launch(c);
+    }
+    dim3 blk(32, 8), grid((S.n0 + 31) / 32, (S.n0 + 7) / 8);
+    k_rotate_back<<<grid, blk, 0, c->stream>>>(S.n0, S.n1, S.nc, ch.a_begin, ch.a_end, c->ang.p,
+                                               (const double2 *)c->fg.p, (const double2 *)c->gi.p,
+                                               c->acc_d.p, c->acc_j.p, c->acc_fe.p);
+    check_launch(c);
+  }
+}
+
+template <typename R>
+void compute_once(sc_ctx *c) {
+  const HostSetup &S = c->S;
+  const size_t nn = c->nn0();
+  if (!c->first_compute) accelerate(c);
+  if (!c->boundary_initialized) boundary_initial<R>(c);
+  extend_reference(c);
+  c->acc_d.zero(c->stream);
+  c->acc_j.zero(c->stream);
+  c->acc_fe.zero(c->stream);
+  run_chunks<R>(c, 0);
+  // Finalize.
+  {
+    double *delta = c->xstate.p, *avec = c->xstate.p + (size_t)2 * S.nc * nn;
+    double *delta_new = c->gstate.p;
+    const double jfactor = (double)(2 * S.charge_sign) * S.temperature;
+    k_finalize<<<c->nb_fin, REDUCE_THREADS, 0, c->stream>>>(
+        S.n0, S.nc, S.h, jfactor, c->has_vp() ? 1 : 0, c->dom.p, c->coupling.p, c->acc_d.p, c->acc_j.p,
+        c->acc_fe.p, delta, avec, delta_new, c->j_real.p, c->partial_fin.p);
+    check_launch(c);
+    FinalizeConsts F{};
+    F.nc = S.nc;
+    F.norm = S.norm;
+    F.n_grain = S.n_grain;
+    F.has_vp = c->has_vp() ? 1 : 0;
+    F.n_elem_field = 2 * nn;
+    F.temperature = S.temperature;
+    F.h = S.h;
+    F.lambda = S.lambda;
+    F.conv = S.conv_crit;
+    double si = 0.0;
+    for (int e = 0; e < S.ne; ++e) si += S.residues[e] / S.e_im[e];
+    F.sum_inv = si * S.temperature;
+    for (int k = 0; k < S.nc; ++k) F.log_t_tc[k] = std::log(S.temperature / S.tc[k]);
+    k_scalars_a<<<1, 256, 0, c->stream>>>(F, c->partial_fin.p, c->nb_fin, c->scalars.p);
+    check_launch(c);
+  }
+  boundary_condition<R>(c);
+  if (c->has_vp()) {
+    double *a_new = c->gstate.p + (size_t)2 * S.nc * nn;
+    const double *avec = c->xstate.p + (size_t)2 * S.nc * nn;
+    poisson(c, c->j_real.p, a_new, 1);
+    k_residual<<<c->nb_vp, REDUCE_THREADS, 0, c->stream>>>(2 * nn, avec, a_new, c->partial_vp.p);
+    check_launch(c);
+  }
+  launch_scalars_b(c, 1, c->has_vp() ? 1 : 0, 1);
+  c->first_compute = false;
+}
+
+template <typename R>
+void burn_in_once(sc_ctx *c) {
+  if (!c->boundary_initialized) boundary_initial<R>(c);
+  extend_reference(c);
+  run_chunks<R>(c, 1);
+  boundary_condition<R>(c);
+  launch_scalars_b(c, 1, 0, 0);
+}
+
+void read_scalars(sc_ctx *c) {
+  CUDA_TRY(cudaMemcpyAsync(&c->host_scalars, c->scalars.p, sizeof(Scalars), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+}
+
+// Chunking of the angles so that the sweep scratch and the frame buffers stay
+// within a device-memory budget.
+void plan_chunks(sc_ctx *c, std::vector<int4> &items) {
+  const HostSetup &S = c->S;
+  const int n1 = S.n1, na = S.n_angles;
+  std::vector<int> kmax(na, 0), count(na, 0);
+  std::vector<std::vector<int4>> per(na);
+  for (int a = 0; a < na; ++a)
+    for (int x = S.x0[a]; x <= S.x1[a]; ++x) {
+      const int lo = S.col_lo[(size_t)a * n1 + x], hi = S.col_hi[(size_t)a * n1 + x];
+      if (lo < 0) continue;
+      per[a].push_back(make_int4(a, x, lo, hi));
+      kmax[a] = std::max(kmax[a], hi - lo + 1);
+    }
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  double budget_mb = 0.35 * (double)free_b / 1048576.0;
+  if (const char *env = std::getenv("SCB_SCRATCH_MB")) budget_mb = std::atof(env);
+  const double budget = budget_mb * 1048576.0;
+  const size_t per_row = (size_t)S.ne * c->esize() + 3 * sizeof(double);
+  const size_t frame_slot = (size_t)n1 * n1 * 2 * sizeof(double2);
+  items.clear();
+  int a = 0;
+  while (a < na) {
+    Chunk ch{a, a, (int)items.size(), (int)items.size(), 0};
+    size_t nitems = 0;
+    while (a < na) {
+      const int k2 = std::max(ch.kmax, kmax[a]);
+      const size_t n2 = nitems + per[a].size();
+      const double need = (double)n2 * k2 * per_row + (double)(a - ch.a_begin + 1) * frame_slot;
+      if (a > ch.a_begin && need > budget) break;
+      ch.kmax = k2;
+      nitems = n2;
+      items.insert(items.end(), per[a].begin(), per[a].end());
+      ++a;
+    }
+    ch.a_end = a;
+    ch.item_end = (int)items.size();
+    c->chunks.push_back(ch);
+  }
+}
+
+void upload_static(sc_ctx *c) {
+  HostSetup &S = c->S;
+  cudaStream_t s = c->stream;
+  const int na = S.n_angles;
+  std::vector<AngleParams> ap(na);
+  for (int a = 0; a < na; ++a) {
+    AngleParams &p = ap[a];
+    p.cD = S.cD[a];
+    p.sD = S.sD[a];
+    p.cA = S.cA[a];
+    p.sA = S.sA[a];
+    p.cB = S.cB[a];
+    p.sB = S.sB[a];
+    p.cE = S.cE[a];
+    p.sE = S.sE[a];
+    p.vx = S.vx[a];
+    p.vy = S.vy[a];
+    p.w = S.weight[a];
+    p.sx = S.vx[a] * S.weight[a];
+    p.sy = S.vy[a] * S.weight[a];
+    for (int k = 0; k < MAX_COMP; ++k) p.eta[k] = k < S.nc ? S.eta[(size_t)a * S.nc + k] : 0.0;
+  }
+  c->ang.upload(ap, s);
+  c->labels.upload(S.labels, s);
+  c->dom.upload(S.domain_ref, s);
+  c->idx_in_g.upload(S.idx_in_g, s);
+  c->idx_out_g.upload(S.idx_out_g, s);
+  c->idx_in_gt.upload(S.idx_in_gt, s);
+  c->idx_out_gt.upload(S.idx_out_gt, s);
+  c->dist_in_g.upload(S.dist_in_g, s);
+  c->dist_out_g.upload(S.dist_out_g, s);
+  c->dist_in_gt.upload(S.dist_in_gt, s);
+  c->dist_out_gt.upload(S.dist_out_gt, s);
+  c->bc_src_g.upload(S.bc_g.src, s);
+  c->bc_w_g.upload(S.bc_g.w, s);
+  c->bc_ws_g.upload(S.bc_g.wsum, s);
+  c->bc_src_gt.upload(S.bc_gt.src, s);
+  c->bc_w_gt.upload(S.bc_gt.w, s);
+  c->bc_ws_gt.upload(S.bc_gt.wsum, s);
+  c->halo_site.upload(S.halo_site, s);
+  c->halo_off.upload(S.halo_src_off, s);
+  c->halo_src.upload(S.halo_src, s);
+  std::vector<int> hang(S.halo_site.size());
+  for (int a = 0; a < na; ++a)
+    for (int k = S.halo_angle_off[a]; k < S.halo_angle_off[a + 1]; ++k) hang[k] = a;
+  c->halo_angle.upload(hang, s);
+  c->rext_site.upload(S.rext_site, s);
+  c->rext_off.upload(S.rext_src_off, s);
+  c->rext_src.upload(S.rext_src, s);
+  c->e_im.upload(S.e_im, s);
+  c->res.upload(S.residues, s);
+  c->coupling.upload(S.coupling, s);
+  if (S.n_filters) {
+    c->filters.upload(S.filters, s);
+    c->filter_pos.upload(S.filter_pos, s);
+  }
+  // Exit nodes (for the homogeneous initial boundary values).
+  std::vector<int> ag, xg, yg, agt, xgt, ygt;
+  ag.resize(S.n_out_g);
+  xg.resize(S.n_out_g);
+  yg.resize(S.n_out_g);
+  agt.resize(S.n_out_gt);
+  xgt.resize(S.n_out_gt);
+  ygt.resize(S.n_out_gt);
+  const int n1 = S.n1;
+  for (int a = 0; a < na; ++a)
+    for (int x = 0; x < n1; ++x) {
+      const size_t ax = (size_t)a * n1 + x;
+      if (S.idx_out_g[ax] >= 0)
+        for (int k = 0; k < S.nisect_g[ax]; ++k) {
+          const int o = S.idx_out_g[ax] + k;
+          ag[o] = a;
+          xg[o] = x;
+          yg[o] = S.coord_g[o];
+        }
+      if (S.idx_out_gt[ax] >= 0)
+        for (int k = 0; k < S.nisect_gt[ax]; ++k) {
+          const int o = S.idx_out_gt[ax] + k;
+          agt[o] = a;
+          xgt[o] = x;
+          ygt[o] = S.coord_gt[o];
+        }
+    }
+  c->onode_a_g.upload(ag, s);
+  c->onode_x_g.upload(xg, s);
+  c->onode_y_g.upload(yg, s);
+  c->onode_a_gt.upload(agt, s);
+  c->onode_x_gt.upload(xgt, s);
+  c->onode_y_gt.upload(ygt, s);
+
+  std::vector<int4> items;
+  plan_chunks(c, items);
+  c->items.upload(items, s);
+  // Energy groups per column.
+  c->groups = 1;
+  c->log_groups = 0;
+  const char *eg = std::getenv("SCB_ENERGY_GROUPS");
+  int want = eg ? std::atoi(eg) : (S.ne > 16 ? 4 : S.ne > 8 ? 2 : 1);
+  while (c->groups < want && c->groups < 8) {
+    c->groups *= 2;
+    c->log_groups++;
+  }
+  c->ept = (S.ne + c->groups - 1) / c->groups;
+  if (c->ept > 16) throw EngineError(SC_ERR_ARG, "too many Ozaki energies per thread");
+
+  // State and work buffers.
+  const size_t nn = c->nn0();
+  const int nf = c->n_fields();
+  c->xstate.alloc((size_t)(2 * S.nc + 2) * nn);
+  c->gstate.alloc((size_t)(2 * S.nc + 2) * nn);
+  c->xstate.zero(s);
+  c->gstate.zero(s);
+  c->dext.alloc((size_t)2 * S.nc * nn);
+  c->j_real.alloc(2 * nn);
+  c->j_real.zero(s);
+  c->acc_d.alloc((size_t)2 * S.nc * nn);
+  c->acc_j.alloc(2 * nn);
+  c->acc_fe.alloc(nn);
+  size_t off = 0;
+  for (int w = 0; w < 4; ++w) {
+    c->bnd_off[w] = off;
+    off += (size_t)c->n_bnd(w) * S.ne * c->esize();
+    off = (off + 255) & ~size_t(255);
+  }
+  c->bnd.alloc(off / sizeof(double) + 1);
+  c->bnd.zero(s);
+  size_t scr = 0, scr2 = 0;
+  int max_slots = 1;
+  for (const Chunk &ch : c->chunks) {
+    const size_t ni = (size_t)(ch.item_end - ch.item_begin);
+    scr = std::max(scr, ni * ch.kmax * S.ne * c->esize());
+    scr2 = std::max(scr2, ni * ch.kmax * 3);
+    max_slots = std::max(max_slots, ch.a_end - ch.a_begin);
+  }
+  c->scratch.alloc(scr / sizeof(double) + 1);
+  c->scratch2.alloc(scr2 + 1);
+  c->fg.alloc((size_t)max_slots * n1 * n1 * 2);
+  c->gi.alloc((size_t)max_slots * n1 * n1 * 2);
+  c->nb_fin = std::min<int>(592, (int)grid1(nn, REDUCE_THREADS));
+  c->nb_bnd = 296;
+  c->nb_vp = std::min<int>(296, (int)grid1(2 * nn, REDUCE_THREADS));
+  c->nb_acc = std::min<int>(148, (int)grid1(nn, REDUCE_THREADS));
+  c->partial_fin.alloc((size_t)c->nb_fin * NQ);
+  c->partial_bg.alloc((size_t)c->nb_bnd * 6);
+  c->partial_bgt.alloc((size_t)c->nb_bnd * 6);
+  c->partial_vp.alloc((size_t)c->nb_vp * 6);
+  c->partial_acc.alloc((size_t)16 * c->nb_acc * 3);
+  c->partial_vp.zero(s);
+  if (S.n_filters) {
+    c->pois_s.alloc(2 * nn);
+    c->pois_t0.alloc((size_t)S.n_filters * 2 * nn);
+    c->pois_t1.alloc((size_t)S.n_filters * 2 * nn);
+  }
+  c->acc_m.alloc((size_t)std::max(nf, 1) * nn);
+  c->acc_m.zero(s);
+  c->acc_state.alloc(1);
+  c->acc_state.zero(s);
+  c->scalars.alloc(1);
+  Scalars init{};
+  init.first_j = 1;
+  init.first_fe = 1;
+  CUDA_TRY(cudaMemcpyAsync(c->scalars.p, &init, sizeof(Scalars), cudaMemcpyHostToDevice, s));
+  c->tmp_io.alloc((size_t)(2 * S.nc + 2) * nn);
+  CUDA_TRY(cudaStreamSynchronize(s));
+}
+
+int fail(sc_ctx *c, const EngineError &e) {
+  if (c) c->err = e.msg;
+  else g_create_error = e.msg;
+  return e.code;
+}
+
+#define API_BEGIN try {
+#define API_END                                              \
+  }                                                          \
+  catch (const EngineError &e) { return fail(ctx, e); }      \
+  catch (const std::exception &e) {                          \
+    return fail(ctx, EngineError(SC_ERR_ARG, e.what()));     \
+  }                                                          \
+  return SC_OK;
+
+}  // namespace
+
+extern "C" {
+
+int sc_create(const char *config_json, int mode, sc_ctx **out) {
+  sc_ctx *ctx = nullptr;
+  if (!config_json || !out) {
+    g_create_error = "sc_create: null argument";
+    return SC_ERR_ARG;
+  }
+  *out = nullptr;
+  if (mode != SC_MODE_FP64 && mode != SC_MODE_MIXED) {
+    g_create_error = "sc_create: mode must be SC_MODE_FP64 or SC_MODE_MIXED";
+    return SC_ERR_ARG;
+  }
+  sc_ctx *c = new sc_ctx();
+  c->mode = mode;
+  try {
+    const std::string e = build_setup(config_json, c->S);
+    if (!e.empty()) throw EngineError(SC_ERR_ARG, e);
+    if (c->S.nc > MAX_COMP) throw EngineError(SC_ERR_ARG, "at most 4 order-parameter components");
+    if (2 * c->S.nc + 2 > 16) throw EngineError(SC_ERR_ARG, "too many accelerator fields");
+    if (c->S.acc.kind == ACC_ANDERSON)
+      throw EngineError(SC_ERR_ARG, "accelerator 'anderson' is not available in this engine");
+    CUDA_TRY(cudaGetDevice(&c->device));
+    CUDA_TRY(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
+    c->stream = c->own_stream;
+    upload_static(c);
+  } catch (const EngineError &e) {
+    g_create_error = e.msg;
+    cudaStream_t s = c->own_stream;
+    delete c;
+    if (s) cudaStreamDestroy(s);
+    return e.code;
+  } catch (const std::exception &e) {
+    g_create_error = e.what();
+    delete c;
+    return SC_ERR_ARG;
+  }
+  *out = c;
+  return SC_OK;
+}
+
+int sc_destroy(sc_ctx *ctx) {
+  if (!ctx) return SC_OK;
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  cudaStream_t s = ctx->own_stream;
+  delete ctx;  // device arrays free themselves
+  if (s) cudaStreamDestroy(s);
+  return SC_OK;
+}
+
+const char *sc_last_error(const sc_ctx *ctx) {
+  return ctx ? ctx->err.c_str() : g_create_error.c_str();
+}
+
+int sc_get_dims(const sc_ctx *ctx, int *n0, int *n1, int *n_angles, int *n_energies, int *n_comp) {
+  if (!ctx) return SC_ERR_ARG;
+  if (n0) *n0 = ctx->S.n0;
+  if (n1) *n1 = ctx->S.n1;
+  if (n_angles) *n_angles = ctx->S.n_angles;
+  if (n_energies) *n_energies = ctx->S.ne;
+  if (n_comp) *n_comp = ctx->S.nc;
+  return SC_OK;
+}
+
+int sc_site_updates(const sc_ctx *ctx, long long *per_iteration) {
+  if (!ctx || !per_iteration) return SC_ERR_ARG;
+  *per_iteration = ctx->S.site_updates_per_iteration();
+  return SC_OK;
+}
+
+int sc_set_stream(sc_ctx *ctx, void *stream) {
+  if (!ctx) return SC_ERR_ARG;
+  API_BEGIN
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+  API_END
+}
+
+int sc_set_state(sc_ctx *ctx, const double *delta, const double *a_internal) {
+  if (!ctx || !delta) return SC_ERR_ARG;
+  API_BEGIN
+  const size_t nn = ctx->nn0(), nd = (size_t)2 * ctx->S.nc * nn;
+  CUDA_TRY(cudaMemcpyAsync(ctx->xstate.p, delta, nd * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  if (a_internal)
+    CUDA_TRY(cudaMemcpyAsync(ctx->xstate.p + nd, a_internal, 2 * nn * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  else
+    CUDA_TRY(cudaMemsetAsync(ctx->xstate.p + nd, 0, 2 * nn * sizeof(double), ctx->stream));
+  if (!ctx->has_vp()) CUDA_TRY(cudaMemsetAsync(ctx->xstate.p + nd, 0, 2 * nn * sizeof(double), ctx->stream));
+  k_mask<<<grid1(nd, 256), 256, 0, ctx->stream>>>(2 * ctx->S.nc, nn, ctx->dom.p, ctx->xstate.p);
+  check_launch(ctx);
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  API_END
+}
+
+int sc_set_state_device(sc_ctx *ctx, const double *d_delta, const double *d_a) {
+  if (!ctx || !d_delta) return SC_ERR_ARG;
+  API_BEGIN
+  const size_t nn = ctx->nn0(), nd = (size_t)2 * ctx->S.nc * nn;
+  CUDA_TRY(cudaMemcpyAsync(ctx->xstate.p, d_delta, nd * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  if (d_a && ctx->has_vp())
+    CUDA_TRY(cudaMemcpyAsync(ctx->xstate.p + nd, d_a, 2 * nn * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  else
+    CUDA_TRY(cudaMemsetAsync(ctx->xstate.p + nd, 0, 2 * nn * sizeof(double), ctx->stream));
+  k_mask<<<grid1(nd, 256), 256, 0, ctx->stream>>>(2 * ctx->S.nc, nn, ctx->dom.p, ctx->xstate.p);
+  check_launch(ctx);
+  API_END
+}
+
+int sc_get_state(sc_ctx *ctx, double *delta, double *a_internal) {
+  if (!ctx) return SC_ERR_ARG;
+  API_BEGIN
+  const size_t nn = ctx->nn0(), nd = (size_t)2 * ctx->S.nc * nn;
+  if (delta) CUDA_TRY(cudaMemcpyAsync(delta, ctx->xstate.p, nd * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  if (a_internal)
+    CUDA_TRY(cudaMemcpyAsync(a_internal, ctx->xstate.p + nd, 2 * nn * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  API_END
+}
+
+int sc_get_state_device(sc_ctx *ctx, double *d_delta, double *d_a) {
+  if (!ctx) return SC_ERR_ARG;
+  API_BEGIN
+  const size_t nn = ctx->nn0(), nd = (size_t)2 * ctx->S.nc * nn;
+  if (d_delta) CUDA_TRY(cudaMemcpyAsync(d_delta, ctx->xstate.p, nd * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  if (d_a) CUDA_TRY(cudaMemcpyAsync(d_a, ctx->xstate.p + nd, 2 * nn * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  API_END
+}
+
+int sc_compute(sc_ctx *ctx, int n, double *residual, int *converged) {
+  if (!ctx || n < 0) return SC_ERR_ARG;
+  API_BEGIN
+  for (int i = 0; i < n; ++i) {
+    if (ctx->mode == SC_MODE_FP64) compute_once<double>(ctx);
+    else compute_once<float>(ctx);
+  }
+  read_scalars(ctx);
+  const Scalars &s = ctx->host_scalars;
+  if (residual) *residual = s.residual;
+  if (converged)
+    *converged = (s.residual < ctx->S.conv_crit && s.conv_op && s.conv_j && s.conv_fe) ? 1 : 0;
+  API_END
+}
+
+int sc_burn_in(sc_ctx *ctx, int n, double *residual, int *converged) {
+  if (!ctx || n < 0) return SC_ERR_ARG;
+  API_BEGIN
+  for (int i = 0; i < n; ++i) {
+    if (ctx->mode == SC_MODE_FP64) burn_in_once<double>(ctx);
+    else burn_in_once<float>(ctx);
+  }
+  read_scalars(ctx);
+  if (residual) *residual = ctx->host_scalars.res_bc;
+  if (converged) *converged = ctx->host_scalars.res_bc < ctx->S.conv_crit ? 1 : 0;
+  API_END
+}
+
+int sc_get_results(sc_ctx *ctx, double *delta_new, double *j, double *a_new) {
+  if (!ctx) return SC_ERR_ARG;
+  API_BEGIN
+  const size_t nn = ctx->nn0(), nd = (size_t)2 * ctx->S.nc * nn;
+  if (delta_new) CUDA_TRY(cudaMemcpyAsync(delta_new, ctx->gstate.p, nd * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  if (j) CUDA_TRY(cudaMemcpyAsync(j, ctx->j_real.p, 2 * nn * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  if (a_new) CUDA_TRY(cudaMemcpyAsync(a_new, ctx->gstate.p + nd, 2 * nn * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  API_END
+}
+
+int sc_get_scalars(sc_ctx *ctx, double *out) {
+  if (!ctx || !out) return SC_ERR_ARG;
+  API_BEGIN
+  read_scalars(ctx);
+  const Scalars &s = ctx->host_scalars;
+  const double v[11] = {s.fe, s.fe_area, s.fe_mag, s.fe_mag_area, s.res_op, s.res_j,
+                        s.res_fe, s.res_vp, s.res_bc, s.residual, (double)ctx->S.n_grain};
+  std::memcpy(out, v, sizeof(v));
+  API_END
+}
+
+int sc_get_frame_labels(const sc_ctx *ctx, int angle, signed char *labels, int *box) {
+  if (!ctx || angle < 0 || angle >= ctx->S.n_angles) return SC_ERR_ARG;
+  const size_t nn1 = (size_t)ctx->S.n1 * ctx->S.n1;
+  if (labels) std::memcpy(labels, &ctx->S.labels[(size_t)angle * nn1], nn1);
+  if (box) {
+    box[0] = ctx->S.x0[angle];
+    box[1] = ctx->S.x1[angle];
+    box[2] = ctx->S.y0[angle];
+    box[3] = ctx->S.y1[angle];
+  }
+  return SC_OK;
+}
+
+int sc_get_domain(const sc_ctx *ctx, signed char *domain) {
+  if (!ctx || !domain) return SC_ERR_ARG;
+  std::memcpy(domain, ctx->S.domain_ref.data(), ctx->S.domain_ref.size());
+  return SC_OK;
+}
+
+int sc_boundary_sizes(const sc_ctx *ctx, int *sizes) {
+  if (!ctx || !sizes) return SC_ERR_ARG;
+  for (int w = 0; w < 4; ++w) sizes[w] = ctx->n_bnd(w);
+  return SC_OK;
+}
+
+int sc_get_boundary(sc_ctx *ctx, int which, double *values) {
+  if (!ctx || which < 0 || which > 3 || !values) return SC_ERR_ARG;
+  API_BEGIN
+  const size_t n = (size_t)ctx->n_bnd(which) * ctx->S.ne;
+  if (n) {
+    if (ctx->mode == SC_MODE_FP64) {
+      CUDA_TRY(cudaMemcpyAsync(values, ctx->bnd_ptr(which), n * 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    } else {
+      double *tmp = nullptr;
+      CUDA_TRY(cudaMallocAsync(&tmp, n * 2 * sizeof(double), ctx->stream));
+      k_to_interleaved<float><<<grid1(n, 256), 256, 0, ctx->stream>>>(n, (const Cx<float> *)ctx->bnd_ptr(which), tmp);
+      check_launch(ctx);
+      CUDA_TRY(cudaMemcpyAsync(values, tmp, n * 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+      CUDA_TRY(cudaFreeAsync(tmp, ctx->stream));
+    }
+  }
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  API_END
+}
+
+int sc_set_boundary(sc_ctx *ctx, int which, const double *values) {
+  if (!ctx || which < 0 || which > 3 || !values) return SC_ERR_ARG;
+  API_BEGIN
+  const size_t n = (size_t)ctx->n_bnd(which) * ctx->S.ne;
+  if (n) {
+    if (ctx->mode == SC_MODE_FP64) {
+      CUDA_TRY(cudaMemcpyAsync(ctx->bnd_ptr(which), values, n * 2 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    } else {
+      double *tmp = nullptr;
+      CUDA_TRY(cudaMallocAsync(&tmp, n * 2 * sizeof(double), ctx->stream));
+      CUDA_TRY(cudaMemcpyAsync(tmp, values, n * 2 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+      k_from_interleaved<float><<<grid1(n, 256), 256, 0, ctx->stream>>>(n, tmp, (Cx<float> *)ctx->bnd_ptr(which));
+      check_launch(ctx);
+      CUDA_TRY(cudaFreeAsync(tmp, ctx->stream));
+    }
+  }
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  ctx->boundary_initialized = true;
+  API_END
+}
+
+int sc_boundary_initial(sc_ctx *ctx) {
+  if (!ctx) return SC_ERR_ARG;
+  API_BEGIN
+  if (ctx->mode == SC_MODE_FP64) boundary_initial<double>(ctx);
+  else boundary_initial<float>(ctx);
+  launch_scalars_b(ctx, 1, 0, 0);
+  read_scalars(ctx);
+  API_END
+}
+
+int sc_angle_greens(sc_ctx *ctx, int angle, double *f, double *g_re, double *i_re) {
+  if (!ctx || angle < 0 || angle >= ctx->S.n_angles) return SC_ERR_ARG;
+  API_BEGIN
+  const HostSetup &S = ctx->S;
+  // Locate the chunk of this angle and sweep only its items.
+  const Chunk *owner = nullptr;
+  for (const Chunk &ch : ctx->chunks)
+    if (angle >= ch.a_begin && angle < ch.a_end) owner = &ch;
+  if (!owner) throw EngineError(SC_ERR_STATE, "angle not planned");
+  std::vector<int4> all(owner->item_end - owner->item_begin);
+  CUDA_TRY(cudaMemcpy(all.data(), ctx->items.p + owner->item_begin, all.size() * sizeof(int4), cudaMemcpyDeviceToHost));
+  int ib = -1, ie = -1;
+  for (size_t k = 0; k < all.size(); ++k)
+    if (all[k].x == angle) {
+      if (ib < 0) ib = (int)k;
+      ie = (int)k + 1;
+    }
+  const size_t nn1 = (size_t)S.n1 * S.n1;
+  extend_reference(ctx);
+  CUDA_TRY(cudaMemsetAsync(ctx->fg.p, 0, nn1 * sizeof(double2), ctx->stream));
+  CUDA_TRY(cudaMemsetAsync(ctx->gi.p, 0, nn1 * sizeof(double2), ctx->stream));
+  if (ib >= 0) {
+    Chunk one{angle, angle + 1, owner->item_begin + ib, owner->item_begin + ie, owner->kmax};
+    if (ctx->mode == SC_MODE_FP64) launch_sweep<double>(ctx, one, 0);
+    else launch_sweep<float>(ctx, one, 0);
+  }
+  std::vector<double2> hf(nn1), hg(nn1);
+  CUDA_TRY(cudaMemcpyAsync(hf.data(), ctx->fg.p, nn1 * sizeof(double2), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaMemcpyAsync(hg.data(), ctx->gi.p, nn1 * sizeof(double2), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  for (size_t i = 0; i < nn1; ++i) {
+    if (f) {
+      f[i] = hf[i].x;
+      f[nn1 + i] = hf[i].y;
+    }
+    if (g_re) g_re[i] = hg[i].x;
+    if (i_re) i_re[i] = hg[i].y;
+  }
+  API_END
+}
+
+int sc_poisson(sc_ctx *ctx, const double *j, double *a_out) {
+  if (!ctx || !j || !a_out) return SC_ERR_ARG;
+  if (!ctx->has_vp()) {
+    ctx->err = "sc_poisson: the configuration has no finite penetration depth";
+    return SC_ERR_STATE;
+  }
+  API_BEGIN
+  const size_t nn2 = 2 * ctx->nn0();
+  // Subtract the mean on the host input (ComputeVectorPotential::subtractMean).
+  std::vector<double> s(j, j + nn2);
+  for (int d = 0; d < 2; ++d) {
+    double sum = 0.0;
+    for (size_t i = 0; i < nn2 / 2; ++i) sum += s[d * nn2 / 2 + i];
+    const double mean = sum / (double)ctx->S.n_grain;
+    for (size_t i = 0; i < nn2 / 2; ++i) s[d * nn2 / 2 + i] -= mean;
+  }
+  CUDA_TRY(cudaMemcpyAsync(ctx->tmp_io.p, s.data(), nn2 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  double *out = ctx->tmp_io.p + nn2;
+  poisson(ctx, ctx->tmp_io.p, out, 0);
+  CUDA_TRY(cudaMemcpyAsync(a_out, out, nn2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  API_END
+}
+
+int sc_launch_count(const sc_ctx *ctx, long long *count) {
+  if (!ctx || !count) return SC_ERR_ARG;
+  *count = ctx->launches;
+  return SC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,262 @@
+"""Python face of the B200 engine, shaped like the reference's C++ Context.
+
+``Context`` owns one libscb200 handle.  Its methods follow the reference's
+orchestration API (include/conga/Context.h): ``compute`` runs
+``Context::compute`` iterations, ``burn_in`` runs ``Context::burnIn``,
+``residual`` / ``is_converged`` mirror ``getResidual`` /
+``isPartiallyConverged``, and the grids come back in the reference's planar
+layout (GridData.h:276-291) as numpy arrays.
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+
+MODES = {"fp64": 0, "mixed": 1}
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+@dataclass
+class Dims:
+    n0: int
+    n1: int
+    n_angles: int
+    n_energies: int
+    n_comp: int
+
+
+class Context:
+    """One self-consistency context on the current CUDA device."""
+
+    def __init__(self, config: dict | str, mode: str = "fp64"):
+        cfg = config if isinstance(config, str) else json.dumps(config)
+        lib = _lib.load()
+        h = ctypes.c_void_p()
+        _lib.check(lib.sc_create(cfg.encode(), MODES[mode], ctypes.byref(h)))
+        self._h = h
+        self.mode = mode
+        ints = [ctypes.c_int() for _ in range(5)]
+        _lib.check(lib.sc_get_dims(h, *[ctypes.byref(i) for i in ints]), h)
+        self.dims = Dims(*[i.value for i in ints])
+
+    # ----------------------------------------------------------- lifetime --
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().sc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, status: int):
+        _lib.check(status, self._h)
+
+    # ------------------------------------------------------------ state ----
+    def _shape_delta(self):
+        d = self.dims
+        return (d.n_comp, 2, d.n0, d.n0)
+
+    def _shape_vec(self):
+        return (2, self.dims.n0, self.dims.n0)
+
+    def set_state(self, delta: np.ndarray, a_internal: np.ndarray | None = None):
+        """x = (order parameter [Nc][2][N0][N0], vector potential [2][N0][N0])."""
+        d = np.ascontiguousarray(delta, np.float64).reshape(self._shape_delta())
+        a = None if a_internal is None else np.ascontiguousarray(a_internal, np.float64).reshape(self._shape_vec())
+        self._check(_lib.load().sc_set_state(self._h, _p(d), _p(a) if a is not None else None))
+
+    def state(self):
+        d = np.zeros(self._shape_delta())
+        a = np.zeros(self._shape_vec())
+        self._check(_lib.load().sc_get_state(self._h, _p(d), _p(a)))
+        return d, a
+
+    def set_state_device(self, delta_ptr: int, a_ptr: int | None = None):
+        self._check(_lib.load().sc_set_state_device(self._h, ctypes.c_void_p(delta_ptr),
+                                                    ctypes.c_void_p(a_ptr) if a_ptr else None))
+
+    def get_state_device(self, delta_ptr: int, a_ptr: int | None = None):
+        self._check(_lib.load().sc_get_state_device(self._h, ctypes.c_void_p(delta_ptr),
+                                                    ctypes.c_void_p(a_ptr) if a_ptr else None))
+
+    def set_stream(self, stream_ptr: int):
+        self._check(_lib.load().sc_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
+
+    # ------------------------------------------------------- iteration ----
+    def compute(self, n: int = 1):
+        """n x Context::compute; returns (residual, converged) of the last one."""
+        r = ctypes.c_double()
+        c = ctypes.c_int()
+        self._check(_lib.load().sc_compute(self._h, int(n), ctypes.byref(r), ctypes.byref(c)))
+        return r.value, bool(c.value)
+
+    def burn_in(self, n: int = 1):
+        r = ctypes.c_double()
+        c = ctypes.c_int()
+        self._check(_lib.load().sc_burn_in(self._h, int(n), ctypes.byref(r), ctypes.byref(c)))
+        return r.value, bool(c.value)
+
+    def run(self, it_min: int, it_max: int, burn_in: int = 0):
+        """runSimulation without I/O (run_simulation.h:124-187): burn-in, then
+        iterate until converged and it_min reached, or it_max reached."""
+        if burn_in:
+            self.burn_in(burn_in)
+        i, conv = 0, False
+        while True:
+            i += 1
+            _, conv = self.compute(1)
+            if (conv and i >= it_min) or (it_max >= 0 and i >= it_max):
+                return i, conv
+
+    def results(self):
+        """g(x): new order parameter, current density, new vector potential."""
+        d = np.zeros(self._shape_delta())
+        j = np.zeros(self._shape_vec())
+        a = np.zeros(self._shape_vec())
+        self._check(_lib.load().sc_get_results(self._h, _p(d), _p(j), _p(a)))
+        return d, j, a
+
+    def scalars(self) -> dict:
+        out = np.zeros(11)
+        self._check(_lib.load().sc_get_scalars(self._h, _p(out)))
+        keys = ["free_energy", "free_energy_per_area", "magnetic_free_energy",
+                "magnetic_free_energy_per_area", "res_order_parameter", "res_current",
+                "res_free_energy", "res_vector_potential", "res_boundary", "residual",
+                "n_grain"]
+        return dict(zip(keys, out.tolist()))
+
+    def site_updates(self) -> int:
+        v = ctypes.c_longlong()
+        self._check(_lib.load().sc_site_updates(self._h, ctypes.byref(v)))
+        return v.value
+
+    def launch_count(self) -> int:
+        v = ctypes.c_longlong()
+        self._check(_lib.load().sc_launch_count(self._h, ctypes.byref(v)))
+        return v.value
+
+    # ---------------------------------------------------------- probes -----
+    def frame_labels(self, angle: int):
+        n1 = self.dims.n1
+        lab = np.zeros((n1, n1), np.int8)
+        box = (ctypes.c_int * 4)()
+        self._check(_lib.load().sc_get_frame_labels(self._h, angle, _p(lab), box))
+        return lab, tuple(box)
+
+    def domain(self):
+        d = np.zeros((self.dims.n0, self.dims.n0), np.int8)
+        self._check(_lib.load().sc_get_domain(self._h, _p(d)))
+        return d
+
+    def boundary_sizes(self):
+        s = (ctypes.c_int * 4)()
+        self._check(_lib.load().sc_boundary_sizes(self._h, s))
+        return list(s)
+
+    def boundary(self, which: int) -> np.ndarray:
+        n = self.boundary_sizes()[which] * self.dims.n_energies
+        v = np.zeros(2 * n)
+        self._check(_lib.load().sc_get_boundary(self._h, which, _p(v)))
+        return v[0::2] + 1j * v[1::2]
+
+    def set_boundary(self, which: int, values: np.ndarray):
+        v = np.ascontiguousarray(np.stack([values.real, values.imag], -1).ravel(), np.float64)
+        self._check(_lib.load().sc_set_boundary(self._h, which, _p(v)))
+
+    def boundary_initial(self):
+        self._check(_lib.load().sc_boundary_initial(self._h))
+
+    def angle_greens(self, angle: int):
+        n1 = self.dims.n1
+        f = np.zeros((2, n1, n1))
+        g = np.zeros((n1, n1))
+        i = np.zeros((n1, n1))
+        self._check(_lib.load().sc_angle_greens(self._h, angle, _p(f), _p(g), _p(i)))
+        return f[0] + 1j * f[1], g, i
+
+    def poisson(self, j: np.ndarray) -> np.ndarray:
+        jj = np.ascontiguousarray(j, np.float64).reshape(self._shape_vec())
+        out = np.zeros(self._shape_vec())
+        self._check(_lib.load().sc_poisson(self._h, _p(jj), _p(out)))
+        return out
+
+
+class Setup:
+    """Host-only view of a configuration's static tables (no GPU needed)."""
+
+    def __init__(self, config: dict | str):
+        cfg = config if isinstance(config, str) else json.dumps(config)
+        lib = _lib.load()
+        h = ctypes.c_void_p()
+        st = lib.sc_setup_create(cfg.encode(), ctypes.byref(h))
+        if st != 0:
+            raise _lib.EngineError(st, lib.sc_setup_last_error().decode())
+        self._h = h
+        ints = [ctypes.c_int() for _ in range(5)]
+        lib.sc_setup_dims(h, *[ctypes.byref(i) for i in ints])
+        self.dims = Dims(*[i.value for i in ints])
+
+    def __del__(self):
+        try:
+            if getattr(self, "_h", None):
+                _lib.load().sc_setup_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+    def energies(self):
+        ne = self.dims.n_energies
+        e = np.zeros(ne)
+        r = np.zeros(ne)
+        _lib.load().sc_setup_energies(self._h, _p(e), _p(r))
+        return e, r
+
+    def frame(self, angle: int):
+        n1 = self.dims.n1
+        lab = np.zeros((n1, n1), np.int8)
+        box = (ctypes.c_int * 4)()
+        _lib.check(_lib.load().sc_setup_frame(self._h, angle, _p(lab), box))
+        return lab, tuple(box)
+
+    def domain(self):
+        d = np.zeros((self.dims.n0, self.dims.n0), np.int8)
+        _lib.load().sc_setup_domain(self._h, _p(d))
+        return d
+
+    def boundary_sizes(self):
+        s = (ctypes.c_int * 4)()
+        _lib.load().sc_setup_boundary_sizes(self._h, s)
+        return list(s)
+
+    def filters(self):
+        lib = _lib.load()
+        n = ctypes.c_int()
+        lib.sc_setup_filters(self._h, ctypes.byref(n), None, None, None)
+        f = np.zeros((n.value, 2 * self.dims.n0 - 1))
+        pos = np.zeros(n.value, np.int32)
+        sc = ctypes.c_double()
+        lib.sc_setup_filters(self._h, ctypes.byref(n), _p(f), pos.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                             ctypes.byref(sc))
+        return f, pos, sc.value
+
+    def site_updates(self) -> int:
+        v = ctypes.c_longlong()
+        _lib.load().sc_setup_site_updates(self._h, ctypes.byref(v))
+        return v.value

@@ -1,0 +1,103 @@
+"""Seeded configurations and inputs shared by the tests.
+
+The configurations use the reference's JSON schema
+(examples/swave_disc_vortex/simulation_config.json in the reference project).
+Sizes are kept small enough for the CPU oracle to finish in seconds.
+"""
+from __future__ import annotations
+
+import copy
+import math
+
+import numpy as np
+
+
+def golden_disc(accelerator: str = "congacc") -> dict:
+    """The accelerator known-answer case of tests/accelerators_test.cu:45-149:
+    disc of width 10 xi0 at 3 points/xi0, 16 angles, T = 0.5, cutoff 16,
+    one flux quantum, lambda = 10, symmetric gauge, L-infinity residuals,
+    convergence 1e-5, bulk s-wave start."""
+    return {
+        "physics": {"temperature": 0.5, "external_flux_quanta": 1.0, "penetration_depth": 10.0,
+                    "charge_sign": -1, "gauge": "symmetric", "crystal_axes_rotation": 0.0,
+                    "order_parameter": {"s": {"critical_temperature": 1.0}}},
+        "geometry": [{"disc": {"add": True, "radius": 5.0, "center_x": 0.0, "center_y": 0.0}}],
+        "numerics": {"points_per_coherence_length": 3.0, "num_fermi_momenta": 16,
+                     "energy_cutoff": 16.0, "convergence_criterion": 1e-5, "norm": "linf",
+                     "vector_potential_error": 1e-6},
+        "accelerator": {"name": accelerator},
+    }
+
+
+GOLDEN_FREE_ENERGY_PER_AREA = -0.0185386592  # tests/accelerators_test.cu:136
+
+
+def small_disc() -> dict:
+    """C1 in miniature: s-wave disc R = 5 xi0 at 5 points/xi0, 32 angles,
+    T = 0.5, cutoff 8 (7 Ozaki poles), b = 0.02 B0, kappa = 2, CongAcc."""
+    r = 5.0
+    return {
+        "physics": {"temperature": 0.5, "external_flux_quanta": 0.02 * math.pi * r * r / math.pi,
+                    "penetration_depth": 2.0, "charge_sign": -1, "gauge": "symmetric",
+                    "crystal_axes_rotation": 0.0,
+                    "order_parameter": {"s": {"critical_temperature": 1.0}}},
+        "geometry": [{"disc": {"add": True, "radius": r, "center_x": 0.0, "center_y": 0.0}}],
+        "numerics": {"points_per_coherence_length": 5.0, "num_fermi_momenta": 32,
+                     "energy_cutoff": 8.0, "convergence_criterion": 1e-6, "norm": "l2",
+                     "vector_potential_error": 1e-6},
+        "accelerator": {"name": "congacc"},
+    }
+
+
+def small_square_d() -> dict:
+    """C2 in miniature: d_{x2-y2} square of side 8 xi0 with axes at 45 degrees,
+    5 points/xi0, 24 angles, T = 0.1 (14 Ozaki poles), no external field,
+    kappa = 2."""
+    return {
+        "physics": {"temperature": 0.1, "external_flux_quanta": 0.0, "penetration_depth": 2.0,
+                    "charge_sign": -1, "gauge": "symmetric", "crystal_axes_rotation": 0.125,
+                    "order_parameter": {"dx2-y2": {"critical_temperature": 1.0}}},
+        "geometry": [{"regular_polygon": {"add": True, "num_edges": 4, "side_length": 8.0,
+                                          "rotation": 0.0, "center_x": 0.0, "center_y": 0.0}}],
+        "numerics": {"points_per_coherence_length": 5.0, "num_fermi_momenta": 24,
+                     "energy_cutoff": 8.0, "convergence_criterion": 1e-6, "norm": "l2",
+                     "vector_potential_error": 1e-6},
+        "accelerator": {"name": "congacc"},
+    }
+
+
+def chiral_annulus() -> dict:
+    """d + i d_xy with a hole: a disc with a smaller disc removed (the remove
+    operator of GeometryGroup.h:216-334), Landau gauge, L1 residuals."""
+    return {
+        "physics": {"temperature": 0.3, "external_flux_quanta": 0.5, "penetration_depth": 3.0,
+                    "charge_sign": -1, "gauge": "landau", "crystal_axes_rotation": 0.0,
+                    "order_parameter": {"dx2-y2": {"critical_temperature": 1.0},
+                                        "dxy": {"critical_temperature": 1.0}}},
+        "geometry": [{"disc": {"add": True, "radius": 5.0, "center_x": 0.0, "center_y": 0.0}},
+                     {"disc": {"add": False, "radius": 1.5, "center_x": 1.0, "center_y": 0.5}}],
+        "numerics": {"points_per_coherence_length": 4.0, "num_fermi_momenta": 20,
+                     "energy_cutoff": 6.0, "convergence_criterion": 1e-6, "norm": "l1",
+                     "vector_potential_error": 1e-6},
+        "accelerator": {"name": "congacc"},
+    }
+
+
+def with_accelerator(cfg: dict, name: str) -> dict:
+    c = copy.deepcopy(cfg)
+    c["accelerator"] = {"name": name}
+    return c
+
+
+def seeded_state(n_comp: int, n0: int, delta_bulk: float, seed: int, noise: float = 0.01,
+                 complex_noise: bool = False, a_scale: float = 0.0):
+    """Delta = delta_bulk * (1 + noise N(0,1)) per component (the complex
+    variant adds i * noise N(0,1)), A = a_scale * N(0,1); planar layouts."""
+    rng = np.random.default_rng(seed)
+    d = np.zeros((n_comp, 2, n0, n0))
+    for c in range(n_comp):
+        d[c, 0] = delta_bulk * (1.0 + noise * rng.standard_normal((n0, n0)))
+        if complex_noise:
+            d[c, 1] = delta_bulk * noise * rng.standard_normal((n0, n0))
+    a = a_scale * rng.standard_normal((2, n0, n0))
+    return d, a

@@ -1,0 +1,171 @@
+"""GPU parity: the CUDA engine (through the C ABI) against the CPU oracle.
+
+FP64 results must agree with the oracle to 1e-10 relative (relative to the
+largest magnitude of the compared field); the mixed-precision form must stay
+within 1e-5 of the FP64 form relative to the bulk gap.
+"""
+import numpy as np
+import pytest
+
+from tests import configs
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10
+
+
+def _rel(a, b):
+    scale = max(np.max(np.abs(b)), 1e-300)
+    return float(np.max(np.abs(np.asarray(a) - np.asarray(b))) / scale)
+
+
+def _pair(cfg, seed=1, noise=0.01, complex_noise=False, a_scale=0.0, mode="fp64"):
+    from oracle import oracle as O
+    import superconga_b200 as sb
+
+    o = O.Oracle(cfg)
+    e = sb.Context(cfg, mode=mode)
+    s = o.setup
+    db = O.delta_bulk(s.temperature, s.symmetries[0])
+    d, a = configs.seeded_state(s.n_comp, s.n0, db, seed, noise, complex_noise, a_scale)
+    o.set_state(d, a)
+    e.set_state(d, a)
+    return o, e, db
+
+
+CASES = {
+    "golden_disc": (configs.golden_disc(), dict(a_scale=0.0)),
+    "small_disc": (configs.small_disc(), dict(a_scale=0.05)),
+    "small_square_d": (configs.small_square_d(), dict(complex_noise=True, noise=0.1, a_scale=0.05)),
+    "chiral_annulus": (configs.chiral_annulus(), dict(complex_noise=True, noise=0.1, a_scale=0.02)),
+}
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_dims_and_geometry(engine_lib, case):
+    cfg, kw = CASES[case]
+    o, e, _ = _pair(cfg, **kw)
+    assert (e.dims.n0, e.dims.n1, e.dims.n_energies) == (o.n0, o.n1, o.setup.n_energies)
+    assert np.array_equal(e.domain(), o.domain())
+    assert e.boundary_sizes() == o.boundary_sizes()
+    x0, x1, y0, y1 = o.ranges()
+    for a in range(o.setup.n_angles):
+        lab, box = e.frame_labels(a)
+        assert np.array_equal(lab, o.geometry(a)[0])
+        assert box == (x0[a], x1[a], y0[a], y1[a])
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_boundary_initial(engine_lib, case):
+    cfg, kw = CASES[case]
+    o, e, _ = _pair(cfg, **kw)
+    o.set_boundary_initial()
+    e.boundary_initial()
+    for which in range(4):
+        assert _rel(e.boundary(which), o.boundary(which)) < TOL, which
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_angle_sweep(engine_lib, case):
+    """Frame Green sums and out-going boundary values of single angles."""
+    cfg, kw = CASES[case]
+    o, e, _ = _pair(cfg, **kw)
+    o.set_boundary_initial()
+    e.boundary_initial()
+    na = o.setup.n_angles
+    for a in sorted({0, 1, na // 3, na // 2, na - 1}):
+        f_o, g_o, i_o, _ = o.angle_greens(a)
+        f_e, g_e, i_e = e.angle_greens(a)
+        assert _rel(f_e, f_o) < TOL, (a, "F")
+        assert _rel(g_e, g_o) < TOL, (a, "G")
+        assert _rel(i_e, i_o) < TOL, (a, "I")
+    for which in (1, 3):
+        assert _rel(e.boundary(which), o.boundary(which)) < TOL, which
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_iterations(engine_lib, case):
+    """Three full Context::compute iterations (the second and third include the
+    accelerator step): g(x), x, free energy and residuals."""
+    cfg, kw = CASES[case]
+    o, e, _ = _pair(cfg, **kw)
+    for it in range(3):
+        o.compute()
+        e.compute(1)
+        d_o, j_o, a_o = o.results()
+        d_e, j_e, a_e = e.results()
+        assert _rel(d_e, d_o) < TOL, (it, "delta")
+        assert _rel(j_e, j_o) < TOL, (it, "current")
+        if o.setup.params.penetration_depth > 0:
+            assert _rel(a_e, a_o) < TOL, (it, "vector potential")
+        x_o, ax_o = o.state()
+        x_e, ax_e = e.state()
+        assert _rel(x_e, x_o) < TOL, (it, "x")
+        so, se = o.scalars(), e.scalars()
+        for k in ("free_energy", "free_energy_per_area", "magnetic_free_energy"):
+            assert abs(se[k] - so[k]) <= TOL * max(abs(so[k]), 1e-12), (it, k)
+        for k in ("res_order_parameter", "res_current", "res_free_energy", "res_boundary",
+                  "res_vector_potential", "residual"):
+            assert abs(se[k] - so[k]) <= 1e-8 * max(abs(so[k]), 1e-12), (it, k, se[k], so[k])
+        for which in range(4):
+            assert _rel(e.boundary(which), o.boundary(which)) < TOL, (it, which)
+
+
+def test_burn_in(engine_lib):
+    cfg, kw = CASES["small_disc"]
+    o, e, _ = _pair(cfg, **kw)
+    for _ in range(2):
+        o.burn_in()
+        r_e, _ = e.burn_in(1)
+    assert abs(r_e - o.scalars()["res_boundary"]) <= 1e-8 * o.scalars()["res_boundary"]
+    for which in range(4):
+        assert _rel(e.boundary(which), o.boundary(which)) < TOL
+
+
+def test_poisson(engine_lib):
+    cfg, _ = CASES["small_square_d"]
+    from oracle import oracle as O
+    import superconga_b200 as sb
+    o = O.Oracle(cfg)
+    e = sb.Context(cfg)
+    rng = np.random.default_rng(7)
+    j = rng.standard_normal((2, o.n0, o.n0)) * (o.domain() > 0)
+    assert _rel(e.poisson(j), o.poisson(j)) < 1e-10
+
+
+@pytest.mark.parametrize("acc", ["congacc", "picard", "polyak", "barzilai-borwein"])
+def test_golden_free_energy(engine_lib, acc):
+    """tests/accelerators_test.cu:45-149 on the engine: converged within 100
+    iterations to Omega/area = -0.0185386592 within 1e-3 relative."""
+    from oracle import oracle as O
+    import superconga_b200 as sb
+    cfg = configs.golden_disc(acc)
+    e = sb.Context(cfg)
+    n0, nc = e.dims.n0, e.dims.n_comp
+    d = np.zeros((nc, 2, n0, n0))
+    d[0, 0] = O.delta_bulk(0.5, "s")
+    e.set_state(d, np.zeros((2, n0, n0)))
+    it, conv = e.run(0, 100)
+    fe = e.scalars()["free_energy_per_area"]
+    assert conv
+    assert abs(fe - configs.GOLDEN_FREE_ENERGY_PER_AREA) <= 1e-3 * abs(configs.GOLDEN_FREE_ENERGY_PER_AREA)
+
+
+def test_mixed_precision(engine_lib):
+    """FP32 stepping with FP64 accumulation against the FP64 form after five
+    iterations: |Delta - Delta_FP64| / Delta_bulk <= 1e-5."""
+    import superconga_b200 as sb
+    from oracle import oracle as O
+    cfg = configs.small_square_d()
+    e64 = sb.Context(cfg, mode="fp64")
+    e32 = sb.Context(cfg, mode="mixed")
+    s = O.make_setup(cfg)
+    db = O.delta_bulk(s.temperature, s.symmetries[0])
+    d, a = configs.seeded_state(s.n_comp, s.n0, db, 3, 0.1, True, 0.05)
+    for e in (e64, e32):
+        e.set_state(d, a)
+        e.compute(5)
+    d64, j64, a64 = e64.results()
+    d32, j32, a32 = e32.results()
+    assert np.max(np.abs(d32 - d64)) / db <= 1e-5
+    assert _rel(j32, j64) <= 1e-4
