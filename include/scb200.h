@@ -131,6 +131,18 @@ int sc_angle_greens(sc_ctx *ctx, int angle, double *f, double *g_re, double *i_r
  * internal units. */
 int sc_poisson(sc_ctx *ctx, const double *j, double *a_out);
 
+/* Measures the FP64 (precision 64) or FP32 (precision 32) FMA throughput of
+ * the current device in FLOP/s: the CUDA-core denominator of the sweep's
+ * compute roofline (the reference has no counterpart; a measurement aid). */
+int sc_measure_fma_peak(int precision, double *flops_per_second);
+
+/* Per-kernel CUDA-event timing on the context's stream.  kernel: 0 Riccati
+ * sweep, 1 rotation back to the reference grid, 2 Poisson filters, 3 boundary
+ * condition.  sc_profile_read returns the summed device time and number of
+ * timed launches since the last read, and resets them. */
+int sc_profile(sc_ctx *ctx, int enable);
+int sc_profile_read(sc_ctx *ctx, int kernel, double *total_ms, long long *launches);
+
 /* Number of this library's kernel launches issued by ctx so far. */
 int sc_launch_count(const sc_ctx *ctx, long long *count);
 

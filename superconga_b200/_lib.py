@@ -39,6 +39,10 @@ SIGNATURES = {
     "sc_angle_greens": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _c_double_p, _c_double_p, _c_double_p]),
     "sc_poisson": (ctypes.c_int, [ctypes.c_void_p, _c_double_p, _c_double_p]),
     "sc_launch_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]),
+    "sc_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "sc_profile_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                       ctypes.POINTER(ctypes.c_longlong)]),
+    "sc_measure_fma_peak": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "sc_setup_create": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p)]),
     "sc_setup_last_error": (ctypes.c_char_p, []),
     "sc_setup_destroy": (ctypes.c_int, [ctypes.c_void_p]),

@@ -924,6 +924,22 @@ __global__ void k_from_interleaved(size_t n, const double *__restrict__ in, Cx<R
   out[i] = Cx<R>{(R)in[2 * i], (R)in[2 * i + 1]};
 }
 
+// FMA throughput probe: 8 independent FMA chains per thread, many warps.
+template <typename T>
+__global__ void __launch_bounds__(256) k_fma_peak(int iters, T a, T b, T *out) {
+  T v[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) v[k] = (T)(threadIdx.x + k);
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = fma(v[k], a, b);
+  }
+  T s = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += v[k];
+  if (s == (T)12345.678) out[0] = s;  // keeps the chains alive
+}
+
 // --------------------------------------------------------------- helpers --
 template <typename T>
 struct DevArray {
@@ -1004,6 +1020,11 @@ struct sc_ctx {
   bool boundary_initialized = false, first_compute = true;
   Scalars host_scalars{};
 
+  // Optional CUDA-event timing of individual kernels (0 sweep, 1 rotate back,
+  // 2 Poisson, 3 boundary condition), recorded on the launching stream.
+  bool profiling = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof[4];
+
   size_t nn0() const { return (size_t)S.n0 * S.n0; }
   size_t esize() const { return mode == SC_MODE_FP64 ? sizeof(Cx<double>) : sizeof(Cx<float>); }
   void *bnd_ptr(int which) const { return (char *)bnd.p + bnd_off[which]; }
@@ -1015,6 +1036,23 @@ struct sc_ctx {
 };
 
 namespace {
+
+struct ProfScope {
+  sc_ctx *c;
+  int k;
+  cudaEvent_t e1 = nullptr;
+  ProfScope(sc_ctx *ctx, int kernel) : c(ctx), k(kernel) {
+    if (!c->profiling) return;
+    cudaEvent_t e0;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, c->stream);
+    c->prof[k].push_back({e0, e1});
+  }
+  ~ProfScope() {
+    if (e1) cudaEventRecord(e1, c->stream);
+  }
+};
 
 void check_launch(sc_ctx *c) {
   c->launches++;
@@ -1078,6 +1116,7 @@ void launch_sweep(sc_ctx *c, const Chunk &ch, int burn_in) {
   const size_t threads = (size_t)A.n_items * c->groups;
   if (!threads) return;
   const unsigned blocks = grid1(threads, 128);
+  ProfScope prof(c, 0);
   if (c->ept <= 4) k_sweep<R, 4><<<blocks, 128, 0, c->stream>>>(A);
   else if (c->ept <= 8) k_sweep<R, 8><<<blocks, 128, 0, c->stream>>>(A);
   else k_sweep<R, 16><<<blocks, 128, 0, c->stream>>>(A);
@@ -1100,6 +1139,7 @@ void extend_reference(sc_ctx *c) {
 template <typename R>
 void boundary_condition(sc_ctx *c) {
   const HostSetup &S = c->S;
+  ProfScope prof(c, 3);
   k_boundary<R><<<c->nb_bnd, REDUCE_THREADS, 0, c->stream>>>(
       S.n_in_g, S.ne, c->bc_src_g.p, c->bc_w_g.p, c->bc_ws_g.p, (const Cx<R> *)c->bnd_ptr(1),
       (Cx<R> *)c->bnd_ptr(0), c->partial_bg.p);
@@ -1154,6 +1194,7 @@ void poisson(sc_ctx *c, const double *j, double *a_out, int mean_from_scalars) {
   }
   dim3 blk(PT, 8);
   dim3 grid((n + PT - 1) / PT, (n + PT - 1) / PT, 2 * nk);
+  ProfScope prof(c, 2);
   k_toeplitz<<<grid, blk, 0, c->stream>>>(n, nk, c->filters.p, c->pois_s.p, 0, c->pois_t0.p);
   check_launch(c);
   k_toeplitz<<<grid, blk, 0, c->stream>>>(n, nk, c->filters.p, c->pois_t0.p, nn2, c->pois_t1.p);
@@ -1208,6 +1249,7 @@ void run_chunks(sc_ctx *c, int burn_in) {
       check_launch(c);
     }
     dim3 blk(32, 8), grid((S.n0 + 31) / 32, (S.n0 + 7) / 8);
+    ProfScope prof(c, 1);
     k_rotate_back<<<grid, blk, 0, c->stream>>>(S.n0, S.n1, S.nc, ch.a_begin, ch.a_end, c->ang.p,
                                                (const double2 *)c->fg.p, (const double2 *)c->gi.p,
                                                c->acc_d.p, c->acc_j.p, c->acc_fe.p);
@@ -1819,6 +1861,62 @@ int sc_poisson(sc_ctx *ctx, const double *j, double *a_out) {
   poisson(ctx, ctx->tmp_io.p, out, 0);
   CUDA_TRY(cudaMemcpyAsync(a_out, out, nn2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  API_END
+}
+
+int sc_measure_fma_peak(int precision, double *flops_per_second) {
+  sc_ctx *ctx = nullptr;
+  if (!flops_per_second || (precision != 32 && precision != 64)) return SC_ERR_ARG;
+  API_BEGIN
+  int dev = 0, sms = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  void *out = nullptr;
+  CUDA_TRY(cudaMalloc(&out, 16));
+  cudaEvent_t e0, e1;
+  CUDA_TRY(cudaEventCreate(&e0));
+  CUDA_TRY(cudaEventCreate(&e1));
+  const int blocks = sms * 8, iters = 4096;
+  float best = 1e30f;
+  for (int rep = 0; rep < 4; ++rep) {
+    CUDA_TRY(cudaEventRecord(e0));
+    if (precision == 64) k_fma_peak<double><<<blocks, 256>>>(iters, 0.999999, 1e-7, (double *)out);
+    else k_fma_peak<float><<<blocks, 256>>>(iters, 0.999999f, 1e-7f, (float *)out);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaEventRecord(e1));
+    CUDA_TRY(cudaEventSynchronize(e1));
+    float ms = 0;
+    CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+    if (rep > 0) best = std::min(best, ms);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  *flops_per_second = 2.0 * 8.0 * (double)iters * blocks * 256.0 / (best * 1e-3);
+  API_END
+}
+
+int sc_profile(sc_ctx *ctx, int enable) {
+  if (!ctx) return SC_ERR_ARG;
+  ctx->profiling = enable != 0;
+  return SC_OK;
+}
+
+int sc_profile_read(sc_ctx *ctx, int kernel, double *total_ms, long long *launches) {
+  if (!ctx || kernel < 0 || kernel > 3) return SC_ERR_ARG;
+  API_BEGIN
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  double t = 0.0;
+  for (auto &pr : ctx->prof[kernel]) {
+    float ms = 0.0f;
+    CUDA_TRY(cudaEventElapsedTime(&ms, pr.first, pr.second));
+    t += ms;
+    cudaEventDestroy(pr.first);
+    cudaEventDestroy(pr.second);
+  }
+  if (total_ms) *total_ms = t;
+  if (launches) *launches = (long long)ctx->prof[kernel].size();
+  ctx->prof[kernel].clear();
   API_END
 }
 

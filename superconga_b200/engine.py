@@ -152,6 +152,18 @@ class Context:
         self._check(_lib.load().sc_launch_count(self._h, ctypes.byref(v)))
         return v.value
 
+    def profile(self, enable: bool = True):
+        """Enables CUDA-event timing of the sweep (0), rotate-back (1), Poisson
+        (2) and boundary (3) kernels."""
+        self._check(_lib.load().sc_profile(self._h, 1 if enable else 0))
+
+    def profile_read(self, kernel: int):
+        """(summed device ms, launches) of one kernel since the last read."""
+        ms = ctypes.c_double()
+        n = ctypes.c_longlong()
+        self._check(_lib.load().sc_profile_read(self._h, kernel, ctypes.byref(ms), ctypes.byref(n)))
+        return ms.value, n.value
+
     # ---------------------------------------------------------- probes -----
     def frame_labels(self, angle: int):
         n1 = self.dims.n1
@@ -196,6 +208,13 @@ class Context:
         out = np.zeros(self._shape_vec())
         self._check(_lib.load().sc_poisson(self._h, _p(jj), _p(out)))
         return out
+
+
+def fma_peak(precision: int = 64) -> float:
+    """Measured FMA throughput of the current device in FLOP/s."""
+    v = ctypes.c_double()
+    _lib.check(_lib.load().sc_measure_fma_peak(int(precision), ctypes.byref(v)))
+    return v.value
 
 
 class Setup:

@@ -1,0 +1,165 @@
+"""The benchmark workloads: seeded synthetic grains in the reference's JSON
+schema, with their initial order parameter and vector potential.
+
+No public dataset is involved: every input is generated here from a fixed
+seed.  The configurations follow the five benchmark cases (C1-C5): the
+energy cutoff is given in the reference's units of 2 pi k_B T_c
+(``energy_cutoff = 8`` is the 16 pi T_c Matsubara cutoff), and a field of b B0
+is ``external_flux_quanta = b * area / pi`` with the area counted from the
+grain's lattice sites (RiccatiSolver.h:137-139).
+"""
+from __future__ import annotations
+
+import json
+import math
+
+import numpy as np
+
+EULER_MASCHERONI = 0.57721566490153286060651209008240243
+S_WAVE_BULK = 0.5 * math.exp(-EULER_MASCHERONI)
+D_WAVE_BULK = math.exp(-EULER_MASCHERONI - 0.5) / math.sqrt(2.0)
+
+
+def bulk_s_wave(t: float) -> float:
+    """Bulk s-wave gap at temperature t (units of 2 pi k_B T_c), the secant
+    iteration of computeOrderParameterBulkSWave (OrderParameterBulk.h:88-221)."""
+    eps = np.finfo(np.float64).eps
+    if t >= 1.0:
+        return 0.0
+    if t < eps:
+        return S_WAVE_BULK
+    ne = int(100.0 / t - 0.5) + 1
+    n = np.arange(ne - 1, -1, -1, dtype=np.float64)
+    en = t * (n + 0.5)
+    coupling = 1.0 / (math.log(t) / t + float(np.sum(1.0 / en)))
+
+    def resid(op):
+        return op * (float(np.sum(1.0 / np.hypot(op, en))) * coupling - 1.0)
+
+    op = S_WAVE_BULK * math.sqrt(1.0 - t ** 3)
+    ops = [op, math.sqrt(op)]
+    res = [resid(ops[0]), resid(ops[1])]
+    for _ in range(10):
+        w = 1.0 / (1.0 - (ops[0] / ops[1]) / (res[0] / res[1]))
+        op = (1.0 - w) * ops[0] + w * ops[1]
+        r = resid(op)
+        if abs(r / op) < 10 * eps:
+            break
+        k = 0 if abs(res[0]) > abs(res[1]) else 1
+        ops[k], res[k] = op, r
+    return op
+
+
+def delta_bulk(t: float, symmetry: str) -> float:
+    s = bulk_s_wave(t)
+    return s * (D_WAVE_BULK / S_WAVE_BULK) if symmetry in ("dx2-y2", "dxy", "g") else s
+
+
+def _base(temperature, ppxi, n_angles, lam, flux, norm="l2"):
+    return {
+        "physics": {"temperature": temperature, "external_flux_quanta": flux,
+                    "penetration_depth": lam, "charge_sign": -1, "gauge": "symmetric",
+                    "crystal_axes_rotation": 0.0, "order_parameter": {}},
+        "geometry": [],
+        "numerics": {"points_per_coherence_length": ppxi, "num_fermi_momenta": n_angles,
+                     "energy_cutoff": 8.0, "convergence_criterion": 1e-6, "norm": norm,
+                     "vector_potential_error": 1e-6, "num_iterations_burnin": 0,
+                     "num_iterations_min": 0, "num_iterations_max": 100},
+        "accelerator": {"name": "congacc"},
+        "misc": {"verbose": False, "save_path": "", "load_path": ""},
+    }
+
+
+def _flux_for_field(cfg: dict, b: float) -> float:
+    """external_flux_quanta giving a uniform field of b B0 on this grain."""
+    from .engine import Setup
+    s = Setup(cfg)
+    h = 1.0 / cfg["numerics"]["points_per_coherence_length"]
+    n_grain = int(np.count_nonzero(s.domain()))
+    return b * (n_grain * h * h) / math.pi
+
+
+def c1() -> dict:
+    """s-wave disc R = 10 xi0 at 10 points/xi0, 64 angles, T = 0.5, b = 0.02, kappa = 2."""
+    cfg = _base(0.5, 10.0, 64, 2.0, 0.0)
+    cfg["geometry"] = [{"disc": {"add": True, "radius": 10.0, "center_x": 0.0, "center_y": 0.0}}]
+    cfg["physics"]["order_parameter"] = {"s": {"critical_temperature": 1.0}}
+    cfg["physics"]["external_flux_quanta"] = _flux_for_field(cfg, 0.02)
+    return cfg
+
+
+def c2() -> dict:
+    """d_{x2-y2} square of side 30 xi0, crystal axes at 45 degrees, 20 points/xi0,
+    256 angles, T = 0.1 (14 Ozaki poles), no external field, kappa = 2."""
+    cfg = _base(0.1, 20.0, 256, 2.0, 0.0)
+    cfg["geometry"] = [{"regular_polygon": {"add": True, "num_edges": 4, "side_length": 30.0,
+                                            "rotation": 0.0, "center_x": 0.0, "center_y": 0.0}}]
+    cfg["physics"]["crystal_axes_rotation"] = 0.125
+    cfg["physics"]["order_parameter"] = {"dx2-y2": {"critical_temperature": 1.0}}
+    return cfg
+
+
+def c2p() -> dict:
+    """The c2 grain with 32 of its 256 angles: a small case of the same kernels
+    for detailed profiler captures."""
+    cfg = c2()
+    cfg["numerics"]["num_fermi_momenta"] = 32
+    return cfg
+
+
+def c4() -> dict:
+    """Chiral d + i d_xy disc R = 15 xi0 at 15 points/xi0, 128 angles, T = 0.3, b = 0.05, kappa = 2."""
+    cfg = _base(0.3, 15.0, 128, 2.0, 0.0)
+    cfg["geometry"] = [{"disc": {"add": True, "radius": 15.0, "center_x": 0.0, "center_y": 0.0}}]
+    cfg["physics"]["order_parameter"] = {"dx2-y2": {"critical_temperature": 1.0},
+                                         "dxy": {"critical_temperature": 1.0,
+                                                 "initial_phase_shift": 0.25}}
+    cfg["physics"]["external_flux_quanta"] = _flux_for_field(cfg, 0.05)
+    return cfg
+
+
+def c5() -> dict:
+    """s-wave square of side 100 xi0 at 16 points/xi0, 128 angles, T = 0.5, b = 0.3, kappa = 5."""
+    cfg = _base(0.5, 16.0, 128, 5.0, 0.0)
+    cfg["geometry"] = [{"regular_polygon": {"add": True, "num_edges": 4, "side_length": 100.0,
+                                            "rotation": 0.0, "center_x": 0.0, "center_y": 0.0}}]
+    cfg["physics"]["order_parameter"] = {"s": {"critical_temperature": 1.0}}
+    cfg["physics"]["external_flux_quanta"] = _flux_for_field(cfg, 0.3)
+    return cfg
+
+
+WORKLOADS = {"c1": c1, "c2": c2, "c2p": c2p, "c4": c4, "c5": c5}
+SEEDS = {"c1": 1, "c2": 2, "c2p": 2, "c4": 4, "c5": 5}
+
+
+def initial_state(name: str, cfg: dict, n0: int):
+    """Seeded initial order parameter [Nc][2][N0][N0] and vector potential
+    [2][N0][N0] (internal units)."""
+    rng = np.random.default_rng(SEEDS[name])
+    t = cfg["physics"]["temperature"]
+    comps = [s for s in ("dx2-y2", "dxy", "g", "s") if s in cfg["physics"]["order_parameter"]]
+    d = np.zeros((len(comps), 2, n0, n0))
+    for c, sym in enumerate(comps):
+        db = delta_bulk(t, sym)
+        if name == "c1":
+            d[c, 0] = db * (1.0 + 0.01 * rng.standard_normal((n0, n0)))
+        elif name == "c5":
+            # nine 2 pi phase windings at seeded interior positions
+            amp = np.full((n0, n0), db, dtype=np.complex128)
+            yy, xx = np.mgrid[0:n0, 0:n0].astype(np.float64)
+            lo, hi = 0.2 * n0, 0.8 * n0
+            for _ in range(9):
+                cx, cy = rng.uniform(lo, hi, size=2)
+                amp *= np.exp(1j * np.arctan2(yy - cy, xx - cx))
+            d[c, 0], d[c, 1] = amp.real, amp.imag
+        else:
+            phase = 2.0 * math.pi * cfg["physics"]["order_parameter"][sym].get("initial_phase_shift", 0.0)
+            z = db * (1.0 + 0.1 * (rng.standard_normal((n0, n0)) + 1j * rng.standard_normal((n0, n0))))
+            z = z * np.exp(1j * phase)
+            d[c, 0], d[c, 1] = z.real, z.imag
+    a = np.zeros((2, n0, n0))
+    return d, a
+
+
+def config_json(name: str) -> str:
+    return json.dumps(WORKLOADS[name]())

@@ -1,0 +1,146 @@
+"""The CPU oracle against the reference's own known answers (CPU only).
+
+Each case restates a check from the reference's test suite; the citations are
+paths inside the reference project.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from tests import configs
+
+
+@pytest.fixture(scope="module")
+def O():
+    from oracle import oracle
+    oracle.build()
+    return oracle
+
+
+def test_num_ozaki_poles(O):
+    # tests/parameters_test.cu:45-58: T = 0.5, cutoff 10/(2 pi) -> 3 poles.
+    assert O.num_ozaki_poles(0.5, 10.0 / (2.0 * math.pi)) == 3
+    # The benchmark cutoff 16 pi T_c (energy_cutoff 8) at T = 0.5/0.1/0.3.
+    assert [O.num_ozaki_poles(t, 8.0) for t in (0.5, 0.1, 0.3)] == [7, 14, 8]
+
+
+def test_grid_resolution(O):
+    # tests/parameters_test.cu:9-43.
+    for width in (1.0, 6.53, 25.6, 50.111):
+        for ppxi in (1.05, 3.9, 10.0, 17.8):
+            n0, n1, _ = O.lattice(width, ppxi)
+            tmp = int(math.ceil(math.sqrt(2.0) * n0))
+            assert n1 == (tmp if (tmp - n0) % 2 == 0 else tmp + 1)
+
+
+def test_homogeneous_solution(O):
+    # tests/riccati_solutions_test.cu:21-45: Delta = 4, energy = 3i -> gamma = i/2.
+    g, gt = O.homogeneous(4 + 0j, 3j)
+    assert abs(g - 0.5j) < 1e-12 and abs(gt - (-0.5j)) < 1e-12
+
+
+def test_step_keeps_homogeneous(O):
+    # tests/riccati_solutions_test.cu:47-80: a step from the homogeneous
+    # solution stays there, for gamma and gammaTilde.
+    d, e = 1 + 0.5j, 0.5 + 1j
+    g, gt = O.homogeneous(d, e)
+    assert abs(O.riccati_step(d, e, g, 1.0) - g) < 1e-12
+    assert abs(O.riccati_step(-d.conjugate(), e, gt, 1.0) - gt) < 1e-12
+
+
+def test_step_zero_length(O):
+    # tests/riccati_solutions_test.cu:82-105: h = 0 leaves the value unchanged.
+    assert abs(O.riccati_step(1 + 0j, 1j, 0.5j, 0.0) - 0.5j) < 1e-15
+    assert abs(O.riccati_step(-1 + 0j, 1j, 0.5j, 0.0) - 0.5j) < 1e-15
+
+
+def test_step_large(O):
+    # tests/riccati_solutions_test.cu:107-140: h -> infinity gives 2 gamma_h - gamma_0 (1%).
+    d, e, g0 = 1 + 0.5j, 0.5 + 1j, 0.5 + 0.5j
+    g, gt = O.homogeneous(d, e)
+    got = O.riccati_step(d, e, g0, 1000.0)
+    want = 2 * g - g0
+    assert abs(got.real - want.real) <= 0.01 * max(abs(want.real), 0.01)
+    assert abs(got.imag - want.imag) <= 0.01 * max(abs(want.imag), 0.01)
+    got_t = O.riccati_step(-d.conjugate(), e, g0, 1000.0)
+    want_t = 2 * gt - g0
+    assert abs(got_t.real - want_t.real) <= 0.01 * max(abs(want_t.real), 0.01)
+    assert abs(got_t.imag - want_t.imag) <= 0.01 * max(abs(want_t.imag), 0.01)
+
+
+def test_green_elements(O):
+    # tests/green_elements_test.cu: with gamma~ = 0, g = -i and f + f~* = -2i gamma.
+    g, f = O.greens(0.3 + 0.2j, 0j)
+    assert abs(g - (-1j)) < 1e-15
+    assert abs(f - (-2j * (0.3 + 0.2j))) < 1e-15
+    # Normalisation g^2 - f f~ = -1 on the homogeneous solution.
+    gam, gamt = O.homogeneous(0.7 + 0.1j, 0.2j)
+    gval, _ = O.greens(gam, gamt)
+    fv = -2j * gam / (1 + gam * gamt)
+    ftv = 2j * gamt / (1 + gam * gamt)
+    assert abs(gval * gval - fv * ftv + 1) < 1e-12
+
+
+def test_bulk_gap(O):
+    # The bulk s-wave gap solves the Matsubara gap equation; near T = 0 it tends
+    # to the zero-temperature value 0.5 exp(-gamma_E) (defines.h:41).
+    assert abs(O.bulk_s_wave(1e-20) - O.S_WAVE_BULK) < 1e-15
+    d = O.bulk_s_wave(0.5)
+    assert 0 < d < O.S_WAVE_BULK
+    assert O.bulk_s_wave(1.0) == 0.0
+
+
+@pytest.mark.parametrize("acc", ["congacc", "picard", "polyak", "barzilai-borwein", "anderson"])
+def test_golden_free_energy(O, acc):
+    """tests/accelerators_test.cu:45-149: every accelerator converges within 100
+    iterations to Omega/area = -0.0185386592 (1e-3 relative)."""
+    cfg = configs.golden_disc(acc)
+    o = O.Oracle(cfg)
+    s = o.setup
+    d = np.zeros((1, 2, s.n0, s.n0))
+    d[0, 0] = O.delta_bulk(0.5, "s")
+    o.set_state(d, np.zeros((2, s.n0, s.n0)))
+    converged = False
+    for _ in range(100):
+        o.compute()
+        if o.is_converged():
+            converged = True
+            break
+    fe = o.scalars()["free_energy_per_area"]
+    assert converged
+    assert abs(fe - configs.GOLDEN_FREE_ENERGY_PER_AREA) <= 1e-3 * abs(configs.GOLDEN_FREE_ENERGY_PER_AREA)
+    # The restatement reproduces the reference's digits far inside the tolerance.
+    if acc == "congacc":
+        assert abs(fe - configs.GOLDEN_FREE_ENERGY_PER_AREA) <= 1e-6 * abs(configs.GOLDEN_FREE_ENERGY_PER_AREA)
+
+
+def test_current_conservation(O):
+    """tests/physics/current_conservation_test.cu:130-162: the mean current of a
+    uniform s-wave disc vanishes."""
+    cfg = configs.small_disc()
+    cfg["physics"]["external_flux_quanta"] = 0.0
+    o = O.Oracle(cfg)
+    s = o.setup
+    d = np.zeros((1, 2, s.n0, s.n0))
+    d[0, 0] = O.delta_bulk(s.temperature, "s")
+    o.set_state(d, np.zeros((2, s.n0, s.n0)))
+    o.compute()
+    _, j, _ = o.results()
+    dom = o.domain() > 0
+    scale = np.abs(j).max() + 1e-300
+    assert abs(j[0][dom].mean()) <= 1e-10 + 10 * np.finfo(float).eps * scale
+    assert abs(j[1][dom].mean()) <= 1e-10 + 10 * np.finfo(float).eps * scale
+
+
+def test_poisson_linearity(O):
+    """The separable Poisson solve is linear in the current
+    (ComputeVectorPotential.h:575-745)."""
+    cfg = configs.small_square_d()
+    o = O.Oracle(cfg)
+    rng = np.random.default_rng(2)
+    dom = o.domain() > 0
+    j1 = rng.standard_normal((2, o.n0, o.n0)) * dom
+    j2 = rng.standard_normal((2, o.n0, o.n0)) * dom
+    a1, a2, a12 = o.poisson(j1), o.poisson(j2), o.poisson(2.0 * j1 - 3.0 * j2)
+    assert np.max(np.abs(a12 - (2.0 * a1 - 3.0 * a2))) <= 1e-12 * np.max(np.abs(a12))
