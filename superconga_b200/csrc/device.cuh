@@ -32,17 +32,29 @@ __device__ __forceinline__ Cx<R> cmul(Cx<R> a, Cx<R> b) {
   return Cx<R>{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
 }
 
-// Principal square root, branch cut on the negative real axis.
+// Precision-specific primitives: IEEE-rounded reciprocal and accurate
+// reciprocal square root in FP64; the fast MUFU approximations in FP32.
+__device__ __forceinline__ double rcp_(double x) { return __drcp_rn(x); }
+__device__ __forceinline__ float rcp_(float x) { return __fdividef(1.0f, x); }
+__device__ __forceinline__ double rsqrt_(double x) { return rsqrt(x); }
+__device__ __forceinline__ float rsqrt_(float x) { return rsqrtf(x); }
+__device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
+__device__ __forceinline__ float sqrt_(float x) { return x > 0.0f ? x * rsqrtf(x) : 0.0f; }
+
+// Principal square root, branch cut on the negative real axis, through one
+// square root and one reciprocal square root:
+//   u = (|z| + |x|)/2, t = sqrt(u), v = |y| / (2 t);
+//   sqrt(z) = (t, sign(y) v) for x >= 0 and (v, sign(y) t) otherwise.
 template <typename R>
 __device__ __forceinline__ Cx<R> csqrt_dev(R x, R y) {
-  const R m = sqrt(x * x + y * y);
-  if (x >= R(0)) {
-    const R t = sqrt(R(0.5) * (m + x));
-    if (t == R(0)) return Cx<R>{R(0), y};
-    return Cx<R>{t, y / (R(2) * t)};
-  }
-  const R t = sqrt(R(0.5) * (m - x));
-  return Cx<R>{fabs(y) / (R(2) * t), copysign(t, y)};
+  const R m = sqrt_(x * x + y * y);
+  const R u = R(0.5) * (m + fabs(x));
+  if (!(u > R(0))) return Cx<R>{R(0), y};
+  const R r = rsqrt_(u);
+  const R t = u * r;
+  const R v = R(0.5) * fabs(y) * r;
+  const bool pos = x >= R(0);
+  return Cx<R>{pos ? t : v, copysign(pos ? v : t, y)};
 }
 
 // Midpoint Riccati step, riccati::computeStep (RiccatiSolutions.h:65-94):
@@ -63,7 +75,7 @@ __device__ __forceinline__ Cx<R> riccati_step(R dre, R dim, R ere, R eim, Cx<R> 
   const Cx<R> ac = cmul(a, c);
   const Cx<R> disc = csqrt_dev<R>(bb.re - R(4) * ac.re, bb.im - R(4) * ac.im);
   const R den_re = disc.re - b.re, den_im = disc.im - b.im;
-  const R inv = R(1) / (den_re * den_re + den_im * den_im);
+  const R inv = rcp_(den_re * den_re + den_im * den_im);
   const R c2r = R(2) * c.re, c2i = R(2) * c.im;
   return Cx<R>{(c2r * den_re + c2i * den_im) * inv, (c2i * den_re - c2r * den_im) * inv};
 }
@@ -76,7 +88,7 @@ __device__ __forceinline__ void riccati_homogeneous(R dre, R dim, R ere, R eim, 
   const R e2re = ere * ere - eim * eim, e2im = ere * eim + eim * ere;
   const Cx<R> om = csqrt_dev<R>(nd - e2re, -e2im);
   const R dr = ere - om.im, di = eim + om.re;  // energy + i * Omega
-  const R inv = R(1) / (dr * dr + di * di);
+  const R inv = rcp_(dr * dr + di * di);
   const Cx<R> invd{dr * inv, -di * inv};
   g = cmul(Cx<R>{-dre, -dim}, invd);
   gt = cmul(Cx<R>{dre, -dim}, invd);
@@ -89,7 +101,7 @@ __device__ __forceinline__ void local_greens(Cx<R> g, Cx<R> gt, R dre, R dim, Cx
                                              R &g_re, R &i_im) {
   const Cx<R> p = cmul(g, gt);
   const R den_re = R(1) + p.re, den_im = p.im;
-  const R inv = R(1) / (den_re * den_re + den_im * den_im);
+  const R inv = rcp_(den_re * den_re + den_im * den_im);
   // (1 - p) / (1 + p)
   const R nr = R(1) - p.re, ni = -p.im;
   const R q_im = (ni * den_re - nr * den_im) * inv;

@@ -161,9 +161,67 @@ __device__ __forceinline__ void frame_fields(const SweepArgs<R> &A, const AngleP
   }
 }
 
-template <typename R, int EMAX>
 __device__ __forceinline__ void group_sum(double &v, int groups, unsigned mask) {
   for (int o = groups >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
+}
+
+// Rotated order parameter and Doppler shift of every site of every trajectory
+// column of a chunk, written to scratch2[row][3][item] for the sweep.
+template <typename R>
+__global__ void __launch_bounds__(128) k_frame_fields(const SweepArgs<R> A, int rows_per_thread) {
+  const int item = blockIdx.x * blockDim.x + threadIdx.x;
+  if (item >= A.n_items) return;
+  const int4 it = A.items[item];
+  const int a = it.x, x = it.y, lo = it.z, hi = it.w;
+  const AngleParams P = A.ang[a];
+  const size_t ni = (size_t)A.n_items;
+  const int r0 = blockIdx.y * rows_per_thread;
+  const int r1 = min(r0 + rows_per_thread, hi - lo + 1);
+  for (int r = r0; r < r1; ++r) {
+    double dre, dim, es;
+    frame_fields(A, P, x, lo + r, dre, dim, es);
+    double *s2 = A.scratch2 + (size_t)r * 3 * ni + item;
+    s2[0] = dre;
+    s2[ni] = dim;
+    s2[2 * ni] = es;
+  }
+}
+
+// One step of one coherence function at one site for EMAX interleaved
+// energies (internal::computeStep, RiccatiSolverConfined.h:129-225): entry
+// sites start from the stored boundary value with the partial step dist*h, grain
+// sites take the midpoint step, exit sites also step on to the boundary and
+// store the out-going value, sites outside the grain reset to zero.
+template <typename R, int EMAX>
+__device__ __forceinline__ void site_step(uint8_t l, uint8_t l_entry, uint8_t l_exit, R dre,
+                                          R dim, R es, R pdre, R pdim, R pes, const R *eim,
+                                          Cx<R> *coh, int ept, int ecount, R h, R dist_in,
+                                          const Cx<R> *bin, R dist_out, Cx<R> *bout) {
+  const bool entry = l == l_entry;
+  const R sdre = entry ? dre : (dre + pdre) * R(0.5);
+  const R sdim = entry ? dim : (dim + pdim) * R(0.5);
+  const R ses = entry ? es : (es + pes) * R(0.5);
+  const R st = entry ? dist_in * h : h;
+#pragma unroll
+  for (int j = 0; j < EMAX; ++j)
+    if (j < ept) {
+      Cx<R> g0 = coh[j];
+      if (entry) g0 = (j < ecount) ? bin[j] : Cx<R>{R(0), R(0)};
+      coh[j] = riccati_step<R>(sdre, sdim, ses, eim[j], g0, st);
+    }
+  if (l == l_exit) {
+    const R sb = dist_out * h;
+#pragma unroll
+    for (int j = 0; j < EMAX; ++j)
+      if (j < ept) {
+        const Cx<R> bv = riccati_step<R>(dre, dim, es, eim[j], coh[j], sb);
+        if (j < ecount) bout[j] = bv;
+      }
+  }
+  if (l == 0) {
+#pragma unroll
+    for (int j = 0; j < EMAX; ++j) coh[j] = Cx<R>{R(0), R(0)};
+  }
 }
 
 // The fused Riccati sweep of one chunk of angles.  G = 2^log_groups threads
@@ -171,8 +229,8 @@ __device__ __forceinline__ void group_sum(double &v, int groups, unsigned mask) 
 // [g*ept, g*ept + ept).  gammaTilde runs down the column first and is kept in
 // scratch; gamma then runs up and the Green sums over all energies are formed
 // site by site (RiccatiSolverConfined.h:129-312, GreensFunctionStatic.h:92-157,
-// ComputeFreeEnergy.h:106-160).  Energies and the frame order parameter are
-// computed in FP64; the coherence functions in R.
+// ComputeFreeEnergy.h:106-160).  The frame order parameter and the energies come
+// from scratch2 (FP64); the coherence functions are integrated in R.
 template <typename R, int EMAX>
 __global__ void __launch_bounds__(128) k_sweep(const SweepArgs<R> A) {
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -184,7 +242,6 @@ __global__ void __launch_bounds__(128) k_sweep(const SweepArgs<R> A) {
   if (item >= A.n_items) return;  // whole groups leave together (groups divide the warp)
   const int4 it = A.items[item];
   const int a = it.x, x = it.y, lo = it.z, hi = it.w;
-  const AngleParams P = A.ang[a];
   const int n1 = A.n1, ne = A.ne;
   const size_t nn1 = (size_t)n1 * n1;
   const uint8_t *lab = A.labels + (size_t)a * nn1;
@@ -200,55 +257,39 @@ __global__ void __launch_bounds__(128) k_sweep(const SweepArgs<R> A) {
   for (int j = 0; j < EMAX; ++j) eim[j] = (j < ecount) ? (R)A.e_im[e0 + j] : R(1);
 
   Cx<R> coh[EMAX];
+  const size_t ax = (size_t)a * n1 + x;
+  // The next site's label, fields and stored gammaTilde are loaded one site
+  // ahead so that their latency overlaps the current site's Riccati steps.
   // ------------------------------------------------------ gammaTilde, down --
   {
-    const int ain = (size_t)a * n1 + x;
-    const int in_base = A.idx_in_gt[ain], out_base = A.idx_out_gt[ain];
+    const int in_base = A.idx_in_gt[ax], out_base = A.idx_out_gt[ax];
     int nin = 0, nout = 0;
     R pdre = 0, pdim = 0, pes = 0;
 #pragma unroll
     for (int j = 0; j < EMAX; ++j) coh[j] = Cx<R>{R(0), R(0)};
+    uint8_t l_nx = lab[(size_t)hi * n1 + x];
+    const double *s2 = A.scratch2 + (size_t)(hi - lo) * 3 * ni + item;
+    double f0 = s2[0], f1 = s2[ni], f2 = s2[2 * ni];
     for (int y = hi; y >= lo; --y) {
       const int r = y - lo;
-      const uint8_t l = lab[(size_t)y * n1 + x];
-      double ddre, ddim, des;
-      frame_fields(A, P, x, y, ddre, ddim, des);
-      if (!A.burn_in) {  // every lane of the group writes the same values
-        double *s2 = A.scratch2 + (size_t)r * 3 * ni + item;
-        s2[0] = ddre;
-        s2[ni] = ddim;
-        s2[2 * ni] = des;
-      }
+      const uint8_t l = l_nx;
       // gammaTilde uses -conj(Delta) (RiccatiSolverConfined.h:74-79).
-      const R dre = (R)(-ddre), dim = (R)ddim, es = (R)des;
-      if (l == 1) {
-        const R mre = (dre + pdre) * R(0.5), mim = (dim + pdim) * R(0.5), mes = (es + pes) * R(0.5);
-#pragma unroll
-        for (int j = 0; j < EMAX; ++j)
-          if (j < A.ept) coh[j] = riccati_step<R>(mre, mim, mes, eim[j], coh[j], h);
-      } else if (l == 3) {  // entry of gammaTilde
-        const R st = (R)A.dist_in_gt[in_base + nin] * h;
-        const Cx<R> *bin = A.bin_gt + (size_t)(in_base + nin) * ne + e0;
-#pragma unroll
-        for (int j = 0; j < EMAX; ++j)
-          if (j < A.ept) coh[j] = riccati_step<R>(dre, dim, es, eim[j], j < ecount ? bin[j] : Cx<R>{R(0), R(0)}, st);
-        nin++;
-      } else if (l == 2) {  // exit of gammaTilde
-        const R mre = (dre + pdre) * R(0.5), mim = (dim + pdim) * R(0.5), mes = (es + pes) * R(0.5);
-        const R st = (R)A.dist_out_gt[out_base + nout] * h;
-        Cx<R> *bout = A.bout_gt + (size_t)(out_base + nout) * ne + e0;
-#pragma unroll
-        for (int j = 0; j < EMAX; ++j)
-          if (j < A.ept) {
-            coh[j] = riccati_step<R>(mre, mim, mes, eim[j], coh[j], h);
-            const Cx<R> bv = riccati_step<R>(dre, dim, es, eim[j], coh[j], st);
-            if (j < ecount) bout[j] = bv;
-          }
-        nout++;
-      } else {
-#pragma unroll
-        for (int j = 0; j < EMAX; ++j) coh[j] = Cx<R>{R(0), R(0)};
+      const R dre = (R)(-f0), dim = (R)f1, es = (R)f2;
+      if (y > lo) {
+        l_nx = lab[(size_t)(y - 1) * n1 + x];
+        const double *s2n = A.scratch2 + (size_t)(r - 1) * 3 * ni + item;
+        f0 = s2n[0];
+        f1 = s2n[ni];
+        f2 = s2n[2 * ni];
       }
+      const bool entry = l == 3, exit = l == 2;
+      const R din = entry ? (R)A.dist_in_gt[in_base + nin] : R(0);
+      const R dout = exit ? (R)A.dist_out_gt[out_base + nout] : R(0);
+      site_step<R, EMAX>(l, 3, 2, dre, dim, es, pdre, pdim, pes, eim, coh, A.ept, ecount, h, din,
+                         A.bin_gt + (size_t)(in_base + nin) * ne + e0, dout,
+                         A.bout_gt + (size_t)(out_base + nout) * ne + e0);
+      nin += entry;
+      nout += exit;
       if (!A.burn_in) {
         Cx<R> *sc = A.scratch + (size_t)r * ne * ni + (size_t)e0 * ni + item;
 #pragma unroll
@@ -262,69 +303,62 @@ __global__ void __launch_bounds__(128) k_sweep(const SweepArgs<R> A) {
   }
   // ----------------------------------------------------------- gamma, up --
   {
-    const int ain = (size_t)a * n1 + x;
-    const int in_base = A.idx_in_g[ain], out_base = A.idx_out_g[ain];
+    const int in_base = A.idx_in_g[ax], out_base = A.idx_out_g[ax];
     int nin = 0, nout = 0;
     R pdre = 0, pdim = 0, pes = 0;
 #pragma unroll
     for (int j = 0; j < EMAX; ++j) coh[j] = Cx<R>{R(0), R(0)};
     double2 *fg = A.fg + (size_t)(a - A.slot_base) * nn1;
     double2 *gi = A.gi + (size_t)(a - A.slot_base) * nn1;
+    uint8_t l_nx = lab[(size_t)lo * n1 + x];
+    double f0 = A.scratch2[item], f1 = A.scratch2[ni + item], f2 = A.scratch2[2 * ni + item];
+    Cx<R> gt_nx[EMAX];
+    if (!A.burn_in) {
+      const Cx<R> *sc = A.scratch + (size_t)e0 * ni + item;
+#pragma unroll
+      for (int j = 0; j < EMAX; ++j)
+        if (j < ecount) gt_nx[j] = sc[(size_t)j * ni];
+    }
     for (int y = lo; y <= hi; ++y) {
       const int r = y - lo;
-      const uint8_t l = lab[(size_t)y * n1 + x];
-      double ddre, ddim, des;
-      if (A.burn_in) {
-        frame_fields(A, P, x, y, ddre, ddim, des);
-      } else {
-        const double *s2 = A.scratch2 + (size_t)r * 3 * ni + item;
-        ddre = s2[0];
-        ddim = s2[ni];
-        des = s2[2 * ni];
+      const uint8_t l = l_nx;
+      const R dre = (R)f0, dim = (R)f1, es = (R)f2;
+      Cx<R> gt[EMAX];
+#pragma unroll
+      for (int j = 0; j < EMAX; ++j) gt[j] = gt_nx[j];
+      if (y < hi) {
+        l_nx = lab[(size_t)(y + 1) * n1 + x];
+        const double *s2n = A.scratch2 + (size_t)(r + 1) * 3 * ni + item;
+        f0 = s2n[0];
+        f1 = s2n[ni];
+        f2 = s2n[2 * ni];
+        if (!A.burn_in) {
+          const Cx<R> *sc = A.scratch + (size_t)(r + 1) * ne * ni + (size_t)e0 * ni + item;
+#pragma unroll
+          for (int j = 0; j < EMAX; ++j)
+            if (j < ecount) gt_nx[j] = sc[(size_t)j * ni];
+        }
       }
-      const R dre = (R)ddre, dim = (R)ddim, es = (R)des;
-      if (l == 1) {
-        const R mre = (dre + pdre) * R(0.5), mim = (dim + pdim) * R(0.5), mes = (es + pes) * R(0.5);
-#pragma unroll
-        for (int j = 0; j < EMAX; ++j)
-          if (j < A.ept) coh[j] = riccati_step<R>(mre, mim, mes, eim[j], coh[j], h);
-      } else if (l == 2) {  // entry of gamma
-        const R st = (R)A.dist_in_g[in_base + nin] * h;
-        const Cx<R> *bin = A.bin_g + (size_t)(in_base + nin) * ne + e0;
-#pragma unroll
-        for (int j = 0; j < EMAX; ++j)
-          if (j < A.ept) coh[j] = riccati_step<R>(dre, dim, es, eim[j], j < ecount ? bin[j] : Cx<R>{R(0), R(0)}, st);
-        nin++;
-      } else if (l == 3) {  // exit of gamma
-        const R mre = (dre + pdre) * R(0.5), mim = (dim + pdim) * R(0.5), mes = (es + pes) * R(0.5);
-        const R st = (R)A.dist_out_g[out_base + nout] * h;
-        Cx<R> *bout = A.bout_g + (size_t)(out_base + nout) * ne + e0;
-#pragma unroll
-        for (int j = 0; j < EMAX; ++j)
-          if (j < A.ept) {
-            coh[j] = riccati_step<R>(mre, mim, mes, eim[j], coh[j], h);
-            const Cx<R> bv = riccati_step<R>(dre, dim, es, eim[j], coh[j], st);
-            if (j < ecount) bout[j] = bv;
-          }
-        nout++;
-      } else {
-#pragma unroll
-        for (int j = 0; j < EMAX; ++j) coh[j] = Cx<R>{R(0), R(0)};
-      }
+      const bool entry = l == 2, exit = l == 3;
+      const R din = entry ? (R)A.dist_in_g[in_base + nin] : R(0);
+      const R dout = exit ? (R)A.dist_out_g[out_base + nout] : R(0);
+      site_step<R, EMAX>(l, 2, 3, dre, dim, es, pdre, pdim, pes, eim, coh, A.ept, ecount, h, din,
+                         A.bin_g + (size_t)(in_base + nin) * ne + e0, dout,
+                         A.bout_g + (size_t)(out_base + nout) * ne + e0);
+      nin += entry;
+      nout += exit;
       pdre = dre;
       pdim = dim;
       pes = es;
       if (A.burn_in) continue;
       double sfr = 0.0, sfi = 0.0, sg = 0.0, si = 0.0;
       if (l != 0) {
-        const Cx<R> *sc = A.scratch + (size_t)r * ne * ni + (size_t)e0 * ni + item;
 #pragma unroll
         for (int j = 0; j < EMAX; ++j)
           if (j < ecount) {
-            const Cx<R> gt = sc[(size_t)j * ni];
             Cx<R> F;
             R gre, iim;
-            local_greens<R>(coh[j], gt, dre, dim, F, gre, iim);
+            local_greens<R>(coh[j], gt[j], dre, dim, F, gre, iim);
             const double rr = A.res[e0 + j];
             sfr += rr * (double)F.re;
             sfi += rr * (double)F.im;
@@ -333,10 +367,10 @@ __global__ void __launch_bounds__(128) k_sweep(const SweepArgs<R> A) {
           }
       }
       if (A.groups > 1) {
-        group_sum<R, EMAX>(sfr, A.groups, gmask);
-        group_sum<R, EMAX>(sfi, A.groups, gmask);
-        group_sum<R, EMAX>(sg, A.groups, gmask);
-        group_sum<R, EMAX>(si, A.groups, gmask);
+        group_sum(sfr, A.groups, gmask);
+        group_sum(sfi, A.groups, gmask);
+        group_sum(sg, A.groups, gmask);
+        group_sum(si, A.groups, gmask);
       }
       if (g == 0) {
         const size_t fi = (size_t)y * n1 + x;
@@ -1116,6 +1150,12 @@ void launch_sweep(sc_ctx *c, const Chunk &ch, int burn_in) {
   const size_t threads = (size_t)A.n_items * c->groups;
   if (!threads) return;
   const unsigned blocks = grid1(threads, 128);
+  {
+    const int rows = 16;
+    dim3 grid(grid1(A.n_items, 128), (unsigned)((ch.kmax + rows - 1) / rows));
+    k_frame_fields<R><<<grid, 128, 0, c->stream>>>(A, rows);
+    check_launch(c);
+  }
   ProfScope prof(c, 0);
   if (c->ept <= 4) k_sweep<R, 4><<<blocks, 128, 0, c->stream>>>(A);
   else if (c->ept <= 8) k_sweep<R, 8><<<blocks, 128, 0, c->stream>>>(A);
@@ -1459,7 +1499,12 @@ void upload_static(sc_ctx *c) {
   c->groups = 1;
   c->log_groups = 0;
   const char *eg = std::getenv("SCB_ENERGY_GROUPS");
-  int want = eg ? std::atoi(eg) : (S.ne > 16 ? 4 : S.ne > 8 ? 2 : 1);
+  // Default: the fewest threads per column that keep at most four energies per
+  // thread (the fastest split measured on B200 for 7-14 Ozaki energies).
+  int want = 1;
+  if (eg) want = std::atoi(eg);
+  else
+    while ((S.ne + want - 1) / want > 4 && want < 8) want *= 2;
   while (c->groups < want && c->groups < 8) {
     c->groups *= 2;
     c->log_groups++;

@@ -100,10 +100,11 @@ def c2() -> dict:
 
 
 def c2p() -> dict:
-    """The c2 grain with 32 of its 256 angles: a small case of the same kernels
-    for detailed profiler captures."""
+    """The c2 grain at 10 points/xi0 with 64 angles: a small case of the same
+    kernels (about 2 GB of sweep scratch) for detailed profiler captures."""
     cfg = c2()
-    cfg["numerics"]["num_fermi_momenta"] = 32
+    cfg["numerics"]["points_per_coherence_length"] = 10.0
+    cfg["numerics"]["num_fermi_momenta"] = 64
     return cfg
 
 
