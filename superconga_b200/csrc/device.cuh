@@ -34,11 +34,20 @@ __device__ __forceinline__ Cx<R> cmul(Cx<R> a, Cx<R> b) {
 
 // Precision-specific primitives: IEEE-rounded reciprocal and accurate
 // reciprocal square root in FP64; the fast MUFU approximations in FP32.
-__device__ __forceinline__ double rcp_(double x) { return __drcp_rn(x); }
+// FP64 reciprocal: the hardware approximation refined by two Newton steps
+// (relative error near 1 ulp; the arguments here are finite and nonzero).
+__device__ __forceinline__ double rcp_(double x) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+  double e = fma(-x, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-x, r, 1.0);
+  return fma(r, e, r);
+}
 __device__ __forceinline__ float rcp_(float x) { return __fdividef(1.0f, x); }
 __device__ __forceinline__ double rsqrt_(double x) { return rsqrt(x); }
 __device__ __forceinline__ float rsqrt_(float x) { return rsqrtf(x); }
-__device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
+__device__ __forceinline__ double sqrt_(double x) { return x > 0.0 ? x * rsqrt(x) : 0.0; }
 __device__ __forceinline__ float sqrt_(float x) { return x > 0.0f ? x * rsqrtf(x) : 0.0f; }
 
 // Principal square root, branch cut on the negative real axis, through one

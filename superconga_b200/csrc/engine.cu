@@ -231,8 +231,11 @@ __device__ __forceinline__ void site_step(uint8_t l, uint8_t l_entry, uint8_t l_
 // site by site (RiccatiSolverConfined.h:129-312, GreensFunctionStatic.h:92-157,
 // ComputeFreeEnergy.h:106-160).  The frame order parameter and the energies come
 // from scratch2 (FP64); the coherence functions are integrated in R.
-template <typename R, int EMAX>
-__global__ void __launch_bounds__(128) k_sweep(const SweepArgs<R> A) {
+template <typename R, int EMAX, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_sweep(const SweepArgs<R> A) {
+  __shared__ double s_res[64];  // Ozaki residues (at most 64 energies)
+  for (int e = threadIdx.x; e < A.ne && e < 64; e += blockDim.x) s_res[e] = A.res[e];
+  __syncthreads();
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int item = tid >> A.log_groups;
   const int g = tid & (A.groups - 1);
@@ -359,7 +362,7 @@ __global__ void __launch_bounds__(128) k_sweep(const SweepArgs<R> A) {
             Cx<R> F;
             R gre, iim;
             local_greens<R>(coh[j], gt[j], dre, dim, F, gre, iim);
-            const double rr = A.res[e0 + j];
+            const double rr = s_res[e0 + j];
             sfr += rr * (double)F.re;
             sfi += rr * (double)F.im;
             sg += rr * (double)gre;
@@ -1157,9 +1160,15 @@ void launch_sweep(sc_ctx *c, const Chunk &ch, int burn_in) {
     check_launch(c);
   }
   ProfScope prof(c, 0);
-  if (c->ept <= 4) k_sweep<R, 4><<<blocks, 128, 0, c->stream>>>(A);
-  else if (c->ept <= 8) k_sweep<R, 8><<<blocks, 128, 0, c->stream>>>(A);
-  else k_sweep<R, 16><<<blocks, 128, 0, c->stream>>>(A);
+  static const int variant = std::getenv("SCB_SWEEP_MINB") ? std::atoi(std::getenv("SCB_SWEEP_MINB")) : 0;
+  if (c->ept <= 4) {
+    if (variant == 4) k_sweep<R, 4, 4><<<blocks, 128, 0, c->stream>>>(A);
+    else k_sweep<R, 4, 1><<<blocks, 128, 0, c->stream>>>(A);
+  } else if (c->ept <= 8) {
+    k_sweep<R, 8, 1><<<blocks, 128, 0, c->stream>>>(A);
+  } else {
+    k_sweep<R, 16, 1><<<blocks, 128, 0, c->stream>>>(A);
+  }
   check_launch(c);
 }
 
@@ -1609,6 +1618,7 @@ int sc_create(const char *config_json, int mode, sc_ctx **out) {
     const std::string e = build_setup(config_json, c->S);
     if (!e.empty()) throw EngineError(SC_ERR_ARG, e);
     if (c->S.nc > MAX_COMP) throw EngineError(SC_ERR_ARG, "at most 4 order-parameter components");
+    if (c->S.ne > 64) throw EngineError(SC_ERR_ARG, "at most 64 Ozaki energies (raise the temperature or lower the cutoff)");
     if (2 * c->S.nc + 2 > 16) throw EngineError(SC_ERR_ARG, "too many accelerator fields");
     if (c->S.acc.kind == ACC_ANDERSON)
       throw EngineError(SC_ERR_ARG, "accelerator 'anderson' is not available in this engine");

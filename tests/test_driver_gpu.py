@@ -1,0 +1,68 @@
+"""The drop-in simulation executable (superconga_b200/bin/simulation_b200):
+the reference's JSON configuration in, the reference's output files out
+(src/simulation.cu, SimulationWriter.h:57-246)."""
+import csv
+import json
+import os
+import subprocess
+
+import pytest
+
+from tests import configs
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+EXE = os.path.join(ROOT, "superconga_b200", "bin", "simulation_b200")
+
+
+def _run(cfg, tmp_path):
+    path = tmp_path / "simulation_config.json"
+    path.write_text(json.dumps(cfg))
+    return subprocess.run([EXE, str(path)], capture_output=True, text=True, timeout=600)
+
+
+def test_driver_golden_disc(engine_lib, tmp_path):
+    cfg = configs.golden_disc("congacc")
+    cfg["physics"]["order_parameter"]["s"].update({"initial_noise_stddev": 0.0,
+                                                  "initial_phase_shift": 0.0, "vortices": []})
+    cfg["numerics"].update({"num_iterations_burnin": 0, "num_iterations_min": 0,
+                            "num_iterations_max": 100})
+    out = tmp_path / "out"
+    cfg["misc"] = {"save_path": str(out), "save_frequency": -1, "load_path": "",
+                   "verbose": False, "data_format": "csv"}
+    r = _run(cfg, tmp_path)
+    assert r.returncode == 0, r.stderr
+    for name in ("domain.csv", "order_parameter.csv", "current_density.csv",
+                 "vector_potential.csv", "magnetic_flux_density.csv", "simulation_config.json",
+                 "simulation_results.json", "internal_parameters.json",
+                 "simulation_convergence.csv"):
+        assert (out / name).exists(), name
+    res = json.loads((out / "simulation_results.json").read_text())
+    fe = res["free_energy_per_unit_area"]
+    assert abs(fe - configs.GOLDEN_FREE_ENERGY_PER_AREA) <= 1e-3 * abs(configs.GOLDEN_FREE_ENERGY_PER_AREA)
+    with open(out / "order_parameter.csv") as f:
+        rows = list(csv.reader(f))
+    assert rows[0] == ["x_idx", "y_idx", "s_re", "s_im"]
+    n0 = int(round(len(rows[1:]) ** 0.5))
+    assert n0 * n0 == len(rows) - 1
+    conv = list(csv.reader(open(out / "simulation_convergence.csv")))
+    assert conv[0][0] == "iteration" and len(conv) > 2
+    # Continue from the written state: load_path reads the files back
+    # (src/simulation.cu:300-377) and the first iteration stays converged.
+    cfg2 = json.loads(json.dumps(cfg))
+    cfg2["misc"]["load_path"] = str(out)
+    cfg2["misc"]["save_path"] = str(tmp_path / "out2")
+    cfg2["numerics"]["num_iterations_max"] = 3
+    r2 = _run(cfg2, tmp_path)
+    assert r2.returncode == 0, r2.stderr
+    res2 = json.loads((tmp_path / "out2" / "simulation_results.json").read_text())
+    assert abs(res2["free_energy_per_unit_area"] - fe) <= 1e-4 * abs(fe)
+
+
+def test_driver_bad_config(engine_lib, tmp_path):
+    cfg = configs.golden_disc()
+    cfg["numerics"]["norm"] = "l7"
+    r = _run(cfg, tmp_path)
+    assert r.returncode != 0
+    assert "norm" in r.stderr
