@@ -28,6 +28,7 @@ typedef struct sc_ctx sc_ctx;
 #define SC_ERR_ARG -1     /* invalid argument or configuration */
 #define SC_ERR_CUDA -2    /* CUDA runtime error (allocation, launch) */
 #define SC_ERR_STATE -3   /* call not valid in the current state */
+#define SC_ERR_SIZE -4    /* problem larger than the fixed scratch of sc_poisson_noalloc */
 
 #define SC_MODE_FP64 0    /* complex FP64 end to end */
 #define SC_MODE_MIXED 1   /* FP32 Riccati stepping, FP64 accumulation */
@@ -130,6 +131,28 @@ int sc_angle_greens(sc_ctx *ctx, int angle, double *f, double *g_re, double *i_r
  * Poisson filters (ComputeVectorPotential::solve, ComputeVectorPotential.h:727-745),
  * internal units. */
 int sc_poisson(sc_ctx *ctx, const double *j, double *a_out);
+
+/* Allocation-free Poisson solve, for callers that cannot call cudaMalloc: a
+ * plugin inside a framework that has reserved the device memory for its own
+ * pool and passes it only the buffers it owns, or a service whose device
+ * footprint is fixed at start-up.  No counterpart in the reference: it
+ * computes what sc_poisson computes (ComputeVectorPotential::solve), with every
+ * buffer owned by the caller and the intermediates in a fixed 24 MiB device
+ * array of the library instead of allocated memory.
+ *   d_filters  [n_filters][2*n0-1] device, the separable filters (sc_setup_filters)
+ *   positive   [n_filters] host, their signs (sc_setup_filters)
+ *   factor     -h^2 * scale (scale from sc_setup_filters, h the lattice spacing)
+ *   n_grain    lattice sites of the grain (the current's mean is sum / n_grain)
+ *   d_j        [2][n0][n0] device current density; d_a [2][n0][n0] device result
+ *   stream     cudaStream_t the work is issued on (asynchronous)
+ * Limit: n0 <= 724 (6 n0^2 + 128 doubles of scratch); larger n0 returns SC_ERR_SIZE
+ * before any work.  It allocates nothing (no cudaMalloc, no allocating
+ * library call).  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) and should come before any stream capture.
+ * All calls share the array: calls whose work overlaps on the GPU race on it
+ * and must be ordered by the caller. */
+int sc_poisson_noalloc(int n0, int n_filters, const double *d_filters, const int *positive,
+                       double factor, int n_grain, const double *d_j, double *d_a, void *stream);
 
 /* Measures the FP64 (precision 64) or FP32 (precision 32) FMA throughput of
  * the current device in FLOP/s: the CUDA-core denominator of the sweep's

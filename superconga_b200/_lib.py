@@ -42,6 +42,9 @@ SIGNATURES = {
     "sc_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "sc_profile_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                        ctypes.POINTER(ctypes.c_longlong)]),
+    "sc_poisson_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, _c_int_p,
+                                          ctypes.c_double, ctypes.c_int, ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.c_void_p]),
     "sc_measure_fma_peak": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "sc_setup_create": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p)]),
     "sc_setup_last_error": (ctypes.c_char_p, []),
