@@ -76,6 +76,7 @@ struct SweepArgs {
   int n0, n1, ne, nc, groups, log_groups, ept, n_items;
   int burn_in, has_vp, has_ext, gauge;
   int slot_base;
+  int pair;  // angle offset of the mirrored partner angle (n_angles / 2), 0 = unpaired
   double h, lam_scale, flux_b, q, area;
   const int4 *items;  // (angle, x, first row, last row)
   const AngleParams *ang;
@@ -261,6 +262,8 @@ __global__ void __launch_bounds__(128, MINB) k_sweep(const SweepArgs<R> A) {
 
   Cx<R> coh[EMAX];
   const size_t ax = (size_t)a * n1 + x;
+  // Mirrored partner column (angle + pi, x -> n1 - 1 - x) when paired.
+  const size_t pax = (size_t)(a + A.pair) * n1 + (n1 - 1 - x);
   // The next site's label, fields and stored gammaTilde are loaded one site
   // ahead so that their latency overlaps the current site's Riccati steps.
   // ------------------------------------------------------ gammaTilde, down --
@@ -291,6 +294,14 @@ __global__ void __launch_bounds__(128, MINB) k_sweep(const SweepArgs<R> A) {
       site_step<R, EMAX>(l, 3, 2, dre, dim, es, pdre, pdim, pes, eim, coh, A.ept, ecount, h, din,
                          A.bin_gt + (size_t)(in_base + nin) * ne + e0, dout,
                          A.bout_gt + (size_t)(out_base + nout) * ne + e0);
+      if (A.pair && exit) {
+        // gamma of the partner angle at its exit is conj(gammaTilde) here.
+        const Cx<R> *src = A.bout_gt + (size_t)(out_base + nout) * ne + e0;
+        Cx<R> *dst = A.bout_g + (size_t)(A.idx_out_g[pax] + nout) * ne + e0;
+#pragma unroll
+        for (int j = 0; j < EMAX; ++j)
+          if (j < ecount) dst[j] = Cx<R>{src[j].re, -src[j].im};
+      }
       nin += entry;
       nout += exit;
       if (!A.burn_in) {
@@ -348,6 +359,14 @@ __global__ void __launch_bounds__(128, MINB) k_sweep(const SweepArgs<R> A) {
       site_step<R, EMAX>(l, 2, 3, dre, dim, es, pdre, pdim, pes, eim, coh, A.ept, ecount, h, din,
                          A.bin_g + (size_t)(in_base + nin) * ne + e0, dout,
                          A.bout_g + (size_t)(out_base + nout) * ne + e0);
+      if (A.pair && exit) {
+        // gammaTilde of the partner angle at its exit is conj(gamma) here.
+        const Cx<R> *src = A.bout_g + (size_t)(out_base + nout) * ne + e0;
+        Cx<R> *dst = A.bout_gt + (size_t)(A.idx_out_gt[pax] + nout) * ne + e0;
+#pragma unroll
+        for (int j = 0; j < EMAX; ++j)
+          if (j < ecount) dst[j] = Cx<R>{src[j].re, -src[j].im};
+      }
       nin += entry;
       nout += exit;
       pdre = dre;
@@ -379,6 +398,13 @@ __global__ void __launch_bounds__(128, MINB) k_sweep(const SweepArgs<R> A) {
         const size_t fi = (size_t)y * n1 + x;
         fg[fi] = make_double2(sfr, sfi);
         gi[fi] = make_double2(sg, -si);
+        if (A.pair) {
+          // Partner angle at the mirrored site: gamma' = conj(gammaTilde),
+          // gammaTilde' = conj(gamma) give F' = F, Re g' = -Re g, Re I' = Re I.
+          const size_t pf = (size_t)A.pair * nn1 + (size_t)(n1 - 1 - y) * n1 + (n1 - 1 - x);
+          fg[pf] = make_double2(sfr, sfi);
+          gi[pf] = make_double2(-sg, -si);
+        }
       }
     }
   }
@@ -1039,6 +1065,7 @@ struct sc_ctx {
   DevArray<int> onode_a_g, onode_x_g, onode_y_g, onode_a_gt, onode_x_gt, onode_y_gt;
   std::vector<Chunk> chunks;
   int groups = 1, log_groups = 0, ept = 1;
+  int pair = 0;  // > 0: mixed mode sweeps angles [0, n/2) and mirrors them onto [n/2, n)
 
   // state: x = [delta | avec], g = [delta_new | a_new]
   DevArray<double> xstate, gstate, dext, j_real;
@@ -1117,6 +1144,7 @@ SweepArgs<R> sweep_args(sc_ctx *c, const Chunk *ch, int burn_in) {
   A.has_ext = std::fabs(A.flux_b) > 0.0;
   A.gauge = S.gauge;
   A.slot_base = ch ? ch->a_begin : 0;
+  A.pair = (ch && ch->a_begin == 0 && ch->a_end == S.n_angles) ? c->pair : 0;
   A.h = S.h;
   A.lam_scale = c->has_vp() ? 1.0 / (S.lambda * S.lambda) : 0.0;
   A.q = (double)S.charge_sign;
@@ -1160,7 +1188,9 @@ void launch_sweep(sc_ctx *c, const Chunk &ch, int burn_in) {
     check_launch(c);
   }
   ProfScope prof(c, 0);
-  static const int variant = std::getenv("SCB_SWEEP_MINB") ? std::atoi(std::getenv("SCB_SWEEP_MINB")) : 0;
+  // FP64 runs best with four resident blocks per SM (measured on B200).
+  static const char *minb_env = std::getenv("SCB_SWEEP_MINB");
+  const int variant = minb_env ? std::atoi(minb_env) : (sizeof(R) == 8 ? 4 : 1);
   if (c->ept <= 4) {
     if (variant == 4) k_sweep<R, 4, 4><<<blocks, 128, 0, c->stream>>>(A);
     else k_sweep<R, 4, 1><<<blocks, 128, 0, c->stream>>>(A);
@@ -1391,6 +1421,22 @@ void plan_chunks(sc_ctx *c, std::vector<int4> &items) {
   const size_t per_row = (size_t)S.ne * c->esize() + 3 * sizeof(double);
   const size_t frame_slot = (size_t)n1 * n1 * 2 * sizeof(double2);
   items.clear();
+  if (c->pair) {
+    // One chunk over all angles; only the first half gets trajectory columns.
+    Chunk ch{0, na, 0, 0, 0};
+    for (int b = 0; b < na / 2; ++b) {
+      items.insert(items.end(), per[b].begin(), per[b].end());
+      ch.kmax = std::max(ch.kmax, kmax[b]);
+    }
+    ch.item_end = (int)items.size();
+    const double need = (double)items.size() * ch.kmax * per_row + (double)na * frame_slot;
+    if (need <= budget) {
+      c->chunks.push_back(ch);
+      return;
+    }
+    c->pair = 0;  // does not fit one chunk: sweep every angle
+    items.clear();
+  }
   int a = 0;
   while (a < na) {
     Chunk ch{a, a, (int)items.size(), (int)items.size(), 0};
@@ -1501,6 +1547,31 @@ void upload_static(sc_ctx *c) {
   c->onode_x_gt.upload(xgt, s);
   c->onode_y_gt.upload(ygt, s);
 
+  // Mirror pairing of angle a with a + n/2 (mixed mode only): every frame of
+  // the second half must be the 180-degree mirror of its partner, with entry
+  // and exit labels exchanged.  All four basis symmetries are even, so the
+  // order parameter is the same on both angles.
+  c->pair = 0;
+  if (c->mode == SC_MODE_MIXED && na % 2 == 0 && !std::getenv("SCB_NO_PAIRING")) {
+    const int n1p = S.n1;
+    const size_t nn1p = (size_t)n1p * n1p;
+    bool ok = true;
+    for (int a = 0; a < na / 2 && ok; ++a) {
+      const uint8_t *la = &S.labels[(size_t)a * nn1p];
+      const uint8_t *lb = &S.labels[(size_t)(a + na / 2) * nn1p];
+      for (int y = 0; y < n1p && ok; ++y)
+        for (int x = 0; x < n1p; ++x) {
+          uint8_t v = la[(size_t)y * n1p + x];
+          if (v == 2) v = 3;
+          else if (v == 3) v = 2;
+          if (lb[(size_t)(n1p - 1 - y) * n1p + (n1p - 1 - x)] != v) {
+            ok = false;
+            break;
+          }
+        }
+    }
+    if (ok) c->pair = na / 2;
+  }
   std::vector<int4> items;
   plan_chunks(c, items);
   c->items.upload(items, s);
@@ -1858,27 +1929,30 @@ int sc_angle_greens(sc_ctx *ctx, int angle, double *f, double *g_re, double *i_r
   if (!ctx || angle < 0 || angle >= ctx->S.n_angles) return SC_ERR_ARG;
   API_BEGIN
   const HostSetup &S = ctx->S;
-  // Locate the chunk of this angle and sweep only its items.
-  const Chunk *owner = nullptr;
-  for (const Chunk &ch : ctx->chunks)
-    if (angle >= ch.a_begin && angle < ch.a_end) owner = &ch;
-  if (!owner) throw EngineError(SC_ERR_STATE, "angle not planned");
-  std::vector<int4> all(owner->item_end - owner->item_begin);
-  CUDA_TRY(cudaMemcpy(all.data(), ctx->items.p + owner->item_begin, all.size() * sizeof(int4), cudaMemcpyDeviceToHost));
-  int ib = -1, ie = -1;
-  for (size_t k = 0; k < all.size(); ++k)
-    if (all[k].x == angle) {
-      if (ib < 0) ib = (int)k;
-      ie = (int)k + 1;
-    }
+  // The trajectory columns of this angle, swept on their own (unpaired) with
+  // the frame written to slot 0.
+  std::vector<int4> cols;
+  int kmax = 0;
+  for (int x = S.x0[angle]; x <= S.x1[angle]; ++x) {
+    const int lo = S.col_lo[(size_t)angle * S.n1 + x], hi = S.col_hi[(size_t)angle * S.n1 + x];
+    if (lo < 0) continue;
+    cols.push_back(make_int4(angle, x, lo, hi));
+    kmax = std::max(kmax, hi - lo + 1);
+  }
   const size_t nn1 = (size_t)S.n1 * S.n1;
   extend_reference(ctx);
   CUDA_TRY(cudaMemsetAsync(ctx->fg.p, 0, nn1 * sizeof(double2), ctx->stream));
   CUDA_TRY(cudaMemsetAsync(ctx->gi.p, 0, nn1 * sizeof(double2), ctx->stream));
-  if (ib >= 0) {
-    Chunk one{angle, angle + 1, owner->item_begin + ib, owner->item_begin + ie, owner->kmax};
+  if (!cols.empty()) {
+    // Place the columns at the front of the item array (restored below).
+    std::vector<int4> saved(cols.size());
+    CUDA_TRY(cudaMemcpy(saved.data(), ctx->items.p, cols.size() * sizeof(int4), cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(ctx->items.p, cols.data(), cols.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    Chunk one{angle, angle + 1, 0, (int)cols.size(), kmax};
     if (ctx->mode == SC_MODE_FP64) launch_sweep<double>(ctx, one, 0);
     else launch_sweep<float>(ctx, one, 0);
+    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    CUDA_TRY(cudaMemcpy(ctx->items.p, saved.data(), cols.size() * sizeof(int4), cudaMemcpyHostToDevice));
   }
   std::vector<double2> hf(nn1), hg(nn1);
   CUDA_TRY(cudaMemcpyAsync(hf.data(), ctx->fg.p, nn1 * sizeof(double2), cudaMemcpyDeviceToHost, ctx->stream));

@@ -169,3 +169,29 @@ def test_mixed_precision(engine_lib):
     d32, j32, a32 = e32.results()
     assert np.max(np.abs(d32 - d64)) / db <= 1e-5
     assert _rel(j32, j64) <= 1e-4
+
+
+def test_mixed_mirror_pairing(engine_lib, monkeypatch):
+    """Mixed mode sweeps only half of the angles and obtains the other half from
+    the particle-hole mirror (gammaTilde(theta) = conj(gamma(theta + pi))); the
+    result agrees with sweeping every angle within the mixed-precision bound."""
+    import superconga_b200 as sb
+    from oracle import oracle as O
+    for cfg in (configs.small_square_d(), configs.small_disc()):
+        s = O.make_setup(cfg)
+        db = O.delta_bulk(s.temperature, s.symmetries[0])
+        d, a = configs.seeded_state(s.n_comp, s.n0, db, 4, 0.1, True, 0.05)
+        out = []
+        for pairing in (True, False):
+            if pairing:
+                monkeypatch.delenv("SCB_NO_PAIRING", raising=False)
+            else:
+                monkeypatch.setenv("SCB_NO_PAIRING", "1")
+            e = sb.Context(cfg, mode="mixed")
+            e.set_state(d, a)
+            e.compute(3)
+            out.append(e.results())
+            e.close()
+        (d1, j1, a1), (d2, j2, a2) = out
+        assert np.max(np.abs(d1 - d2)) / db <= 1e-5
+        assert _rel(j1, j2) <= 1e-4
