@@ -154,6 +154,43 @@ int sc_poisson(sc_ctx *ctx, const double *j, double *a_out);
 int sc_poisson_noalloc(int n0, int n_filters, const double *d_filters, const int *positive,
                        double factor, int n_grain, const double *d_j, double *d_a, void *stream);
 
+/* ---- LDOS postprocess (Keldysh path) ------------------------------------- */
+
+/* Context of an LDOS postprocess: replaces the Context that src/postprocess.cu
+ * :60-400 builds (IntegrationIteratorKeldysh, ComputeLDOS,
+ * RiccatiSolverConfined with BoundaryConditionSpecular).  simulation_json is
+ * the simulation_config.json of the loaded run; postprocess_json holds the
+ * "spectroscopy" (energy_min, energy_max, num_energies, energy_broadening) and
+ * "numerics" (num_fermi_momenta, convergence_criterion, norm,
+ * num_energies_per_block, num_iterations_*) sections.  The real energies
+ * E_k + i delta are swept one block at a time.  Load Delta and A with
+ * sc_set_state (A in internal units: the file's A times lambda^2).  On such a
+ * context sc_compute returns SC_ERR_STATE; sc_burn_in converges the boundary
+ * of the current block; in sc_get_scalars slot 7 holds the LDOS residual. */
+int sc_ldos_create(const char *simulation_json, const char *postprocess_json, int mode,
+                   sc_ctx **out);
+int sc_ldos_dims(const sc_ctx *ctx, int *n_energies, int *per_block, int *n_blocks);
+/* The real energies E_k (IntegrationIteratorKeldysh.h:91-124) and delta. */
+int sc_ldos_energies(const sc_ctx *ctx, double *energies, double *broadening);
+/* Switches the sweep to energy block b and re-initialises the boundary with
+ * homogeneous values (IntegrationIteratorKeldysh.h:250-268). */
+int sc_ldos_begin_block(sc_ctx *ctx, int block);
+/* n LDOS iterations of the current block (IntegrationIteratorKeldysh::compute,
+ * IntegrationIteratorKeldysh.h:300-389; ComputeLDOS.h:123-193): sweeps, Im g
+ * per energy rotated back, boundary condition, residual of the block's LDOS.
+ * *converged: max(LDOS, boundary) residual below the criterion. */
+int sc_ldos_iterate(sc_ctx *ctx, int n, double *residual, int *converged);
+/* The whole postprocess loop (runPostprocess, run_simulation.h:44-104):
+ * per block burn-in (burnin < 0: until the boundary converges), then
+ * iterations until converged and at least it_min (at most it_max, < 0 = no
+ * limit); stops at the first block that does not converge.  Loops without a
+ * limit stop after 100000 iterations. */
+int sc_ldos_run(sc_ctx *ctx, int burnin, int it_min, int it_max, int *converged,
+                int *iterations);
+/* The LDOS of every energy [n_energies][N0][N0] (ComputeLDOS::getResult). */
+int sc_ldos_get(sc_ctx *ctx, double *ldos);
+int sc_ldos_get_device(sc_ctx *ctx, double *d_ldos);
+
 /* Measures the FP64 (precision 64) or FP32 (precision 32) FMA throughput of
  * the current device in FLOP/s: the CUDA-core denominator of the sweep's
  * compute roofline (the reference has no counterpart; a measurement aid). */

@@ -209,6 +209,7 @@ struct AngleGeom {
 struct Oracle {
   orc_params p;
   std::vector<double> e_im, res;  // Ozaki energies (imag part) and residues
+  std::vector<double> e_re;       // real parts (zero on the Matsubara axis; LDOS energies)
   std::vector<int> sym;           // basis symmetry per component
   std::vector<double> tc;         // relative Tc per component
   std::vector<double> norm_factor, coupling;
@@ -819,7 +820,7 @@ struct Oracle {
 #pragma omp parallel for schedule(dynamic, 4) collapse(2)
       for (int x = x0; x <= x1; ++x)
         for (int e = 0; e < ne; ++e) {
-          const cx e0 = mk(0.0, e_im[e]);
+          const cx e0 = mk(e_re[e], e_im[e]);
           int nin = 0, nout = 0;
           const int ystart = is_g ? y0 : y1;
           const int dy = is_g ? 1 : -1;
@@ -873,7 +874,7 @@ struct Oracle {
       cx *bout = is_g ? bout_g.data() : bout_gt.data();
       for (int x = xr0[a]; x < n; ++x)
         for (int e = 0; e < ne; ++e) {
-          const cx e0 = mk(0.0, e_im[e]);
+          const cx e0 = mk(e_re[e], e_im[e]);
           int nout = 0;
           const int ys = is_g ? 0 : n - 1, dy = is_g ? 1 : -1;
           for (int i = 0; i < n; ++i) {
@@ -1515,6 +1516,43 @@ struct Oracle {
     res_bc = compute_bc();
     n_iterations++;
   }
+  // IntegrationIteratorKeldysh::compute(false) with ComputeLDOS as the only
+  // compute object (IntegrationIteratorKeldysh.h:300-389, ComputeLDOS.h:123-193):
+  // per angle Im g of every energy, extended, weighted and rotated back; then
+  // the boundary condition; LDOS = -sum, zero outside the grain, residual
+  // against the previous iteration of this energy block.
+  std::vector<double> ldos_prev;
+  double res_ldos = 0.0;
+  void ldos_iteration(int n_fields) {
+    if (!boundary_initialized) set_boundary_initial();
+    const int n0 = N0(), n1 = N1(), ne = p.n_energies;
+    const size_t nn0 = (size_t)n0 * n0, nn1 = (size_t)n1 * n1;
+    std::vector<double> acc((size_t)ne * nn0, 0.0), gim(nn1);
+    std::vector<double> dre, dim, es;
+    for (int a = 0; a < p.n_angles; ++a) {
+      rotated_delta(a, dre, dim);
+      energy_shift(a, es);
+      clear_coherence();
+      sweep(a, dre, dim, es, true);
+      const double w = integrand(a), sa = sys_angle(a);
+      for (int e = 0; e < ne; ++e) {
+        for (size_t i = 0; i < nn1; ++i)
+          gim[i] = greens_g(gam[(size_t)e * nn1 + i], gamt[(size_t)e * nn1 + i]).im;
+        extend(ag[a].label, n1, gim.data());
+        for (size_t i = 0; i < nn1; ++i) gim[i] *= w;
+        rotate_insert(acc.data() + (size_t)e * nn0, n0, gim.data(), n1, sa, true);
+      }
+    }
+    res_bc = compute_bc();
+    const size_t n = (size_t)n_fields * nn0;
+    std::vector<double> nw(n);
+    for (size_t i = 0; i < n; ++i) nw[i] = domain_ref[i % nn0] ? -acc[i] : 0.0;
+    if (ldos_prev.size() != n) ldos_prev.assign(n, 0.0);
+    res_ldos = residual_grid(ldos_prev.data(), nw.data(), n, p.norm_type);
+    ldos_prev = nw;
+    n_iterations++;
+  }
+
   // Context::getResidual, Context.h:462-483
   double total_residual() const {
     double r = 0.0;
@@ -1538,6 +1576,7 @@ void *orc_create(const orc_params *p, const double *energies_im, const double *r
   Oracle *o = new Oracle();
   o->p = *p;
   o->e_im.assign(energies_im, energies_im + p->n_energies);
+  o->e_re.assign(p->n_energies, 0.0);
   o->res.assign(residues, residues + p->n_energies);
   o->sym.assign(comp_symmetry, comp_symmetry + p->n_comp);
   o->tc.assign(comp_tc, comp_tc + p->n_comp);
@@ -1743,6 +1782,25 @@ void orc_angle_greens(void *h, int a, double *fre, double *fim, double *gre, dou
   std::memcpy(dre, vdre.data(), nn * 8);
   std::memcpy(dim, vdim.data(), nn * 8);
 }
+// Real parts of the sweep energies (LDOS energies E_k; the imaginary parts,
+// the broadening, are those given to orc_create).  Starts a new energy block:
+// fresh boundary values and LDOS history.
+void orc_set_energies_re(void *h, const double *e_re) {
+  Oracle *o = (Oracle *)h;
+  o->e_re.assign(e_re, e_re + o->p.n_energies);
+  o->boundary_initialized = false;
+  o->ldos_prev.clear();
+}
+
+// One LDOS iteration; ldos_out [n_fields][N0][N0] (may be NULL), residuals out.
+void orc_ldos_iterate(void *h, int n_fields, double *ldos_out, double *res_ldos, double *res_bc) {
+  Oracle *o = (Oracle *)h;
+  o->ldos_iteration(n_fields);
+  if (ldos_out) std::copy(o->ldos_prev.begin(), o->ldos_prev.end(), ldos_out);
+  if (res_ldos) *res_ldos = o->res_ldos;
+  if (res_bc) *res_bc = o->res_bc;
+}
+
 void orc_energy_shift(void *h, int a, double *es) {
   Oracle *o = (Oracle *)h;
   std::vector<double> v;

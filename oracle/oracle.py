@@ -382,7 +382,7 @@ class Setup:
 
     @property
     def n_energies(self) -> int:
-        return len(self.poles)
+        return int(self.params.n_energies) if self.params is not None else len(self.poles)
 
 
 def make_setup(cfg: dict) -> Setup:
@@ -447,15 +447,21 @@ def make_setup(cfg: dict) -> Setup:
 class Oracle:
     """One self-consistency context on the CPU (mirror of conga::Context)."""
 
-    def __init__(self, cfg: dict | str):
+    def __init__(self, cfg: dict | str, energies: tuple | None = None):
+        """energies: optional (imaginary parts, residues) replacing the Ozaki
+        set (the LDOS path sweeps real energies with a common broadening)."""
         if isinstance(cfg, str):
             cfg = json.loads(cfg)
         self.setup = s = make_setup(cfg)
+        e_im, e_res = s.energies_im, s.residues
+        if energies is not None:
+            e_im, e_res = (np.ascontiguousarray(v, np.float64) for v in energies)
+            s.params.n_energies = len(e_im)
         L = lib()
         types, adds, nverts, data = s.geom
         self._keep = [
-            np.ascontiguousarray(s.energies_im, np.float64),
-            np.ascontiguousarray(s.residues, np.float64),
+            np.ascontiguousarray(e_im, np.float64),
+            np.ascontiguousarray(e_res, np.float64),
             np.array([SYMMETRY_ID[x] for x in s.symmetries], np.int32),
             np.array(s.tcs, np.float64),
             np.array(types, np.int32), np.array(adds, np.int32),
@@ -571,6 +577,60 @@ class Oracle:
         out = np.zeros((2, self.n0, self.n0))
         lib().orc_poisson(self.h, _ptr(jj), _ptr(out))
         return out
+
+
+class LdosOracle:
+    """The LDOS postprocess on the CPU (src/postprocess.cu:60-425 with
+    runPostprocess, run_simulation.h:44-104): the simulation configuration with
+    angles, criterion and norm from the postprocess configuration; real
+    energies E_k + i delta (IntegrationIteratorKeldysh.h:91-160) swept one
+    block at a time."""
+
+    def __init__(self, simulation: dict, postprocess: dict):
+        cfg = json.loads(json.dumps(simulation))
+        num, ppn, sp = cfg["numerics"], postprocess["numerics"], postprocess["spectroscopy"]
+        num["num_fermi_momenta"] = int(ppn["num_fermi_momenta"])
+        num["convergence_criterion"] = float(ppn["convergence_criterion"])
+        num["norm"] = ppn.get("norm", "l2")
+        ne = int(sp["num_energies"])
+        emin, emax = float(sp["energy_min"]), float(sp["energy_max"])
+        step = (emax - emin) / (ne - 1) if ne > 1 else 0.0
+        self.energies = np.array([emin + step * i for i in range(ne)])
+        self.broadening = float(sp["energy_broadening"])
+        per = int(ppn.get("num_energies_per_block", 0))
+        self.block = ne if per < 1 else min(per, ne)
+        self.n_blocks = (ne + self.block - 1) // self.block
+        self.oracle = Oracle(cfg, (np.full(self.block, self.broadening), np.zeros(self.block)))
+        self.n0 = self.oracle.n0
+        self.ldos = np.zeros((ne, self.n0, self.n0))
+        self.current = -1
+
+    def set_state(self, delta, a_internal=None):
+        self.oracle.set_state(delta, a_internal)
+
+    def begin_block(self, b: int):
+        ne = len(self.energies)
+        e = np.array([self.energies[min(b * self.block + i, ne - 1)] for i in range(self.block)])
+        self._e = np.ascontiguousarray(e)
+        lib().orc_set_energies_re(self.oracle.h, _ptr(self._e))
+        self.current = b
+
+    def count(self, b: int) -> int:
+        return min(self.block, len(self.energies) - b * self.block)
+
+    def burn_in(self) -> float:
+        self.oracle.burn_in()
+        return self.oracle.scalars()["res_boundary"]
+
+    def iterate(self):
+        """One LDOS iteration; returns (residual, LDOS residual, boundary residual)."""
+        nf = self.count(self.current)
+        out = np.zeros((nf, self.n0, self.n0))
+        rl, rb = ctypes.c_double(), ctypes.c_double()
+        lib().orc_ldos_iterate(self.oracle.h, nf, _ptr(out), ctypes.byref(rl), ctypes.byref(rb))
+        b0 = self.current * self.block
+        self.ldos[b0:b0 + nf] = out
+        return max(rl.value, rb.value), rl.value, rb.value
 
 
 def riccati_step(delta: complex, energy: complex, g0: complex, h: float) -> complex:

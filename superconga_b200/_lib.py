@@ -45,6 +45,15 @@ SIGNATURES = {
     "sc_poisson_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, _c_int_p,
                                           ctypes.c_double, ctypes.c_int, ctypes.c_void_p,
                                           ctypes.c_void_p, ctypes.c_void_p]),
+    "sc_ldos_create": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int,
+                                      ctypes.POINTER(ctypes.c_void_p)]),
+    "sc_ldos_dims": (ctypes.c_int, [ctypes.c_void_p, _c_int_p, _c_int_p, _c_int_p]),
+    "sc_ldos_energies": (ctypes.c_int, [ctypes.c_void_p, _c_double_p, ctypes.POINTER(ctypes.c_double)]),
+    "sc_ldos_begin_block": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "sc_ldos_iterate": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double), _c_int_p]),
+    "sc_ldos_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _c_int_p, _c_int_p]),
+    "sc_ldos_get": (ctypes.c_int, [ctypes.c_void_p, _c_double_p]),
+    "sc_ldos_get_device": (ctypes.c_int, [ctypes.c_void_p, _c_double_p]),
     "sc_measure_fma_peak": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "sc_setup_create": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p)]),
     "sc_setup_last_error": (ctypes.c_char_p, []),

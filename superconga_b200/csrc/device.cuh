@@ -125,6 +125,16 @@ __device__ __forceinline__ void local_greens(Cx<R> g, Cx<R> gt, R dre, R dim, Cx
   i_im = (dre * g.im - dim * g.re) - (dre * gt.im + dim * gt.re);
 }
 
+// Im g of one real energy, g = -i (1 - g gt) / (1 + g gt) (LocalGreens.h:32-43).
+template <typename R>
+__device__ __forceinline__ R greens_g_im(Cx<R> g, Cx<R> gt) {
+  const Cx<R> p = cmul(g, gt);
+  const R den_re = R(1) + p.re, den_im = p.im;
+  const R inv = rcp_(den_re * den_re + den_im * den_im);
+  const R nr = R(1) - p.re, ni = -p.im;
+  return -(nr * den_re + ni * den_im) * inv;
+}
+
 // Bilinear lookup of insertRotatedGrid(_Additive)_kernel
 // (GridFunctions_GPU.h:436-546): coordinates of site (x, y) of an n_out grid in
 // an n_in grid rotated by the angle whose (cos, sin) of minus the angle are

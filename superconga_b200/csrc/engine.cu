@@ -87,10 +87,11 @@ struct SweepArgs {
   Cx<R> *bout_g, *bout_gt;
   const double *dext;  // [c][2][n0*n0]
   const double *avec;  // [2][n0*n0]
-  const double *e_im, *res;
+  const double *e_re, *e_im, *res;
   Cx<R> *scratch;   // [row][energy][item]
   double *scratch2; // [row][3][item]: Re D, Im D, energy shift
   double2 *fg, *gi; // frame buffers [slot][n1*n1]: (Re F, Im F), (Re G, Re I)
+  double *ldf;      // LDOS frame buffer [slot][energy][n1*n1]: Im g per real energy
 };
 
 // Gauges, include/conga/riccati/energy_shift/Gauges.h:25-62.
@@ -193,11 +194,11 @@ __global__ void __launch_bounds__(128) k_frame_fields(const SweepArgs<R> A, int 
 // sites start from the stored boundary value with the partial step dist*h, grain
 // sites take the midpoint step, exit sites also step on to the boundary and
 // store the out-going value, sites outside the grain reset to zero.
-template <typename R, int EMAX>
+template <typename R, int EMAX, bool KEL>
 __device__ __forceinline__ void site_step(uint8_t l, uint8_t l_entry, uint8_t l_exit, R dre,
-                                          R dim, R es, R pdre, R pdim, R pes, const R *eim,
-                                          Cx<R> *coh, int ept, int ecount, R h, R dist_in,
-                                          const Cx<R> *bin, R dist_out, Cx<R> *bout) {
+                                          R dim, R es, R pdre, R pdim, R pes, const R *ere,
+                                          const R *eim, Cx<R> *coh, int ept, int ecount, R h,
+                                          R dist_in, const Cx<R> *bin, R dist_out, Cx<R> *bout) {
   const bool entry = l == l_entry;
   const R sdre = entry ? dre : (dre + pdre) * R(0.5);
   const R sdim = entry ? dim : (dim + pdim) * R(0.5);
@@ -208,14 +209,14 @@ __device__ __forceinline__ void site_step(uint8_t l, uint8_t l_entry, uint8_t l_
     if (j < ept) {
       Cx<R> g0 = coh[j];
       if (entry) g0 = (j < ecount) ? bin[j] : Cx<R>{R(0), R(0)};
-      coh[j] = riccati_step<R>(sdre, sdim, ses, eim[j], g0, st);
+      coh[j] = riccati_step<R>(sdre, sdim, KEL ? ses + ere[j] : ses, eim[j], g0, st);
     }
   if (l == l_exit) {
     const R sb = dist_out * h;
 #pragma unroll
     for (int j = 0; j < EMAX; ++j)
       if (j < ept) {
-        const Cx<R> bv = riccati_step<R>(dre, dim, es, eim[j], coh[j], sb);
+        const Cx<R> bv = riccati_step<R>(dre, dim, KEL ? es + ere[j] : es, eim[j], coh[j], sb);
         if (j < ecount) bout[j] = bv;
       }
   }
@@ -232,7 +233,10 @@ __device__ __forceinline__ void site_step(uint8_t l, uint8_t l_entry, uint8_t l_
 // site by site (RiccatiSolverConfined.h:129-312, GreensFunctionStatic.h:92-157,
 // ComputeFreeEnergy.h:106-160).  The frame order parameter and the energies come
 // from scratch2 (FP64); the coherence functions are integrated in R.
-template <typename R, int EMAX, int MINB>
+// KEL: real energies e_re + i e_im (the LDOS path, IntegrationIteratorKeldysh.h
+// :219-389); instead of the energy sums, Im g of every energy is written to the
+// LDOS frame buffer (GreensFunctionStatic.h:66-90, ComputeLDOS.h:123-144).
+template <typename R, int EMAX, int MINB, bool KEL>
 __global__ void __launch_bounds__(128, MINB) k_sweep(const SweepArgs<R> A) {
   __shared__ double s_res[64];  // Ozaki residues (at most 64 energies)
   for (int e = threadIdx.x; e < A.ne && e < 64; e += blockDim.x) s_res[e] = A.res[e];
@@ -256,9 +260,12 @@ __global__ void __launch_bounds__(128, MINB) k_sweep(const SweepArgs<R> A) {
   if (ecount > A.ept) ecount = A.ept;
   if (ecount < 0) ecount = 0;
 
-  R eim[EMAX];
+  R eim[EMAX], ere[EMAX];
 #pragma unroll
-  for (int j = 0; j < EMAX; ++j) eim[j] = (j < ecount) ? (R)A.e_im[e0 + j] : R(1);
+  for (int j = 0; j < EMAX; ++j) {
+    eim[j] = (j < ecount) ? (R)A.e_im[e0 + j] : R(1);
+    ere[j] = (KEL && j < ecount) ? (R)A.e_re[e0 + j] : R(0);
+  }
 
   Cx<R> coh[EMAX];
   const size_t ax = (size_t)a * n1 + x;
@@ -291,7 +298,7 @@ __global__ void __launch_bounds__(128, MINB) k_sweep(const SweepArgs<R> A) {
       const bool entry = l == 3, exit = l == 2;
       const R din = entry ? (R)A.dist_in_gt[in_base + nin] : R(0);
       const R dout = exit ? (R)A.dist_out_gt[out_base + nout] : R(0);
-      site_step<R, EMAX>(l, 3, 2, dre, dim, es, pdre, pdim, pes, eim, coh, A.ept, ecount, h, din,
+      site_step<R, EMAX, KEL>(l, 3, 2, dre, dim, es, pdre, pdim, pes, ere, eim, coh, A.ept, ecount, h, din,
                          A.bin_gt + (size_t)(in_base + nin) * ne + e0, dout,
                          A.bout_gt + (size_t)(out_base + nout) * ne + e0);
       if (A.pair && exit) {
@@ -356,7 +363,7 @@ __global__ void __launch_bounds__(128, MINB) k_sweep(const SweepArgs<R> A) {
       const bool entry = l == 2, exit = l == 3;
       const R din = entry ? (R)A.dist_in_g[in_base + nin] : R(0);
       const R dout = exit ? (R)A.dist_out_g[out_base + nout] : R(0);
-      site_step<R, EMAX>(l, 2, 3, dre, dim, es, pdre, pdim, pes, eim, coh, A.ept, ecount, h, din,
+      site_step<R, EMAX, KEL>(l, 2, 3, dre, dim, es, pdre, pdim, pes, ere, eim, coh, A.ept, ecount, h, din,
                          A.bin_g + (size_t)(in_base + nin) * ne + e0, dout,
                          A.bout_g + (size_t)(out_base + nout) * ne + e0);
       if (A.pair && exit) {
@@ -373,6 +380,15 @@ __global__ void __launch_bounds__(128, MINB) k_sweep(const SweepArgs<R> A) {
       pdim = dim;
       pes = es;
       if (A.burn_in) continue;
+      if constexpr (KEL) {
+        if (l != 0) {
+          double *o = A.ldf + ((size_t)(a - A.slot_base) * ne + e0) * nn1 + (size_t)y * n1 + x;
+#pragma unroll
+          for (int j = 0; j < EMAX; ++j)
+            if (j < ecount) o[(size_t)j * nn1] = (double)greens_g_im<R>(coh[j], gt[j]);
+        }
+        continue;
+      }
       double sfr = 0.0, sfi = 0.0, sg = 0.0, si = 0.0;
       if (l != 0) {
 #pragma unroll
@@ -480,6 +496,53 @@ __global__ void __launch_bounds__(256) k_rotate_back(int n0, int n1, int nc, int
   acc_fe[i] = fe;
 }
 
+// LDOS frame extension next to the boundary, every energy of the block
+// (ComputeLDOS.h:137-138 through domain_ops.h:11-69).
+__global__ void k_halo_ldos(int n_entries, int entry0, int n1, int ne,
+                            const int *__restrict__ entry_angle, int slot_base,
+                            const int *__restrict__ site, const int *__restrict__ off,
+                            const int *__restrict__ src, double *ldf) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n_entries) return;
+  const int e = entry0 + k;
+  const size_t nn1 = (size_t)n1 * n1;
+  double *f = ldf + ((size_t)(entry_angle[e] - slot_base) * ne + blockIdx.y) * nn1;
+  const int b = off[e], en = off[e + 1];
+  double v = f[src[b]];
+  for (int i = b + 1; i < en; ++i) v = __dadd_rn(v, f[src[i]]);
+  f[site[e]] = __ddiv_rn(v, (double)(en - b));
+}
+
+// LDOS frames rotated back onto the reference grid and accumulated in angle
+// order, Im part weighted by the integrand factor (ComputeLDOS.h:140-144,
+// insertRotatedGridAdditive with Type::imag, GridFunctions_GPU.h:991-1054).
+__global__ void __launch_bounds__(256) k_rotate_back_ldos(int n0, int n1, int ne, int a_begin, int a_end,
+                                                          const AngleParams *__restrict__ ang,
+                                                          const double *__restrict__ ldf, double *acc) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int e = blockIdx.z;
+  if (x >= n0 || y >= n0) return;
+  const size_t nn0 = (size_t)n0 * n0, nn1 = (size_t)n1 * n1;
+  const size_t i = (size_t)e * nn0 + (size_t)y * n0 + x;
+  double v = acc[i];
+  for (int a = a_begin; a < a_end; ++a) {
+    const AngleParams &P = ang[a];
+    Bilinear b;
+    if (!rotated_lookup(x, y, n0, n1, P.cB, P.sB, b)) continue;
+    const double *f = ldf + ((size_t)(a - a_begin) * ne + e) * nn1 + b.i00;
+    v += bilerp(f[0] * P.w, f[1] * P.w, f[n1] * P.w, f[n1 + 1] * P.w, b.xf, b.yf);
+  }
+  acc[i] = v;
+}
+
+// ComputeLDOS::computePropertyFromGreens (ComputeLDOS.h:146-193): LDOS = -sum,
+// zero outside the grain, residual against the block's previous LDOS, stored
+// into the full LDOS array.
+__global__ void __launch_bounds__(256) k_ldos_finalize(int n0, int n_fields, const uint8_t *__restrict__ dom,
+                                                       const double *__restrict__ acc, double *ldos,
+                                                       double *partial);
+
 // Residual partial sums of one (old, new) pair: sum d^2, sum old^2, sum |d|,
 // sum |old|, max |d|, max |old| (ComputeResidual.h:54-106).
 struct Res6 {
@@ -574,6 +637,20 @@ __global__ void __launch_bounds__(REDUCE_THREADS) k_finalize(
   block_reduce(q, NQ, FIN_MAX_MASK, partial + (size_t)blockIdx.x * NQ);
 }
 
+__global__ void __launch_bounds__(256) k_ldos_finalize(int n0, int n_fields, const uint8_t *__restrict__ dom,
+                                                       const double *__restrict__ acc, double *ldos,
+                                                       double *partial) {
+  double q[6] = {0, 0, 0, 0, 0, 0};
+  const size_t nn = (size_t)n0 * n0, n = nn * n_fields;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const double nv = dom[i % nn] ? -acc[i] : 0.0;
+    res_add(q, ldos[i], nv);
+    ldos[i] = nv;
+  }
+  block_reduce(q, 6, 0x30ull, partial + (size_t)blockIdx.x * 6);
+}
+
 // Residual partials of a boundary gather (in-place update) or of any (old, new)
 // pair of arrays.
 __global__ void __launch_bounds__(REDUCE_THREADS) k_residual(size_t n, const double *__restrict__ o,
@@ -635,7 +712,7 @@ __global__ void k_boundary_initial(int n_out, int ne, int is_g, const int *__res
   double dre, dim, es;
   frame_fields(A, P, node_x[k], node_y[k], dre, dim, es);
   Cx<R> g, gt;
-  riccati_homogeneous<R>((R)dre, (R)dim, (R)es, (R)A.e_im[e], g, gt);
+  riccati_homogeneous<R>((R)dre, (R)dim, (R)(es + A.e_re[e]), (R)A.e_im[e], g, gt);
   bout[t] = is_g ? g : gt;
 }
 
@@ -1059,7 +1136,7 @@ struct sc_ctx {
   DevArray<int> halo_site, halo_off, halo_src, halo_angle;
   DevArray<int> rext_site, rext_off, rext_src;
   DevArray<int4> items;
-  DevArray<double> e_im, res, coupling;
+  DevArray<double> e_re, e_im, res, coupling;
   DevArray<double> filters;
   DevArray<int> filter_pos;
   DevArray<int> onode_a_g, onode_x_g, onode_y_g, onode_a_gt, onode_x_gt, onode_y_gt;
@@ -1080,6 +1157,10 @@ struct sc_ctx {
   DevArray<Scalars> scalars;
   DevArray<double> tmp_io;
   int nb_fin = 0, nb_bnd = 0, nb_vp = 0, nb_acc = 0;
+
+  // LDOS postprocess: frame buffer, block accumulator, all energies.
+  DevArray<double> ldf, ldos_acc, ldos_all;
+  int ldos_block = -1;  // block whose energies the sweep uses
 
   bool boundary_initialized = false, first_compute = true;
   Scalars host_scalars{};
@@ -1166,8 +1247,10 @@ SweepArgs<R> sweep_args(sc_ctx *c, const Chunk *ch, int burn_in) {
   A.bout_gt = (Cx<R> *)c->bnd_ptr(3);
   A.dext = c->dext.p;
   A.avec = c->xstate.p + (size_t)2 * S.nc * c->nn0();
+  A.e_re = c->e_re.p;
   A.e_im = c->e_im.p;
   A.res = c->res.p;
+  A.ldf = c->ldf.p;
   A.scratch = (Cx<R> *)c->scratch.p;
   A.scratch2 = c->scratch2.p;
   A.fg = (double2 *)c->fg.p;
@@ -1191,13 +1274,17 @@ void launch_sweep(sc_ctx *c, const Chunk &ch, int burn_in) {
   // FP64 runs best with four resident blocks per SM (measured on B200).
   static const char *minb_env = std::getenv("SCB_SWEEP_MINB");
   const int variant = minb_env ? std::atoi(minb_env) : (sizeof(R) == 8 ? 4 : 1);
-  if (c->ept <= 4) {
-    if (variant == 4) k_sweep<R, 4, 4><<<blocks, 128, 0, c->stream>>>(A);
-    else k_sweep<R, 4, 1><<<blocks, 128, 0, c->stream>>>(A);
+  if (c->S.keldysh) {
+    if (c->ept <= 4) k_sweep<R, 4, 1, true><<<blocks, 128, 0, c->stream>>>(A);
+    else if (c->ept <= 8) k_sweep<R, 8, 1, true><<<blocks, 128, 0, c->stream>>>(A);
+    else k_sweep<R, 16, 1, true><<<blocks, 128, 0, c->stream>>>(A);
+  } else if (c->ept <= 4) {
+    if (variant == 4) k_sweep<R, 4, 4, false><<<blocks, 128, 0, c->stream>>>(A);
+    else k_sweep<R, 4, 1, false><<<blocks, 128, 0, c->stream>>>(A);
   } else if (c->ept <= 8) {
-    k_sweep<R, 8, 1><<<blocks, 128, 0, c->stream>>>(A);
+    k_sweep<R, 8, 1, false><<<blocks, 128, 0, c->stream>>>(A);
   } else {
-    k_sweep<R, 16, 1><<<blocks, 128, 0, c->stream>>>(A);
+    k_sweep<R, 16, 1, false><<<blocks, 128, 0, c->stream>>>(A);
   }
   check_launch(c);
 }
@@ -1250,10 +1337,11 @@ void boundary_initial(sc_ctx *c) {
   c->boundary_initialized = true;
 }
 
-void launch_scalars_b(sc_ctx *c, int do_bc, int do_vp, int compute_mode) {
+void launch_scalars_b(sc_ctx *c, int do_bc, int do_vp, int compute_mode, size_t n_elem_vp = 0) {
   const HostSetup &S = c->S;
+  if (!n_elem_vp) n_elem_vp = 2 * c->nn0();
   k_scalars_b<<<1, 256, 0, c->stream>>>(S.norm, (size_t)2 * S.n_in_g * S.ne,
-                                         (size_t)2 * S.n_in_gt * S.ne, 2 * c->nn0(), do_bc, do_vp,
+                                         (size_t)2 * S.n_in_gt * S.ne, n_elem_vp, do_bc, do_vp,
                                          compute_mode, c->partial_bg.p, c->nb_bnd, c->partial_bgt.p,
                                          c->nb_bnd, c->partial_vp.p, c->nb_vp, c->scalars.p);
   check_launch(c);
@@ -1309,9 +1397,38 @@ void accelerate(sc_ctx *c) {
 }
 
 template <typename R>
+void run_chunks_ldos(sc_ctx *c, int burn_in) {
+  const HostSetup &S = c->S;
+  const size_t nn1 = (size_t)S.n1 * S.n1;
+  for (const Chunk &ch : c->chunks) {
+    const int nslots = ch.a_end - ch.a_begin;
+    if (!burn_in)
+      CUDA_TRY(cudaMemsetAsync(c->ldf.p, 0, (size_t)nslots * S.ne * nn1 * sizeof(double), c->stream));
+    launch_sweep<R>(c, ch, burn_in);
+    if (burn_in) continue;
+    const int h0 = S.halo_angle_off[ch.a_begin], h1 = S.halo_angle_off[ch.a_end];
+    if (h1 > h0) {
+      dim3 grid(grid1(h1 - h0, 128), S.ne);
+      k_halo_ldos<<<grid, 128, 0, c->stream>>>(h1 - h0, h0, S.n1, S.ne, c->halo_angle.p, ch.a_begin,
+                                               c->halo_site.p, c->halo_off.p, c->halo_src.p, c->ldf.p);
+      check_launch(c);
+    }
+    dim3 blk(32, 8), grid((S.n0 + 31) / 32, (S.n0 + 7) / 8, S.ne);
+    ProfScope prof(c, 1);
+    k_rotate_back_ldos<<<grid, blk, 0, c->stream>>>(S.n0, S.n1, S.ne, ch.a_begin, ch.a_end, c->ang.p,
+                                                    c->ldf.p, c->ldos_acc.p);
+    check_launch(c);
+  }
+}
+
+template <typename R>
 void run_chunks(sc_ctx *c, int burn_in) {
   const HostSetup &S = c->S;
   const size_t nn1 = (size_t)S.n1 * S.n1;
+  if (S.keldysh) {
+    run_chunks_ldos<R>(c, burn_in);
+    return;
+  }
   for (const Chunk &ch : c->chunks) {
     const int nslots = ch.a_end - ch.a_begin;
     if (!burn_in) {
@@ -1385,13 +1502,54 @@ void compute_once(sc_ctx *c) {
   c->first_compute = false;
 }
 
+void ldos_begin_block(sc_ctx *c, int b);
+
 template <typename R>
 void burn_in_once(sc_ctx *c) {
+  if (c->S.keldysh && c->ldos_block < 0) ldos_begin_block(c, 0);
   if (!c->boundary_initialized) boundary_initial<R>(c);
   extend_reference(c);
   run_chunks<R>(c, 1);
   boundary_condition<R>(c);
   launch_scalars_b(c, 1, 0, 0);
+}
+
+// Energies of LDOS block b and fresh homogeneous boundary values
+// (IntegrationIteratorKeldysh.h:250-268: a new energy interval re-initialises
+// the Riccati solver and the boundary).
+void ldos_begin_block(sc_ctx *c, int b) {
+  const HostSetup &S = c->S;
+  if (b < 0 || b >= S.ldos_n_blocks) throw EngineError(SC_ERR_ARG, "LDOS block out of range");
+  std::vector<double> e;
+  ldos_block_energies(S, b, e);
+  CUDA_TRY(cudaMemcpyAsync(c->e_re.p, e.data(), e.size() * sizeof(double), cudaMemcpyHostToDevice,
+                           c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  c->ldos_block = b;
+  c->boundary_initialized = false;
+}
+
+int ldos_block_count(const sc_ctx *c, int b) {
+  const int n = (int)c->S.ldos_energies.size();
+  return std::min(c->S.ldos_block, n - b * c->S.ldos_block);
+}
+
+// One LDOS iteration of the current block (IntegrationIteratorKeldysh::compute
+// with inIsBurnIn = false, IntegrationIteratorKeldysh.h:300-389).
+template <typename R>
+void ldos_once(sc_ctx *c) {
+  const HostSetup &S = c->S;
+  if (c->ldos_block < 0) ldos_begin_block(c, 0);
+  if (!c->boundary_initialized) boundary_initial<R>(c);
+  extend_reference(c);
+  c->ldos_acc.zero(c->stream);
+  run_chunks<R>(c, 0);
+  boundary_condition<R>(c);
+  const int nf = ldos_block_count(c, c->ldos_block);
+  double *blk = c->ldos_all.p + (size_t)c->ldos_block * S.ldos_block * c->nn0();
+  k_ldos_finalize<<<c->nb_vp, 256, 0, c->stream>>>(S.n0, nf, c->dom.p, c->ldos_acc.p, blk, c->partial_vp.p);
+  check_launch(c);
+  launch_scalars_b(c, 1, 1, 0, (size_t)nf * c->nn0());
 }
 
 void read_scalars(sc_ctx *c) {
@@ -1419,7 +1577,8 @@ void plan_chunks(sc_ctx *c, std::vector<int4> &items) {
   if (const char *env = std::getenv("SCB_SCRATCH_MB")) budget_mb = std::atof(env);
   const double budget = budget_mb * 1048576.0;
   const size_t per_row = (size_t)S.ne * c->esize() + 3 * sizeof(double);
-  const size_t frame_slot = (size_t)n1 * n1 * 2 * sizeof(double2);
+  const size_t frame_slot = S.keldysh ? (size_t)n1 * n1 * S.ne * sizeof(double)
+                                      : (size_t)n1 * n1 * 2 * sizeof(double2);
   items.clear();
   if (c->pair) {
     // One chunk over all angles; only the first half gets trajectory columns.
@@ -1506,6 +1665,7 @@ void upload_static(sc_ctx *c) {
   c->rext_site.upload(S.rext_site, s);
   c->rext_off.upload(S.rext_src_off, s);
   c->rext_src.upload(S.rext_src, s);
+  c->e_re.upload(S.e_re, s);
   c->e_im.upload(S.e_im, s);
   c->res.upload(S.residues, s);
   c->coupling.upload(S.coupling, s);
@@ -1552,7 +1712,7 @@ void upload_static(sc_ctx *c) {
   // and exit labels exchanged.  All four basis symmetries are even, so the
   // order parameter is the same on both angles.
   c->pair = 0;
-  if (c->mode == SC_MODE_MIXED && na % 2 == 0 && !std::getenv("SCB_NO_PAIRING")) {
+  if (c->mode == SC_MODE_MIXED && !S.keldysh && na % 2 == 0 && !std::getenv("SCB_NO_PAIRING")) {
     const int n1p = S.n1;
     const size_t nn1p = (size_t)n1p * n1p;
     bool ok = true;
@@ -1623,8 +1783,15 @@ void upload_static(sc_ctx *c) {
   }
   c->scratch.alloc(scr / sizeof(double) + 1);
   c->scratch2.alloc(scr2 + 1);
-  c->fg.alloc((size_t)max_slots * n1 * n1 * 2);
-  c->gi.alloc((size_t)max_slots * n1 * n1 * 2);
+  if (S.keldysh) {
+    c->ldf.alloc((size_t)max_slots * S.ne * n1 * n1);
+    c->ldos_acc.alloc((size_t)S.ne * nn);
+    c->ldos_all.alloc((size_t)S.ldos_n_blocks * S.ldos_block * nn);
+    c->ldos_all.zero(s);
+  } else {
+    c->fg.alloc((size_t)max_slots * n1 * n1 * 2);
+    c->gi.alloc((size_t)max_slots * n1 * n1 * 2);
+  }
   c->nb_fin = std::min<int>(592, (int)grid1(nn, REDUCE_THREADS));
   c->nb_bnd = 296;
   c->nb_vp = std::min<int>(296, (int)grid1(2 * nn, REDUCE_THREADS));
@@ -1635,7 +1802,7 @@ void upload_static(sc_ctx *c) {
   c->partial_vp.alloc((size_t)c->nb_vp * 6);
   c->partial_acc.alloc((size_t)16 * c->nb_acc * 3);
   c->partial_vp.zero(s);
-  if (S.n_filters) {
+  if (S.n_filters && !S.keldysh) {
     c->pois_s.alloc(2 * nn);
     c->pois_t0.alloc((size_t)S.n_filters * 2 * nn);
     c->pois_t1.alloc((size_t)S.n_filters * 2 * nn);
@@ -1672,26 +1839,32 @@ int fail(sc_ctx *c, const EngineError &e) {
 
 extern "C" {
 
-int sc_create(const char *config_json, int mode, sc_ctx **out) {
-  sc_ctx *ctx = nullptr;
-  if (!config_json || !out) {
-    g_create_error = "sc_create: null argument";
+}  // extern "C"
+
+namespace {
+// Shared part of sc_create / sc_ldos_create: the setup is built by `make`.
+template <typename F>
+int create_context(int mode, sc_ctx **out, F make) {
+  if (!out) {
+    g_create_error = "null output handle";
     return SC_ERR_ARG;
   }
   *out = nullptr;
   if (mode != SC_MODE_FP64 && mode != SC_MODE_MIXED) {
-    g_create_error = "sc_create: mode must be SC_MODE_FP64 or SC_MODE_MIXED";
+    g_create_error = "mode must be SC_MODE_FP64 or SC_MODE_MIXED";
     return SC_ERR_ARG;
   }
   sc_ctx *c = new sc_ctx();
   c->mode = mode;
   try {
-    const std::string e = build_setup(config_json, c->S);
+    const std::string e = make(c->S);
     if (!e.empty()) throw EngineError(SC_ERR_ARG, e);
     if (c->S.nc > MAX_COMP) throw EngineError(SC_ERR_ARG, "at most 4 order-parameter components");
-    if (c->S.ne > 64) throw EngineError(SC_ERR_ARG, "at most 64 Ozaki energies (raise the temperature or lower the cutoff)");
+    if (c->S.ne > 64)
+      throw EngineError(SC_ERR_ARG, c->S.keldysh ? "at most 64 energies per LDOS block"
+                                                 : "at most 64 Ozaki energies (raise the temperature or lower the cutoff)");
     if (2 * c->S.nc + 2 > 16) throw EngineError(SC_ERR_ARG, "too many accelerator fields");
-    if (c->S.acc.kind == ACC_ANDERSON)
+    if (!c->S.keldysh && c->S.acc.kind == ACC_ANDERSON)
       throw EngineError(SC_ERR_ARG, "accelerator 'anderson' is not available in this engine");
     CUDA_TRY(cudaGetDevice(&c->device));
     CUDA_TRY(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
@@ -1705,11 +1878,34 @@ int sc_create(const char *config_json, int mode, sc_ctx **out) {
     return e.code;
   } catch (const std::exception &e) {
     g_create_error = e.what();
+    cudaStream_t s = c->own_stream;
     delete c;
+    if (s) cudaStreamDestroy(s);
     return SC_ERR_ARG;
   }
   *out = c;
   return SC_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int sc_create(const char *config_json, int mode, sc_ctx **out) {
+  if (!config_json) {
+    g_create_error = "sc_create: null argument";
+    return SC_ERR_ARG;
+  }
+  return create_context(mode, out, [&](HostSetup &S) { return build_setup(config_json, S); });
+}
+
+int sc_ldos_create(const char *simulation_json, const char *postprocess_json, int mode, sc_ctx **out) {
+  if (!simulation_json || !postprocess_json) {
+    g_create_error = "sc_ldos_create: null argument";
+    return SC_ERR_ARG;
+  }
+  return create_context(mode, out, [&](HostSetup &S) {
+    return build_ldos_setup(simulation_json, postprocess_json, S);
+  });
 }
 
 int sc_destroy(sc_ctx *ctx) {
@@ -1801,6 +1997,10 @@ int sc_get_state_device(sc_ctx *ctx, double *d_delta, double *d_a) {
 
 int sc_compute(sc_ctx *ctx, int n, double *residual, int *converged) {
   if (!ctx || n < 0) return SC_ERR_ARG;
+  if (ctx->S.keldysh) {
+    ctx->err = "sc_compute: an LDOS context iterates with sc_ldos_iterate";
+    return SC_ERR_STATE;
+  }
   API_BEGIN
   for (int i = 0; i < n; ++i) {
     if (ctx->mode == SC_MODE_FP64) compute_once<double>(ctx);
@@ -1834,6 +2034,103 @@ int sc_get_results(sc_ctx *ctx, double *delta_new, double *j, double *a_new) {
   if (delta_new) CUDA_TRY(cudaMemcpyAsync(delta_new, ctx->gstate.p, nd * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   if (j) CUDA_TRY(cudaMemcpyAsync(j, ctx->j_real.p, 2 * nn * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   if (a_new) CUDA_TRY(cudaMemcpyAsync(a_new, ctx->gstate.p + nd, 2 * nn * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  API_END
+}
+
+int sc_ldos_dims(const sc_ctx *ctx, int *n_energies, int *per_block, int *n_blocks) {
+  if (!ctx || !ctx->S.keldysh) return SC_ERR_ARG;
+  if (n_energies) *n_energies = (int)ctx->S.ldos_energies.size();
+  if (per_block) *per_block = ctx->S.ldos_block;
+  if (n_blocks) *n_blocks = ctx->S.ldos_n_blocks;
+  return SC_OK;
+}
+
+int sc_ldos_energies(const sc_ctx *ctx, double *energies, double *broadening) {
+  if (!ctx || !ctx->S.keldysh) return SC_ERR_ARG;
+  if (energies)
+    std::memcpy(energies, ctx->S.ldos_energies.data(), ctx->S.ldos_energies.size() * sizeof(double));
+  if (broadening) *broadening = ctx->S.ldos_broadening;
+  return SC_OK;
+}
+
+int sc_ldos_begin_block(sc_ctx *ctx, int block) {
+  if (!ctx || !ctx->S.keldysh) return SC_ERR_ARG;
+  API_BEGIN
+  ldos_begin_block(ctx, block);
+  API_END
+}
+
+int sc_ldos_iterate(sc_ctx *ctx, int n, double *residual, int *converged) {
+  if (!ctx || !ctx->S.keldysh || n < 0) return SC_ERR_ARG;
+  API_BEGIN
+  for (int i = 0; i < n; ++i) {
+    if (ctx->mode == SC_MODE_FP64) ldos_once<double>(ctx);
+    else ldos_once<float>(ctx);
+  }
+  read_scalars(ctx);
+  const Scalars &s = ctx->host_scalars;
+  if (residual) *residual = s.residual;
+  if (converged) *converged = s.residual < ctx->S.conv_crit ? 1 : 0;
+  API_END
+}
+
+int sc_ldos_run(sc_ctx *ctx, int burnin, int it_min, int it_max, int *converged, int *iterations) {
+  if (!ctx || !ctx->S.keldysh) return SC_ERR_ARG;
+  API_BEGIN
+  // runPostprocess (run_simulation.h:44-104) with runIterations
+  // (run_iteration.h:75-130); "until converged" loops stop after 100000.
+  const int cap = 100000;
+  const double crit = ctx->S.conv_crit;
+  int total = 0;
+  bool all = true;
+  for (int b = 0; b < ctx->S.ldos_n_blocks; ++b) {
+    ldos_begin_block(ctx, b);
+    if (!(burnin == 0)) {
+      for (int i = 1; i <= cap; ++i) {
+        if (ctx->mode == SC_MODE_FP64) burn_in_once<double>(ctx);
+        else burn_in_once<float>(ctx);
+        read_scalars(ctx);
+        ++total;
+        const bool conv = ctx->host_scalars.res_bc < crit;
+        if ((conv && i >= burnin) || (burnin >= 0 && i >= burnin)) break;
+      }
+    }
+    bool conv = false;
+    if (!(it_min == 0 && it_max == 0)) {
+      for (int i = 1; i <= cap; ++i) {
+        if (ctx->mode == SC_MODE_FP64) ldos_once<double>(ctx);
+        else ldos_once<float>(ctx);
+        read_scalars(ctx);
+        ++total;
+        conv = ctx->host_scalars.residual < crit;
+        if ((conv && i >= it_min) || (it_max >= 0 && i >= it_max)) break;
+      }
+    }
+    if (!conv) {
+      all = false;
+      break;
+    }
+  }
+  if (converged) *converged = all ? 1 : 0;
+  if (iterations) *iterations = total;
+  API_END
+}
+
+int sc_ldos_get(sc_ctx *ctx, double *ldos) {
+  if (!ctx || !ctx->S.keldysh || !ldos) return SC_ERR_ARG;
+  API_BEGIN
+  const size_t n = ctx->S.ldos_energies.size() * ctx->nn0();
+  CUDA_TRY(cudaMemcpyAsync(ldos, ctx->ldos_all.p, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  API_END
+}
+
+int sc_ldos_get_device(sc_ctx *ctx, double *d_ldos) {
+  if (!ctx || !ctx->S.keldysh || !d_ldos) return SC_ERR_ARG;
+  API_BEGIN
+  const size_t n = ctx->S.ldos_energies.size() * ctx->nn0();
+  CUDA_TRY(cudaMemcpyAsync(d_ldos, ctx->ldos_all.p, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
   CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   API_END
 }
@@ -1927,6 +2224,10 @@ int sc_boundary_initial(sc_ctx *ctx) {
 
 int sc_angle_greens(sc_ctx *ctx, int angle, double *f, double *g_re, double *i_re) {
   if (!ctx || angle < 0 || angle >= ctx->S.n_angles) return SC_ERR_ARG;
+  if (ctx->S.keldysh) {
+    ctx->err = "sc_angle_greens: not available on an LDOS context";
+    return SC_ERR_STATE;
+  }
   API_BEGIN
   const HostSetup &S = ctx->S;
   // The trajectory columns of this angle, swept on their own (unpaired) with
@@ -1971,8 +2272,8 @@ int sc_angle_greens(sc_ctx *ctx, int angle, double *f, double *g_re, double *i_r
 
 int sc_poisson(sc_ctx *ctx, const double *j, double *a_out) {
   if (!ctx || !j || !a_out) return SC_ERR_ARG;
-  if (!ctx->has_vp()) {
-    ctx->err = "sc_poisson: the configuration has no finite penetration depth";
+  if (!ctx->has_vp() || ctx->S.keldysh) {
+    ctx->err = "sc_poisson: the configuration has no finite penetration depth (or is an LDOS context)";
     return SC_ERR_STATE;
   }
   API_BEGIN

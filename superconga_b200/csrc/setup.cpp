@@ -546,7 +546,7 @@ struct BoundaryNode {
 
 }  // namespace
 
-std::string build_setup(const std::string &json, HostSetup &S) {
+std::string build_setup(const std::string &json, HostSetup &S, const SetupOverrides *ov) {
   JsonValue cfg;
   try {
     cfg = JsonValue::parse(json);
@@ -575,6 +575,11 @@ std::string build_setup(const std::string &json, HostSetup &S) {
   S.burnin = num["num_iterations_burnin"].as_int(0);
   S.it_min = num["num_iterations_min"].as_int(0);
   S.it_max = num["num_iterations_max"].as_int(-1);
+  if (ov) {
+    if (ov->n_angles > 0) S.n_angles = ov->n_angles;
+    if (ov->conv_crit > 0.0) S.conv_crit = ov->conv_crit;
+    if (ov->norm >= 0) S.norm = ov->norm;
+  }
   if (!(S.temperature > 0.0) || !(ppxi > 0.0) || !(cutoff > 0.0) || S.n_angles < 1)
     return "config: temperature, points_per_coherence_length, energy_cutoff and "
            "num_fermi_momenta must be positive";
@@ -691,6 +696,7 @@ std::string build_setup(const std::string &json, HostSetup &S) {
   ozaki_poles(S.ne, poles.data(), S.residues.data());
   S.e_im.resize(S.ne);
   for (int i = 0; i < S.ne; ++i) S.e_im[i] = poles[i] * S.temperature / (2.0 * M_PI);
+  S.e_re.assign(S.ne, 0.0);
 
   // Order parameter (src/simulation.cu:199-295).
   const JsonValue &ops = phys["order_parameter"];
@@ -1108,6 +1114,62 @@ std::string build_setup(const std::string &json, HostSetup &S) {
     }
   }
   return std::string();
+}
+
+std::string build_ldos_setup(const std::string &simulation_json, const std::string &postprocess_json,
+                             HostSetup &S) {
+  JsonValue pp;
+  try {
+    pp = JsonValue::parse(postprocess_json);
+  } catch (const std::exception &ex) {
+    return std::string("postprocess config: ") + ex.what();
+  }
+  const JsonValue &sp = pp["spectroscopy"], &num = pp["numerics"];
+  if (!sp.is_object() || !num.is_object())
+    return "postprocess config: 'spectroscopy' and 'numerics' are required";
+  // src/postprocess.cu:152-186: angles, criterion and norm come from the
+  // postprocess configuration, everything else from the loaded simulation.
+  SetupOverrides ov;
+  ov.n_angles = num["num_fermi_momenta"].as_int(-1);
+  ov.conv_crit = num["convergence_criterion"].as_double(-1.0);
+  const std::string norm = num["norm"].as_string("l2");
+  if (norm == "l1") ov.norm = NORM_L1;
+  else if (norm == "l2") ov.norm = NORM_L2;
+  else if (norm == "linf") ov.norm = NORM_LINF;
+  else return "postprocess config: norm type '" + norm + "' not understood";
+  if (ov.n_angles < 1) return "postprocess config: num_fermi_momenta must be positive";
+  const std::string e = build_setup(simulation_json, S, &ov);
+  if (!e.empty()) return e;
+  S.burnin = num["num_iterations_burnin"].as_int(0);
+  S.it_min = num["num_iterations_min"].as_int(0);
+  S.it_max = num["num_iterations_max"].as_int(-1);
+  // IntegrationIteratorKeldysh::initEnergies / initIterators
+  // (IntegrationIteratorKeldysh.h:91-160).
+  const double emin = sp["energy_min"].as_double(), emax = sp["energy_max"].as_double();
+  const int ne = sp["num_energies"].as_int(0);
+  const double delta = sp["energy_broadening"].as_double();
+  if (ne < 1) return "postprocess config: num_energies must be positive";
+  if (!(delta > 0.0)) return "postprocess config: energy_broadening must be positive";
+  const double step = ne > 1 ? (emax - emin) / (double)(ne - 1) : 0.0;
+  S.ldos_energies.resize(ne);
+  for (int i = 0; i < ne; ++i) S.ldos_energies[i] = emin + step * (double)i;
+  S.ldos_broadening = delta;
+  const int per = num["num_energies_per_block"].as_int(0);
+  S.ldos_block = per < 1 ? ne : std::min(per, ne);
+  S.ldos_n_blocks = (ne + S.ldos_block - 1) / S.ldos_block;
+  S.keldysh = 1;
+  S.ne = S.ldos_block;
+  S.e_im.assign(S.ne, delta);
+  S.residues.assign(S.ne, 0.0);
+  ldos_block_energies(S, 0, S.e_re);
+  return std::string();
+}
+
+void ldos_block_energies(const HostSetup &S, int b, std::vector<double> &e_re) {
+  const int n = (int)S.ldos_energies.size();
+  e_re.resize(S.ldos_block);
+  for (int i = 0; i < S.ldos_block; ++i)
+    e_re[i] = S.ldos_energies[std::min(b * S.ldos_block + i, n - 1)];
 }
 
 }  // namespace scb

@@ -52,8 +52,17 @@ struct HostSetup {
   AccelParams acc;
   std::vector<GeomComp> geom;
 
-  // Ozaki energies (imaginary parts) and residues.
-  std::vector<double> e_im, residues;
+  // Energies of the sweep, e = e_re + i e_im, and their residues.  The
+  // self-consistency path sums Ozaki poles (e_re = 0); the LDOS path takes one
+  // block of real energies with a common broadening (e_im = delta, residues 0).
+  std::vector<double> e_re, e_im, residues;
+
+  // LDOS postprocess (src/postprocess.cu:140-160,218-224;
+  // IntegrationIteratorKeldysh.h:91-170): all real energies and the block size.
+  int keldysh = 0;
+  std::vector<double> ldos_energies;
+  double ldos_broadening = 0.0;
+  int ldos_block = 0, ldos_n_blocks = 0;
 
   // Order-parameter components (ordered as the reference: dx2-y2, dxy, g, s).
   std::vector<int> sym;                    // 0 s, 1 dx2-y2, 2 dxy, 3 g
@@ -104,9 +113,26 @@ struct HostSetup {
   long long site_updates_per_iteration() const;  // 2 * ne * sum_a #{label > 0}
 };
 
+// Settings a postprocess configuration takes over from the simulation
+// configuration it loads (src/postprocess.cu:152-186).
+struct SetupOverrides {
+  int n_angles = -1;
+  double conv_crit = -1.0;
+  int norm = -1;
+};
+
 // Parses a reference JSON configuration and builds all static tables.
 // Returns an empty string on success, otherwise an error message.
-std::string build_setup(const std::string &json, HostSetup &out);
+std::string build_setup(const std::string &json, HostSetup &out,
+                        const SetupOverrides *ov = nullptr);
+
+// Setup of an LDOS postprocess: the simulation configuration of the loaded run
+// plus the postprocess configuration (spectroscopy and numerics sections).
+// The sweep energies are those of block 0.
+std::string build_ldos_setup(const std::string &simulation_json,
+                             const std::string &postprocess_json, HostSetup &out);
+// Energies of LDOS block b (a short last block repeats its final energy).
+void ldos_block_energies(const HostSetup &S, int b, std::vector<double> &e_re);
 
 // Individual pieces, exposed for tests.
 int num_ozaki_poles(double temperature, double cutoff);

@@ -279,3 +279,59 @@ class Setup:
         v = ctypes.c_longlong()
         _lib.load().sc_setup_site_updates(self._h, ctypes.byref(v))
         return v.value
+
+
+class LdosContext(Context):
+    """LDOS postprocess on the current CUDA device, shaped like the Context that
+    src/postprocess.cu builds (IntegrationIteratorKeldysh + ComputeLDOS).
+
+    ``simulation`` is the simulation configuration of the loaded run and
+    ``postprocess`` the postprocess configuration.  Load the converged state
+    with ``set_state`` (A in internal units), then ``run`` (runPostprocess) or
+    ``begin_block`` / ``burn_in`` / ``iterate`` step by step; ``ldos`` returns
+    [n_energies][N0][N0].
+    """
+
+    def __init__(self, simulation: dict | str, postprocess: dict | str, mode: str = "fp64"):
+        sim = simulation if isinstance(simulation, str) else json.dumps(simulation)
+        pp = postprocess if isinstance(postprocess, str) else json.dumps(postprocess)
+        lib = _lib.load()
+        h = ctypes.c_void_p()
+        _lib.check(lib.sc_ldos_create(sim.encode(), pp.encode(), MODES[mode], ctypes.byref(h)))
+        self._h = h
+        self.mode = mode
+        ints = [ctypes.c_int() for _ in range(5)]
+        _lib.check(lib.sc_get_dims(h, *[ctypes.byref(i) for i in ints]), h)
+        self.dims = Dims(*[i.value for i in ints])
+        ld = [ctypes.c_int() for _ in range(3)]
+        _lib.check(lib.sc_ldos_dims(h, *[ctypes.byref(i) for i in ld]), h)
+        self.n_ldos_energies, self.per_block, self.n_blocks = (i.value for i in ld)
+
+    def energies(self):
+        e = np.zeros(self.n_ldos_energies)
+        d = ctypes.c_double()
+        self._check(_lib.load().sc_ldos_energies(self._h, _p(e), ctypes.byref(d)))
+        return e, d.value
+
+    def begin_block(self, block: int):
+        self._check(_lib.load().sc_ldos_begin_block(self._h, int(block)))
+
+    def iterate(self, n: int = 1):
+        """n LDOS iterations of the current block; returns (residual, converged)."""
+        r = ctypes.c_double()
+        c = ctypes.c_int()
+        self._check(_lib.load().sc_ldos_iterate(self._h, int(n), ctypes.byref(r), ctypes.byref(c)))
+        return r.value, bool(c.value)
+
+    def run(self, burn_in: int, it_min: int, it_max: int):
+        """runPostprocess: returns (converged, total iterations)."""
+        c = ctypes.c_int()
+        it = ctypes.c_int()
+        self._check(_lib.load().sc_ldos_run(self._h, int(burn_in), int(it_min), int(it_max),
+                                            ctypes.byref(c), ctypes.byref(it)))
+        return bool(c.value), it.value
+
+    def ldos(self):
+        out = np.zeros((self.n_ldos_energies, self.dims.n0, self.dims.n0))
+        self._check(_lib.load().sc_ldos_get(self._h, _p(out)))
+        return out

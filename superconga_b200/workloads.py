@@ -100,11 +100,12 @@ def c2() -> dict:
 
 
 def c2p() -> dict:
-    """The c2 grain at 10 points/xi0 with 64 angles: a small case of the same
-    kernels (about 2 GB of sweep scratch) for detailed profiler captures."""
+    """The c2 grain at 10 points/xi0 with 128 angles: a small case of the same
+    kernels (about 4 GB of FP64 sweep scratch, at least one full wave of
+    resident blocks in both precisions) for detailed profiler captures."""
     cfg = c2()
     cfg["numerics"]["points_per_coherence_length"] = 10.0
-    cfg["numerics"]["num_fermi_momenta"] = 64
+    cfg["numerics"]["num_fermi_momenta"] = 128
     return cfg
 
 

@@ -101,3 +101,28 @@ def seeded_state(n_comp: int, n0: int, delta_bulk: float, seed: int, noise: floa
             d[c, 1] = delta_bulk * noise * rng.standard_normal((n0, n0))
     a = a_scale * rng.standard_normal((2, n0, n0))
     return d, a
+
+
+def ldos_postprocess(delta0: float, n_energies: int = 12, per_block: int = 8, n_angles: int = 32,
+                     broadening: float = 0.05, crit: float = 1e-5) -> dict:
+    """Postprocess configuration (examples/*/postprocess_config.json schema):
+    energies uniform in [-2 delta0, 2 delta0]; a block size that leaves a short
+    last block when n_energies is not a multiple of it."""
+    return {
+        "spectroscopy": {"energy_min": -2.0 * delta0, "energy_max": 2.0 * delta0,
+                         "num_energies": n_energies, "energy_broadening": broadening},
+        "numerics": {"convergence_criterion": crit, "norm": "l2", "num_energies_per_block": per_block,
+                     "num_fermi_momenta": n_angles, "num_iterations_burnin": 2,
+                     "num_iterations_min": 0, "num_iterations_max": 60},
+        "misc": {"data_format": "csv", "load_path": "", "save_path": "", "verbose": False},
+    }
+
+
+def bcs_dos(energy: np.ndarray, broadening: float, delta: float) -> np.ndarray:
+    """Bulk s-wave density of states Re[e / sqrt(e^2 - delta^2)], e = E + i delta_b
+    (retarded branch: the root with positive imaginary part times sign)."""
+    e = energy + 1j * broadening
+    root = np.sqrt(e * e - delta * delta + 0j)
+    root = np.where(np.imag(root) * np.sign(np.real(e) + 1e-300) < 0, -root, root)
+    root = np.where(np.real(e / root) < 0, -root, root)
+    return np.real(e / root)
