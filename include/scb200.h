@@ -191,6 +191,42 @@ int sc_ldos_run(sc_ctx *ctx, int burnin, int it_min, int it_max, int *converged,
 int sc_ldos_get(sc_ctx *ctx, double *ldos);
 int sc_ldos_get_device(sc_ctx *ctx, double *d_ldos);
 
+/* ---- batched grains -------------------------------------------------------- */
+
+/* Many independent grains advanced together: one context per configuration
+ * (each its own Context in the reference, src/simulation.cu:95-537, run one by
+ * one there), with a shared pool for the sweep work buffers.  Every call of
+ * sc_batch_compute runs one self-consistency iteration of each grain that has
+ * not finished (converged and at least num_iterations_min, or
+ * num_iterations_max reached, each grain by its own configuration); a grain
+ * that finishes leaves the batch.  The Riccati sweep of all grains of a wave
+ * (the grains whose work buffers fit the pool together) is one persistent
+ * launch; from the second iteration on, the iteration is a CUDA graph. */
+typedef struct sc_batch sc_batch;
+int sc_batch_create(const char *const *configs, int n, int mode, sc_batch **out);
+int sc_batch_destroy(sc_batch *b);
+const char *sc_batch_last_error(const sc_batch *b);
+int sc_batch_size(const sc_batch *b, int *n);
+/* The context of grain i (owned by the batch: set its state, read its
+ * results and scalars through the sc_* calls above; do not destroy it). */
+int sc_batch_grain(sc_batch *b, int i, sc_ctx **ctx);
+/* Up to n iterations of the active grains; *n_active: grains still running. */
+int sc_batch_compute(sc_batch *b, int n, int *n_active);
+/* Per grain: still active, iterations done, last residual (arrays of size n). */
+int sc_batch_status(const sc_batch *b, int *active, int *iterations, double *residual);
+/* CUDA-graph replay of the iteration on (default) or off. */
+int sc_batch_set_graph(sc_batch *b, int enable);
+/* Mapping of the persistent sweep: 2^log_groups threads per trajectory column
+ * and the resident-block variant minb (1: up to 255 registers per thread,
+ * 4: at most 128).  sc_batch_autotune times every feasible choice on the
+ * current state (after at least one iteration) and keeps the fastest. */
+int sc_batch_config(sc_batch *b, int log_groups, int minb);
+int sc_batch_get_config(const sc_batch *b, int *log_groups, int *minb, int *n_waves);
+int sc_batch_autotune(sc_batch *b, int *log_groups, int *minb, double *best_ms);
+/* Device time of the sweeps of all waves (average of `repeats`), state unchanged. */
+int sc_batch_time_sweeps(sc_batch *b, int repeats, double *ms);
+int sc_batch_launch_count(const sc_batch *b, long long *count);
+
 /* Measures the FP64 (precision 64) or FP32 (precision 32) FMA throughput of
  * the current device in FLOP/s: the CUDA-core denominator of the sweep's
  * compute roofline (the reference has no counterpart; a measurement aid). */

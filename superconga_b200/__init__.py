@@ -3,9 +3,10 @@
 The engine (libscb200.so, C ABI in include/scb200.h) runs the Riccati sweep,
 Green accumulation, specular boundary condition, vector-potential Poisson
 solve and accelerators as CUDA kernels for sm_100a.  ``Context`` is the Python
-face of one engine handle; ``LdosContext`` runs the LDOS postprocess.
+face of one engine handle; ``LdosContext`` runs the LDOS postprocess and
+``Batch`` advances many grains together.
 """
-from .engine import Context, Dims, LdosContext, Setup  # noqa: F401
+from .engine import Batch, Context, Dims, LdosContext, Setup  # noqa: F401
 from ._lib import EngineError, LIB_PATH, load  # noqa: F401
 
-__all__ = ["Context", "Dims", "LdosContext", "Setup", "EngineError", "LIB_PATH", "load"]
+__all__ = ["Batch", "Context", "Dims", "LdosContext", "Setup", "EngineError", "LIB_PATH", "load"]

@@ -54,6 +54,20 @@ SIGNATURES = {
     "sc_ldos_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _c_int_p, _c_int_p]),
     "sc_ldos_get": (ctypes.c_int, [ctypes.c_void_p, _c_double_p]),
     "sc_ldos_get_device": (ctypes.c_int, [ctypes.c_void_p, _c_double_p]),
+    "sc_batch_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_char_p), ctypes.c_int, ctypes.c_int,
+                                       ctypes.POINTER(ctypes.c_void_p)]),
+    "sc_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "sc_batch_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "sc_batch_size": (ctypes.c_int, [ctypes.c_void_p, _c_int_p]),
+    "sc_batch_grain": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "sc_batch_compute": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _c_int_p]),
+    "sc_batch_status": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "sc_batch_set_graph": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "sc_batch_config": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "sc_batch_get_config": (ctypes.c_int, [ctypes.c_void_p, _c_int_p, _c_int_p, _c_int_p]),
+    "sc_batch_autotune": (ctypes.c_int, [ctypes.c_void_p, _c_int_p, _c_int_p, ctypes.POINTER(ctypes.c_double)]),
+    "sc_batch_time_sweeps": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
+    "sc_batch_launch_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]),
     "sc_measure_fma_peak": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "sc_setup_create": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p)]),
     "sc_setup_last_error": (ctypes.c_char_p, []),

@@ -33,12 +33,12 @@ def _sources():
 
 def _deps():
     return _sources() + glob.glob(os.path.join(CSRC, "*.hpp")) + glob.glob(os.path.join(CSRC, "*.cuh")) + [
-        os.path.join(ROOT, "include", "scb200.h"), os.path.abspath(__file__),
-        os.path.join(CSRC, "driver", "simulation_b200.cpp")]
+        os.path.join(ROOT, "include", "scb200.h"), os.path.abspath(__file__)] + glob.glob(
+        os.path.join(CSRC, "driver", "*"))
 
 
 def up_to_date() -> bool:
-    if not os.path.exists(LIB) or not os.path.exists(os.path.join(PKG, "bin", "simulation_b200")):
+    if not os.path.exists(LIB) or not all(os.path.exists(d) for d in DRIVERS.values()):
         return False
     t = os.path.getmtime(LIB)
     return all(os.path.getmtime(d) <= t for d in _deps())
@@ -74,19 +74,20 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     return LIB
 
 
-DRIVER_SRC = os.path.join(CSRC, "driver", "simulation_b200.cpp")
-DRIVER = os.path.join(PKG, "bin", "simulation_b200")
+DRIVERS = {name: os.path.join(PKG, "bin", name) for name in ("simulation_b200", "postprocess_b200")}
+DRIVER = DRIVERS["simulation_b200"]
 
 
-def build_driver(verbose: bool = False) -> str:
-    """The drop-in simulation executable, linked against libscb200.so."""
-    os.makedirs(os.path.dirname(DRIVER), exist_ok=True)
-    cmd = ["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"), DRIVER_SRC, "-o", DRIVER,
-           "-L", PKG, "-lscb200", "-Wl,-rpath,$ORIGIN/.."]
-    if verbose:
-        print(" ".join(cmd), flush=True)
-    subprocess.check_call(cmd)
-    return DRIVER
+def build_driver(verbose: bool = False) -> None:
+    """The drop-in simulation and postprocess executables, linked against libscb200.so."""
+    for name, exe in DRIVERS.items():
+        os.makedirs(os.path.dirname(exe), exist_ok=True)
+        cmd = ["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"),
+               os.path.join(CSRC, "driver", name + ".cpp"), "-o", exe,
+               "-L", PKG, "-lscb200", "-Wl,-rpath,$ORIGIN/.."]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.check_call(cmd)
 
 
 if __name__ == "__main__":

@@ -15,151 +15,12 @@
 //   (CSVSimulationIterationWriter.h:42-101).
 // The optional key b200.precision selects "fp64" (default) or "mixed".
 // Exit status EXIT_SUCCESS / EXIT_FAILURE as the reference driver.
-#include <algorithm>
-#include <cmath>
-#include <cstdio>
-#include <cstdlib>
-#include <filesystem>
-#include <fstream>
-#include <iomanip>
-#include <iostream>
-#include <map>
 #include <random>
-#include <sstream>
-#include <string>
-#include <vector>
 
-#include "../json.hpp"
+#include "common.hpp"
 #include "scb200.h"
 
-namespace fs = std::filesystem;
-
-namespace {
-
-constexpr double EULER_GAMMA = 0.57721566490153286060651209008240243;
-
-// computeOrderParameterBulkSWave (OrderParameterBulk.h:88-221).
-double bulk_s_wave(double t) {
-  const double eps = 2.220446049250313e-16;
-  if (t >= 1.0) return 0.0;
-  const double s_bulk = 0.5 * std::exp(-EULER_GAMMA);
-  if (t < eps) return s_bulk;
-  const int ne = (int)(100.0 / t - 0.5) + 1;
-  double es = 0.0;
-  for (int n = ne - 1; n >= 0; --n) es += 1.0 / (t * ((double)n + 0.5));
-  const double coupling = 1.0 / (std::log(t) / t + es);
-  auto resid = [&](double op) {
-    double integ = 0.0;
-    for (int n = ne - 1; n >= 0; --n) integ += 1.0 / std::hypot(op, t * ((double)n + 0.5));
-    return op * (integ * coupling - 1.0);
-  };
-  double op = s_bulk * std::sqrt(1.0 - t * t * t);
-  double ops[2] = {op, std::sqrt(op)}, rs[2] = {resid(ops[0]), resid(ops[1])};
-  for (int it = 0; it < 10; ++it) {
-    const double w = 1.0 / (1.0 - (ops[0] / ops[1]) / (rs[0] / rs[1]));
-    op = (1.0 - w) * ops[0] + w * ops[1];
-    const double r = resid(op);
-    if (std::fabs(r / op) < 10.0 * eps) break;
-    const int k = std::fabs(rs[0]) > std::fabs(rs[1]) ? 0 : 1;
-    ops[k] = op;
-    rs[k] = r;
-  }
-  return op;
-}
-
-// One CSV file as column name -> values (CSVReader.h).
-bool read_csv(const fs::path &p, std::map<std::string, std::vector<double>> &cols) {
-  std::ifstream in(p);
-  if (!in.good()) return false;
-  std::string line;
-  if (!std::getline(in, line)) return false;
-  std::vector<std::string> names;
-  {
-    std::stringstream ss(line);
-    std::string cell;
-    while (std::getline(ss, cell, ',')) names.push_back(cell);
-  }
-  while (std::getline(in, line)) {
-    if (line.empty()) continue;
-    std::stringstream ss(line);
-    std::string cell;
-    size_t k = 0;
-    while (std::getline(ss, cell, ',') && k < names.size()) cols[names[k++]].push_back(std::atof(cell.c_str()));
-  }
-  return true;
-}
-
-// CSVGridWriter::saveInternal layout: x_idx,y_idx,<fields...>, row-major y then x.
-bool write_grid(const fs::path &p, int n, const std::vector<std::string> &titles, bool is_complex,
-                const std::vector<const double *> &planes, bool integral = false) {
-  std::ofstream out(p);
-  if (!out.good()) return false;
-  out << "x_idx,y_idx,";
-  for (size_t k = 0; k < titles.size(); ++k) {
-    out << titles[k];
-    if (is_complex) out << "_re," << titles[k] << "_im";
-    if (k + 1 < titles.size()) out << ",";
-  }
-  out << "\n";
-  std::ostringstream oss;
-  for (int y = 0; y < n; ++y)
-    for (int x = 0; x < n; ++x) {
-      oss.str("");
-      oss << std::scientific << std::setprecision(8) << x << "," << y << ",";
-      const size_t i = (size_t)y * n + x;
-      for (size_t k = 0; k < planes.size(); ++k) {
-        if (integral) oss << (int)planes[k][i];
-        else oss << planes[k][i];
-        if (k + 1 < planes.size()) oss << ",";
-      }
-      out << oss.str() << "\n";
-    }
-  return out.good();
-}
-
-std::string json_number(double v) {
-  std::ostringstream o;
-  o << std::setprecision(17) << v;
-  return o.str();
-}
-
-// Serialises the parsed configuration back (simulation_config.json).
-void dump_json(std::ostream &o, const scb::JsonValue &v, int ind) {
-  const std::string pad(ind, ' ');
-  switch (v.kind()) {
-  case scb::JsonValue::Null: o << "null"; break;
-  case scb::JsonValue::Bool: o << (v.as_bool() ? "true" : "false"); break;
-  case scb::JsonValue::Number: o << json_number(v.as_double()); break;
-  case scb::JsonValue::String: o << "\"" << v.as_string() << "\""; break;
-  case scb::JsonValue::Array: {
-    o << "[";
-    for (size_t i = 0; i < v.size(); ++i) {
-      if (i) o << ", ";
-      dump_json(o, v[i], ind);
-    }
-    o << "]";
-    break;
-  }
-  case scb::JsonValue::Object: {
-    o << "{\n";
-    const auto keys = v.keys();
-    for (size_t i = 0; i < keys.size(); ++i) {
-      o << pad << "    \"" << keys[i] << "\": ";
-      dump_json(o, v[keys[i]], ind + 4);
-      o << (i + 1 < keys.size() ? ",\n" : "\n");
-    }
-    o << pad << "}";
-    break;
-  }
-  }
-}
-
-int fail(const std::string &m) {
-  std::cerr << "-- ERROR! " << m << std::endl;
-  return EXIT_FAILURE;
-}
-
-}  // namespace
+using namespace drv;
 
 int main(int argc, char *argv[]) {
   if (argc < 2) return fail("Please provide a config file.");

@@ -24,6 +24,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -236,18 +237,11 @@ __device__ __forceinline__ void site_step(uint8_t l, uint8_t l_entry, uint8_t l_
 // KEL: real energies e_re + i e_im (the LDOS path, IntegrationIteratorKeldysh.h
 // :219-389); instead of the energy sums, Im g of every energy is written to the
 // LDOS frame buffer (GreensFunctionStatic.h:66-90, ComputeLDOS.h:123-144).
-template <typename R, int EMAX, int MINB, bool KEL>
-__global__ void __launch_bounds__(128, MINB) k_sweep(const SweepArgs<R> A) {
-  __shared__ double s_res[64];  // Ozaki residues (at most 64 energies)
-  for (int e = threadIdx.x; e < A.ne && e < 64; e += blockDim.x) s_res[e] = A.res[e];
-  __syncthreads();
-  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-  const int item = tid >> A.log_groups;
-  const int g = tid & (A.groups - 1);
-  const int lane = threadIdx.x & 31;
-  const unsigned gmask = ((A.groups == 32) ? 0xffffffffu : ((1u << A.groups) - 1u))
-                         << (lane & ~(A.groups - 1));
-  if (item >= A.n_items) return;  // whole groups leave together (groups divide the warp)
+// One trajectory column (item) for thread g of its group; s_res holds the
+// residues of the energies.
+template <typename R, int EMAX, bool KEL>
+__device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double *s_res, int item,
+                                             int g, unsigned gmask) {
   const int4 it = A.items[item];
   const int a = it.x, x = it.y, lo = it.z, hi = it.w;
   const int n1 = A.n1, ne = A.ne;
@@ -423,6 +417,47 @@ __global__ void __launch_bounds__(128, MINB) k_sweep(const SweepArgs<R> A) {
         }
       }
     }
+  }
+}
+
+template <typename R, int EMAX, int MINB, bool KEL>
+__global__ void __launch_bounds__(128, MINB) k_sweep(const SweepArgs<R> A) {
+  __shared__ double s_res[64];  // residues (at most 64 energies)
+  for (int e = threadIdx.x; e < A.ne && e < 64; e += blockDim.x) s_res[e] = A.res[e];
+  __syncthreads();
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int item = tid >> A.log_groups;
+  const int g = tid & (A.groups - 1);
+  const int lane = threadIdx.x & 31;
+  const unsigned gmask = ((A.groups == 32) ? 0xffffffffu : ((1u << A.groups) - 1u))
+                         << (lane & ~(A.groups - 1));
+  if (item >= A.n_items) return;  // whole groups leave together (groups divide the warp)
+  sweep_column<R, EMAX, KEL>(A, s_res, item, g, gmask);
+}
+
+// The sweep of many grains in one persistent launch.  A work unit is one
+// warp's worth of trajectory columns (32 / G of them) of one grain; warps take
+// units from a global counter, longest columns first (the unit list is sorted
+// by the host), so ragged grains share the GPU without a tail per grain.  All
+// grains of a batch use the same G = 2^log_groups threads per column.
+template <typename R, int EMAX, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_sweep_batch(const SweepArgs<R> *__restrict__ args,
+                                                           const int2 *__restrict__ units, int n_units,
+                                                           int *counter, int log_groups) {
+  const int lane = threadIdx.x & 31;
+  const int groups = 1 << log_groups;
+  const int g = lane & (groups - 1);
+  const int sub = lane >> log_groups;
+  const unsigned gmask = ((groups == 32) ? 0xffffffffu : ((1u << groups) - 1u)) << (lane & ~(groups - 1));
+  for (;;) {
+    int u = 0;
+    if (lane == 0) u = atomicAdd(counter, 1);
+    u = __shfl_sync(0xffffffffu, u, 0);
+    if (u >= n_units) break;
+    const int2 wu = units[u];
+    const SweepArgs<R> &A = args[wu.x];
+    const int item = wu.y + sub;
+    if (item < A.n_items) sweep_column<R, EMAX, false>(A, A.res, item, g, gmask);
   }
 }
 
@@ -1158,6 +1193,12 @@ struct sc_ctx {
   DevArray<double> tmp_io;
   int nb_fin = 0, nb_bnd = 0, nb_vp = 0, nb_acc = 0;
 
+  // Work buffers of the sweep (scratch, fields, frame buffers): the
+  // context's own arrays, or a batch's shared pool (batch_member).
+  bool batch_member = false;
+  double *w_scratch = nullptr, *w_scratch2 = nullptr, *w_fg = nullptr, *w_gi = nullptr;
+  size_t need_scratch = 0, need_scratch2 = 0, need_frame = 0;  // bytes of each (frame: fg and gi each)
+
   // LDOS postprocess: frame buffer, block accumulator, all energies.
   DevArray<double> ldf, ldos_acc, ldos_all;
   int ldos_block = -1;  // block whose energies the sweep uses
@@ -1251,11 +1292,20 @@ SweepArgs<R> sweep_args(sc_ctx *c, const Chunk *ch, int burn_in) {
   A.e_im = c->e_im.p;
   A.res = c->res.p;
   A.ldf = c->ldf.p;
-  A.scratch = (Cx<R> *)c->scratch.p;
-  A.scratch2 = c->scratch2.p;
-  A.fg = (double2 *)c->fg.p;
-  A.gi = (double2 *)c->gi.p;
+  A.scratch = (Cx<R> *)c->w_scratch;
+  A.scratch2 = c->w_scratch2;
+  A.fg = (double2 *)c->w_fg;
+  A.gi = (double2 *)c->w_gi;
   return A;
+}
+
+template <typename R>
+void launch_frame_fields(sc_ctx *c, const Chunk &ch, const SweepArgs<R> &A) {
+  if (!A.n_items) return;
+  const int rows = 16;
+  dim3 grid(grid1(A.n_items, 128), (unsigned)((ch.kmax + rows - 1) / rows));
+  k_frame_fields<R><<<grid, 128, 0, c->stream>>>(A, rows);
+  check_launch(c);
 }
 
 template <typename R>
@@ -1264,12 +1314,7 @@ void launch_sweep(sc_ctx *c, const Chunk &ch, int burn_in) {
   const size_t threads = (size_t)A.n_items * c->groups;
   if (!threads) return;
   const unsigned blocks = grid1(threads, 128);
-  {
-    const int rows = 16;
-    dim3 grid(grid1(A.n_items, 128), (unsigned)((ch.kmax + rows - 1) / rows));
-    k_frame_fields<R><<<grid, 128, 0, c->stream>>>(A, rows);
-    check_launch(c);
-  }
+  launch_frame_fields<R>(c, ch, A);
   ProfScope prof(c, 0);
   // FP64 runs best with four resident blocks per SM (measured on B200).
   static const char *minb_env = std::getenv("SCB_SWEEP_MINB");
@@ -1396,6 +1441,24 @@ void accelerate(sc_ctx *c) {
   check_launch(c);
 }
 
+// Frame extension and rotation back of one swept chunk.
+void frame_to_reference(sc_ctx *c, const Chunk &ch) {
+  const HostSetup &S = c->S;
+  const int h0 = S.halo_angle_off[ch.a_begin], h1 = S.halo_angle_off[ch.a_end];
+  if (h1 > h0) {
+    k_halo<<<grid1(h1 - h0, 128), 128, 0, c->stream>>>(h1 - h0, h0, S.n1, c->halo_angle.p, ch.a_begin,
+                                                        c->halo_site.p, c->halo_off.p, c->halo_src.p,
+                                                        (double2 *)c->w_fg, (double2 *)c->w_gi);
+    check_launch(c);
+  }
+  dim3 blk(32, 8), grid((S.n0 + 31) / 32, (S.n0 + 7) / 8);
+  ProfScope prof(c, 1);
+  k_rotate_back<<<grid, blk, 0, c->stream>>>(S.n0, S.n1, S.nc, ch.a_begin, ch.a_end, c->ang.p,
+                                             (const double2 *)c->w_fg, (const double2 *)c->w_gi,
+                                             c->acc_d.p, c->acc_j.p, c->acc_fe.p);
+  check_launch(c);
+}
+
 template <typename R>
 void run_chunks_ldos(sc_ctx *c, int burn_in) {
   const HostSetup &S = c->S;
@@ -1432,38 +1495,42 @@ void run_chunks(sc_ctx *c, int burn_in) {
   for (const Chunk &ch : c->chunks) {
     const int nslots = ch.a_end - ch.a_begin;
     if (!burn_in) {
-      CUDA_TRY(cudaMemsetAsync(c->fg.p, 0, (size_t)nslots * nn1 * sizeof(double2), c->stream));
-      CUDA_TRY(cudaMemsetAsync(c->gi.p, 0, (size_t)nslots * nn1 * sizeof(double2), c->stream));
+      CUDA_TRY(cudaMemsetAsync(c->w_fg, 0, (size_t)nslots * nn1 * sizeof(double2), c->stream));
+      CUDA_TRY(cudaMemsetAsync(c->w_gi, 0, (size_t)nslots * nn1 * sizeof(double2), c->stream));
     }
     launch_sweep<R>(c, ch, burn_in);
     if (burn_in) continue;
-    const int h0 = S.halo_angle_off[ch.a_begin], h1 = S.halo_angle_off[ch.a_end];
-    if (h1 > h0) {
-      k_halo<<<grid1(h1 - h0, 128), 128, 0, c->stream>>>(h1 - h0, h0, S.n1, c->halo_angle.p, ch.a_begin,
-                                                          c->halo_site.p, c->halo_off.p, c->halo_src.p,
-                                                          (double2 *)c->fg.p, (double2 *)c->gi.p);
-      check_launch(c);
-    }
-    dim3 blk(32, 8), grid((S.n0 + 31) / 32, (S.n0 + 7) / 8);
-    ProfScope prof(c, 1);
-    k_rotate_back<<<grid, blk, 0, c->stream>>>(S.n0, S.n1, S.nc, ch.a_begin, ch.a_end, c->ang.p,
-                                               (const double2 *)c->fg.p, (const double2 *)c->gi.p,
-                                               c->acc_d.p, c->acc_j.p, c->acc_fe.p);
-    check_launch(c);
+    frame_to_reference(c, ch);
   }
 }
 
+// Context::compute in three parts: before the sweep (accelerator step,
+// extended order parameter, cleared accumulators), the sweep with the frame
+// rotation, and after it (finalize, boundary condition, vector potential).
 template <typename R>
-void compute_once(sc_ctx *c) {
-  const HostSetup &S = c->S;
-  const size_t nn = c->nn0();
+void compute_pre(sc_ctx *c) {
   if (!c->first_compute) accelerate(c);
   if (!c->boundary_initialized) boundary_initial<R>(c);
   extend_reference(c);
   c->acc_d.zero(c->stream);
   c->acc_j.zero(c->stream);
   c->acc_fe.zero(c->stream);
+}
+
+template <typename R>
+void compute_post(sc_ctx *c);
+
+template <typename R>
+void compute_once(sc_ctx *c) {
+  compute_pre<R>(c);
   run_chunks<R>(c, 0);
+  compute_post<R>(c);
+}
+
+template <typename R>
+void compute_post(sc_ctx *c) {
+  const HostSetup &S = c->S;
+  const size_t nn = c->nn0();
   // Finalize.
   {
     double *delta = c->xstate.p, *avec = c->xstate.p + (size_t)2 * S.nc * nn;
@@ -1575,7 +1642,8 @@ void plan_chunks(sc_ctx *c, std::vector<int4> &items) {
   cudaMemGetInfo(&free_b, &total_b);
   double budget_mb = 0.35 * (double)free_b / 1048576.0;
   if (const char *env = std::getenv("SCB_SCRATCH_MB")) budget_mb = std::atof(env);
-  const double budget = budget_mb * 1048576.0;
+  // A batch grain sweeps all its angles in one chunk (the batch pools memory).
+  const double budget = c->batch_member ? 1e300 : budget_mb * 1048576.0;
   const size_t per_row = (size_t)S.ne * c->esize() + 3 * sizeof(double);
   const size_t frame_slot = S.keldysh ? (size_t)n1 * n1 * S.ne * sizeof(double)
                                       : (size_t)n1 * n1 * 2 * sizeof(double2);
@@ -1781,16 +1849,29 @@ void upload_static(sc_ctx *c) {
     scr2 = std::max(scr2, ni * ch.kmax * 3);
     max_slots = std::max(max_slots, ch.a_end - ch.a_begin);
   }
-  c->scratch.alloc(scr / sizeof(double) + 1);
-  c->scratch2.alloc(scr2 + 1);
-  if (S.keldysh) {
+  c->need_scratch = scr + 8;
+  c->need_scratch2 = (scr2 + 1) * sizeof(double);
+  c->need_frame = (size_t)max_slots * n1 * n1 * 2 * sizeof(double);
+  if (c->batch_member) {
+    // Work buffers come from the batch's pool.
+  } else if (S.keldysh) {
+    c->scratch.alloc(scr / sizeof(double) + 1);
+    c->scratch2.alloc(scr2 + 1);
+    c->w_scratch = c->scratch.p;
+    c->w_scratch2 = c->scratch2.p;
     c->ldf.alloc((size_t)max_slots * S.ne * n1 * n1);
     c->ldos_acc.alloc((size_t)S.ne * nn);
     c->ldos_all.alloc((size_t)S.ldos_n_blocks * S.ldos_block * nn);
     c->ldos_all.zero(s);
   } else {
+    c->scratch.alloc(scr / sizeof(double) + 1);
+    c->scratch2.alloc(scr2 + 1);
+    c->w_scratch = c->scratch.p;
+    c->w_scratch2 = c->scratch2.p;
     c->fg.alloc((size_t)max_slots * n1 * n1 * 2);
     c->gi.alloc((size_t)max_slots * n1 * n1 * 2);
+    c->w_fg = c->fg.p;
+    c->w_gi = c->gi.p;
   }
   c->nb_fin = std::min<int>(592, (int)grid1(nn, REDUCE_THREADS));
   c->nb_bnd = 296;
@@ -2242,8 +2323,8 @@ int sc_angle_greens(sc_ctx *ctx, int angle, double *f, double *g_re, double *i_r
   }
   const size_t nn1 = (size_t)S.n1 * S.n1;
   extend_reference(ctx);
-  CUDA_TRY(cudaMemsetAsync(ctx->fg.p, 0, nn1 * sizeof(double2), ctx->stream));
-  CUDA_TRY(cudaMemsetAsync(ctx->gi.p, 0, nn1 * sizeof(double2), ctx->stream));
+  CUDA_TRY(cudaMemsetAsync(ctx->w_fg, 0, nn1 * sizeof(double2), ctx->stream));
+  CUDA_TRY(cudaMemsetAsync(ctx->w_gi, 0, nn1 * sizeof(double2), ctx->stream));
   if (!cols.empty()) {
     // Place the columns at the front of the item array (restored below).
     std::vector<int4> saved(cols.size());
@@ -2256,8 +2337,8 @@ int sc_angle_greens(sc_ctx *ctx, int angle, double *f, double *g_re, double *i_r
     CUDA_TRY(cudaMemcpy(ctx->items.p, saved.data(), cols.size() * sizeof(int4), cudaMemcpyHostToDevice));
   }
   std::vector<double2> hf(nn1), hg(nn1);
-  CUDA_TRY(cudaMemcpyAsync(hf.data(), ctx->fg.p, nn1 * sizeof(double2), cudaMemcpyDeviceToHost, ctx->stream));
-  CUDA_TRY(cudaMemcpyAsync(hg.data(), ctx->gi.p, nn1 * sizeof(double2), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaMemcpyAsync(hf.data(), ctx->w_fg, nn1 * sizeof(double2), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaMemcpyAsync(hg.data(), ctx->w_gi, nn1 * sizeof(double2), cudaMemcpyDeviceToHost, ctx->stream));
   CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   for (size_t i = 0; i < nn1; ++i) {
     if (f) {
@@ -2353,6 +2434,503 @@ int sc_profile_read(sc_ctx *ctx, int kernel, double *total_ms, long long *launch
 int sc_launch_count(const sc_ctx *ctx, long long *count) {
   if (!ctx || !count) return SC_ERR_ARG;
   *count = ctx->launches;
+  return SC_OK;
+}
+
+}  // extern "C"
+
+// ===================================================================== batch
+// Many independent grains advanced together (one iteration of every active
+// grain per call).  Each grain is an ordinary context (its own state, static
+// tables, accelerator and convergence) whose sweep work buffers come from one
+// pool.  Grains are packed into waves that fit the pool; the Riccati sweep of a
+// wave is ONE persistent launch over the columns of all its grains, longest
+// columns first.  After the first iteration the whole iteration (all waves and
+// all per-grain kernels) is captured once in a CUDA graph and replayed until a
+// grain converges and leaves the active set.
+struct sc_batch {
+  std::vector<sc_ctx *> grains;
+  int mode = SC_MODE_FP64;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  int log_groups = 2;  // threads per trajectory column: 2^log_groups
+  int minb = 1;        // resident-block variant of the persistent sweep
+  int n_sm = 148;
+  std::vector<char> active;
+  std::vector<int> iterations;
+  DevArray<double> pool;
+  size_t pool_bytes = 0;
+  struct Wave {
+    std::vector<int> grains;
+    DevArray<int2> units;
+    int n_units = 0;
+    DevArray<unsigned char> args;  // SweepArgs<R> of the wave's grains
+  };
+  std::vector<std::unique_ptr<Wave>> waves;
+  DevArray<int> counters;
+  DevArray<const Scalars *> scalar_src;
+  DevArray<Scalars> scalars;  // gathered [grain] after every iteration
+  std::vector<Scalars> host_scalars;
+  bool use_graph = true;
+  cudaGraphExec_t exec = nullptr;
+  bool graph_dirty = true;
+  long long launches = 0;           // batch-level launches issued eagerly or at capture
+  long long graph_launches = 0;     // kernel launches in the captured iteration
+  long long replayed_launches = 0;  // launches executed through graph replays
+  long long captured_launches = 0;  // launches recorded into graphs (not run at capture)
+  ~sc_batch() {
+    if (exec) cudaGraphExecDestroy(exec);
+    for (sc_ctx *c : grains) delete c;
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+__global__ void k_gather_scalars(int n, const Scalars *const *src, Scalars *dst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = *src[i];
+}
+
+size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+size_t grain_footprint(const sc_ctx *c) {
+  return align256(c->need_scratch) + align256(c->need_scratch2) + 2 * align256(c->need_frame);
+}
+
+// Packs the active grains into waves (largest first, first fit) and points
+// every grain's work buffers into the pool at its wave offset.
+template <typename R>
+void batch_plan(sc_batch *b) {
+  std::vector<int> order;
+  for (int g = 0; g < (int)b->grains.size(); ++g)
+    if (b->active[g]) order.push_back(g);
+  std::sort(order.begin(), order.end(), [&](int x, int y) {
+    return grain_footprint(b->grains[x]) > grain_footprint(b->grains[y]);
+  });
+  std::vector<size_t> used;
+  std::vector<std::vector<int>> members;
+  for (int g : order) {
+    const size_t f = grain_footprint(b->grains[g]);
+    size_t w = 0;
+    while (w < used.size() && used[w] + f > b->pool_bytes) ++w;
+    if (w == used.size()) {
+      used.push_back(0);
+      members.emplace_back();
+    }
+    sc_ctx *c = b->grains[g];
+    char *base = (char *)b->pool.p + used[w];
+    c->w_scratch = (double *)base;
+    base += align256(c->need_scratch);
+    c->w_scratch2 = (double *)base;
+    base += align256(c->need_scratch2);
+    c->w_fg = (double *)base;
+    base += align256(c->need_frame);
+    c->w_gi = (double *)base;
+    used[w] += f;
+    members[w].push_back(g);
+  }
+  b->waves.clear();
+  const int G = 1 << b->log_groups, per_warp = 32 >> b->log_groups;
+  for (auto &m : members) {
+    auto wv = std::make_unique<sc_batch::Wave>();
+    wv->grains = m;
+    std::vector<SweepArgs<R>> args;
+    std::vector<std::pair<int, int2>> keyed;  // (column length, unit)
+    for (int k = 0; k < (int)m.size(); ++k) {
+      sc_ctx *c = b->grains[m[k]];
+      c->groups = G;
+      c->log_groups = b->log_groups;
+      c->ept = (c->S.ne + G - 1) / G;
+      const Chunk &ch = c->chunks[0];
+      args.push_back(sweep_args<R>(c, &ch, 0));
+      const int n = ch.item_end - ch.item_begin;
+      std::vector<int4> items(n);
+      if (n)
+        CUDA_TRY(cudaMemcpy(items.data(), c->items.p + ch.item_begin, n * sizeof(int4), cudaMemcpyDeviceToHost));
+      for (int i = 0; i < n; i += per_warp) {
+        int len = 0;
+        for (int j = i; j < std::min(n, i + per_warp); ++j) len = std::max(len, items[j].w - items[j].z + 1);
+        keyed.push_back({len, make_int2(k, i)});
+      }
+    }
+    std::stable_sort(keyed.begin(), keyed.end(), [](const auto &x, const auto &y) { return x.first > y.first; });
+    std::vector<int2> units;
+    for (auto &kv : keyed) units.push_back(kv.second);
+    wv->n_units = (int)units.size();
+    wv->units.upload(units, b->stream);
+    std::vector<unsigned char> raw(args.size() * sizeof(SweepArgs<R>));
+    std::memcpy(raw.data(), args.data(), raw.size());
+    wv->args.upload(raw, b->stream);
+    b->waves.push_back(std::move(wv));
+  }
+  b->counters.alloc(std::max<size_t>(1, b->waves.size()));
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  b->graph_dirty = true;
+}
+
+template <typename R>
+void launch_batch_sweep(sc_batch *b, sc_batch::Wave &w, int wi) {
+  const SweepArgs<R> *args = (const SweepArgs<R> *)w.args.p;
+  int *counter = b->counters.p + wi;
+  CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(int), b->stream));
+  int ept = 0;
+  for (int g : w.grains) ept = std::max(ept, b->grains[g]->ept);
+  auto run = [&](auto kernel) {
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 128, 0);
+    const int blocks = std::max(1, per_sm) * b->n_sm;
+    kernel<<<blocks, 128, 0, b->stream>>>(args, w.units.p, w.n_units, counter, b->log_groups);
+  };
+  if (ept <= 4) {
+    if (b->minb == 4) run(k_sweep_batch<R, 4, 4>);
+    else run(k_sweep_batch<R, 4, 1>);
+  } else if (ept <= 8) {
+    run(k_sweep_batch<R, 8, 1>);
+  } else {
+    run(k_sweep_batch<R, 16, 1>);
+  }
+  b->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) throw EngineError(SC_ERR_CUDA, std::string("batch sweep launch: ") + cudaGetErrorString(e));
+}
+
+// The sweeps of all waves (with the per-grain frame fields before and the
+// frame rotation after each wave's launch).
+template <typename R>
+void batch_sweeps(sc_batch *b) {
+  const int nw = (int)b->waves.size();
+  for (int wi = 0; wi < nw; ++wi) {
+    sc_batch::Wave &w = *b->waves[wi];
+    for (int g : w.grains) {
+      sc_ctx *c = b->grains[g];
+      const Chunk &ch = c->chunks[0];
+      const size_t nn1 = (size_t)c->S.n1 * c->S.n1;
+      const int nslots = ch.a_end - ch.a_begin;
+      CUDA_TRY(cudaMemsetAsync(c->w_fg, 0, (size_t)nslots * nn1 * sizeof(double2), b->stream));
+      CUDA_TRY(cudaMemsetAsync(c->w_gi, 0, (size_t)nslots * nn1 * sizeof(double2), b->stream));
+      launch_frame_fields<R>(c, ch, sweep_args<R>(c, &ch, 0));
+    }
+    launch_batch_sweep<R>(b, w, wi);
+    for (int g : w.grains) frame_to_reference(b->grains[g], b->grains[g]->chunks[0]);
+  }
+}
+
+template <typename R>
+void batch_iteration(sc_batch *b) {
+  for (size_t g = 0; g < b->grains.size(); ++g)
+    if (b->active[g]) compute_pre<R>(b->grains[g]);
+  batch_sweeps<R>(b);
+  int n = 0;
+  for (size_t g = 0; g < b->grains.size(); ++g)
+    if (b->active[g]) {
+      compute_post<R>(b->grains[g]);
+      ++n;
+    }
+  k_gather_scalars<<<grid1(b->grains.size(), 128), 128, 0, b->stream>>>((int)b->grains.size(), b->scalar_src.p,
+                                                                          b->scalars.p);
+  b->launches++;
+}
+
+template <typename R>
+void batch_step(sc_batch *b) {
+  bool first = false;
+  for (size_t g = 0; g < b->grains.size(); ++g)
+    if (b->active[g] && (b->grains[g]->first_compute || !b->grains[g]->boundary_initialized)) first = true;
+  if (!b->use_graph || first) {
+    batch_iteration<R>(b);  // first iterations differ (no accelerator step, initial boundary)
+  } else {
+    if (b->graph_dirty || !b->exec) {
+      if (b->exec) {
+        cudaGraphExecDestroy(b->exec);
+        b->exec = nullptr;
+      }
+      cudaGraph_t graph = nullptr;
+      const long long launches0 = b->launches;
+      long long grain_launches0 = 0;
+      for (const sc_ctx *c : b->grains) grain_launches0 += c->launches;
+      CUDA_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+      try {
+        batch_iteration<R>(b);
+      } catch (...) {
+        cudaStreamEndCapture(b->stream, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        throw;
+      }
+      CUDA_TRY(cudaStreamEndCapture(b->stream, &graph));
+      b->graph_launches = b->launches - launches0;
+      for (const sc_ctx *c : b->grains) b->graph_launches += c->launches;
+      b->graph_launches -= grain_launches0;
+      b->captured_launches += b->graph_launches;  // counted at capture, run by replays
+      const cudaError_t e = cudaGraphInstantiate(&b->exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess) throw EngineError(SC_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+      b->graph_dirty = false;
+    }
+    CUDA_TRY(cudaGraphLaunch(b->exec, b->stream));
+    b->replayed_launches += b->graph_launches;
+  }
+  CUDA_TRY(cudaMemcpyAsync(b->host_scalars.data(), b->scalars.p, b->grains.size() * sizeof(Scalars),
+                           cudaMemcpyDeviceToHost, b->stream));
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  bool changed = false;
+  for (size_t g = 0; g < b->grains.size(); ++g) {
+    if (!b->active[g]) continue;
+    sc_ctx *c = b->grains[g];
+    c->host_scalars = b->host_scalars[g];
+    b->iterations[g]++;
+    const Scalars &s = c->host_scalars;
+    const bool conv = s.residual < c->S.conv_crit && s.conv_op && s.conv_j && s.conv_fe;
+    const bool done = (conv && b->iterations[g] >= c->S.it_min) ||
+                      (c->S.it_max >= 0 && b->iterations[g] >= c->S.it_max);
+    if (done) {
+      b->active[g] = 0;
+      changed = true;
+    }
+  }
+  if (changed) batch_plan<R>(b);
+}
+
+int batch_fail(sc_batch *b, const EngineError &e) {
+  if (b) b->err = e.msg;
+  else g_create_error = e.msg;
+  return e.code;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sc_batch_create(const char *const *configs, int n, int mode, sc_batch **out) {
+  if (!configs || n < 1 || !out || (mode != SC_MODE_FP64 && mode != SC_MODE_MIXED)) {
+    g_create_error = "sc_batch_create: bad argument";
+    return SC_ERR_ARG;
+  }
+  *out = nullptr;
+  sc_batch *b = new sc_batch();
+  b->mode = mode;
+  try {
+    CUDA_TRY(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    CUDA_TRY(cudaDeviceGetAttribute(&b->n_sm, cudaDevAttrMultiProcessorCount, dev));
+    for (int i = 0; i < n; ++i) {
+      if (!configs[i]) throw EngineError(SC_ERR_ARG, "null configuration");
+      sc_ctx *c = new sc_ctx();
+      b->grains.push_back(c);
+      c->mode = mode;
+      c->batch_member = true;
+      const std::string e = build_setup(configs[i], c->S);
+      if (!e.empty()) throw EngineError(SC_ERR_ARG, "grain " + std::to_string(i) + ": " + e);
+      if (c->S.nc > MAX_COMP) throw EngineError(SC_ERR_ARG, "at most 4 order-parameter components");
+      if (c->S.ne > 32) throw EngineError(SC_ERR_ARG, "grain " + std::to_string(i) + ": at most 32 Ozaki energies in a batch");
+      if (c->S.acc.kind == ACC_ANDERSON)
+        throw EngineError(SC_ERR_ARG, "accelerator 'anderson' is not available in this engine");
+      c->device = dev;
+      c->stream = b->stream;
+      upload_static(c);
+    }
+    // Pool: every grain's own footprint must fit; the pool holds as many
+    // grains per wave as 60% of the free memory allows.
+    size_t free_b = 0, total_b = 0;
+    CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+    size_t budget = (size_t)(0.6 * (double)free_b);
+    if (const char *env = std::getenv("SCB_BATCH_POOL_MB")) budget = (size_t)(std::atof(env) * 1048576.0);
+    size_t total = 0, largest = 0;
+    for (sc_ctx *c : b->grains) {
+      total += grain_footprint(c);
+      largest = std::max(largest, grain_footprint(c));
+    }
+    if (largest > budget) throw EngineError(SC_ERR_SIZE, "a grain's sweep buffers exceed the device memory budget");
+    b->pool_bytes = std::min(total, budget);
+    b->pool.alloc(b->pool_bytes / sizeof(double) + 1);
+    b->active.assign(n, 1);
+    b->iterations.assign(n, 0);
+    std::vector<const Scalars *> src(n);
+    for (int i = 0; i < n; ++i) src[i] = b->grains[i]->scalars.p;
+    b->scalar_src.upload(src, b->stream);
+    b->scalars.alloc(n);
+    b->host_scalars.resize(n);
+    // Threads per column: enough that no thread integrates more than four
+    // energies of the grain with the most energies.
+    int ne_max = 1;
+    for (sc_ctx *c : b->grains) ne_max = std::max(ne_max, c->S.ne);
+    b->log_groups = 0;
+    while (((ne_max + (1 << b->log_groups) - 1) >> b->log_groups) > 4 && b->log_groups < 3) b->log_groups++;
+    b->minb = mode == SC_MODE_FP64 ? 4 : 1;
+    if (mode == SC_MODE_FP64) batch_plan<double>(b);
+    else batch_plan<float>(b);
+  } catch (const EngineError &e) {
+    g_create_error = e.msg;
+    delete b;
+    return e.code;
+  } catch (const std::exception &e) {
+    g_create_error = e.what();
+    delete b;
+    return SC_ERR_ARG;
+  }
+  *out = b;
+  return SC_OK;
+}
+
+int sc_batch_destroy(sc_batch *b) {
+  if (!b) return SC_OK;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  delete b;
+  return SC_OK;
+}
+
+const char *sc_batch_last_error(const sc_batch *b) { return b ? b->err.c_str() : g_create_error.c_str(); }
+
+int sc_batch_size(const sc_batch *b, int *n) {
+  if (!b || !n) return SC_ERR_ARG;
+  *n = (int)b->grains.size();
+  return SC_OK;
+}
+
+int sc_batch_grain(sc_batch *b, int i, sc_ctx **ctx) {
+  if (!b || !ctx || i < 0 || i >= (int)b->grains.size()) return SC_ERR_ARG;
+  *ctx = b->grains[i];
+  return SC_OK;
+}
+
+int sc_batch_compute(sc_batch *b, int n, int *n_active) {
+  if (!b || n < 0) return SC_ERR_ARG;
+  try {
+    for (int i = 0; i < n; ++i) {
+      bool any = false;
+      for (char a : b->active) any = any || a;
+      if (!any) break;
+      if (b->mode == SC_MODE_FP64) batch_step<double>(b);
+      else batch_step<float>(b);
+    }
+    if (n_active) {
+      int k = 0;
+      for (char a : b->active) k += a;
+      *n_active = k;
+    }
+  } catch (const EngineError &e) {
+    return batch_fail(b, e);
+  }
+  return SC_OK;
+}
+
+int sc_batch_status(const sc_batch *b, int *active, int *iterations, double *residual) {
+  if (!b) return SC_ERR_ARG;
+  for (size_t g = 0; g < b->grains.size(); ++g) {
+    if (active) active[g] = b->active[g];
+    if (iterations) iterations[g] = b->iterations[g];
+    if (residual) residual[g] = b->grains[g]->host_scalars.residual;
+  }
+  return SC_OK;
+}
+
+int sc_batch_set_graph(sc_batch *b, int enable) {
+  if (!b) return SC_ERR_ARG;
+  b->use_graph = enable != 0;
+  b->graph_dirty = true;
+  return SC_OK;
+}
+
+int sc_batch_config(sc_batch *b, int log_groups, int minb) {
+  if (!b || log_groups < 0 || log_groups > 3 || (minb != 1 && minb != 4)) return SC_ERR_ARG;
+  int ne_max = 1;
+  for (sc_ctx *c : b->grains) ne_max = std::max(ne_max, c->S.ne);
+  if (((ne_max + (1 << log_groups) - 1) >> log_groups) > 16) return SC_ERR_ARG;
+  try {
+    CUDA_TRY(cudaStreamSynchronize(b->stream));
+    b->log_groups = log_groups;
+    b->minb = minb;
+    if (b->mode == SC_MODE_FP64) batch_plan<double>(b);
+    else batch_plan<float>(b);
+  } catch (const EngineError &e) {
+    return batch_fail(b, e);
+  }
+  return SC_OK;
+}
+
+int sc_batch_get_config(const sc_batch *b, int *log_groups, int *minb, int *n_waves) {
+  if (!b) return SC_ERR_ARG;
+  if (log_groups) *log_groups = b->log_groups;
+  if (minb) *minb = b->minb;
+  if (n_waves) *n_waves = (int)b->waves.size();
+  return SC_OK;
+}
+
+// Times the sweeps of all waves for the current configuration (no state
+// changes: the sweeps rewrite the same outgoing boundary values and frames).
+int sc_batch_time_sweeps(sc_batch *b, int repeats, double *ms) {
+  if (!b || repeats < 1 || !ms) return SC_ERR_ARG;
+  try {
+    for (size_t g = 0; g < b->grains.size(); ++g)
+      if (b->active[g] && !b->grains[g]->boundary_initialized)
+        throw EngineError(SC_ERR_STATE, "sc_batch_time_sweeps: run one iteration first");
+    cudaEvent_t e0, e1;
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    CUDA_TRY(cudaEventRecord(e0, b->stream));
+    for (int r = 0; r < repeats; ++r) {
+      if (b->mode == SC_MODE_FP64) batch_sweeps<double>(b);
+      else batch_sweeps<float>(b);
+    }
+    CUDA_TRY(cudaEventRecord(e1, b->stream));
+    CUDA_TRY(cudaEventSynchronize(e1));
+    float t = 0.0f;
+    cudaEventElapsedTime(&t, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = (double)t / repeats;
+  } catch (const EngineError &e) {
+    return batch_fail(b, e);
+  }
+  return SC_OK;
+}
+
+int sc_batch_launch_count(const sc_batch *b, long long *count) {
+  if (!b || !count) return SC_ERR_ARG;
+  long long k = b->launches + b->replayed_launches - b->captured_launches;
+  for (const sc_ctx *c : b->grains) k += c->launches;
+  *count = k;
+  return SC_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+// Autotuner of the persistent batch sweep: tries every feasible mapping of
+// trajectory columns to threads (2, 4 or 8 threads per column, i.e. 16, 8 or 4
+// columns per warp) and both resident-block variants (register budget of 255
+// or 128 per thread), times the sweeps of all waves for each on the current
+// state, keeps the fastest and returns it.
+int sc_batch_autotune(sc_batch *b, int *log_groups, int *minb, double *best_ms) {
+  if (!b) return SC_ERR_ARG;
+  int ne_max = 1;
+  for (sc_ctx *c : b->grains) ne_max = std::max(ne_max, c->S.ne);
+  int best_lg = b->log_groups, best_mb = b->minb;
+  double best = 1e300;
+  for (int lg = 1; lg <= 3; ++lg) {
+    const int ept = (ne_max + (1 << lg) - 1) >> lg;
+    if (ept > 16) continue;
+    for (int mb : {1, 4}) {
+      if (mb == 4 && ept > 4) continue;  // the 128-register variant only for <= 4 energies per thread
+      int st = sc_batch_config(b, lg, mb);
+      if (st != SC_OK) return st;
+      double ms = 0.0;
+      st = sc_batch_time_sweeps(b, 1, &ms);  // warm-up
+      if (st == SC_OK) st = sc_batch_time_sweeps(b, 2, &ms);
+      if (st != SC_OK) return st;
+      if (ms < best) {
+        best = ms;
+        best_lg = lg;
+        best_mb = mb;
+      }
+    }
+  }
+  const int st = sc_batch_config(b, best_lg, best_mb);
+  if (st != SC_OK) return st;
+  if (log_groups) *log_groups = best_lg;
+  if (minb) *minb = best_mb;
+  if (best_ms) *best_ms = best;
   return SC_OK;
 }
 

@@ -335,3 +335,107 @@ class LdosContext(Context):
         out = np.zeros((self.n_ldos_energies, self.dims.n0, self.dims.n0))
         self._check(_lib.load().sc_ldos_get(self._h, _p(out)))
         return out
+
+
+class _Grain(Context):
+    """Context view of one grain of a Batch (the batch owns the handle)."""
+
+    def __init__(self, handle: ctypes.c_void_p, batch: "Batch"):
+        self._h = handle
+        self._batch = batch
+        self.mode = batch.mode
+        ints = [ctypes.c_int() for _ in range(5)]
+        _lib.check(_lib.load().sc_get_dims(handle, *[ctypes.byref(i) for i in ints]), handle)
+        self.dims = Dims(*[i.value for i in ints])
+
+    def close(self):
+        self._h = None
+
+
+class Batch:
+    """Many independent grains advanced together on the current CUDA device.
+
+    ``grains[i]`` is a Context view of grain i (set its state, read its
+    results).  ``compute(n)`` runs up to n iterations of every grain that has
+    not finished (each converges, or stops, by its own configuration); the
+    sweep of all grains of a wave is one persistent launch and, from the second
+    iteration on, each iteration replays a CUDA graph.  ``autotune`` picks the
+    column-to-thread mapping and register variant of the persistent sweep.
+    """
+
+    def __init__(self, configs: list, mode: str = "mixed"):
+        texts = [c if isinstance(c, str) else json.dumps(c) for c in configs]
+        arr = (ctypes.c_char_p * len(texts))(*[t.encode() for t in texts])
+        lib = _lib.load()
+        h = ctypes.c_void_p()
+        st = lib.sc_batch_create(arr, len(texts), MODES[mode], ctypes.byref(h))
+        if st != 0:
+            raise _lib.EngineError(st, (lib.sc_batch_last_error(None) or b"").decode())
+        self._h = h
+        self.mode = mode
+        self.n = len(texts)
+        self.grains = []
+        for i in range(self.n):
+            g = ctypes.c_void_p()
+            self._check(lib.sc_batch_grain(h, i, ctypes.byref(g)))
+            self.grains.append(_Grain(g, self))
+
+    def _check(self, st: int):
+        if st != 0:
+            msg = _lib.load().sc_batch_last_error(self._h)
+            raise _lib.EngineError(st, (msg or b"").decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            for g in self.grains:
+                g.close()
+            _lib.load().sc_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def compute(self, n: int = 1) -> int:
+        """Up to n iterations of the active grains; returns the number still active."""
+        k = ctypes.c_int()
+        self._check(_lib.load().sc_batch_compute(self._h, int(n), ctypes.byref(k)))
+        return k.value
+
+    def status(self):
+        act = np.zeros(self.n, np.int32)
+        it = np.zeros(self.n, np.int32)
+        res = np.zeros(self.n)
+        self._check(_lib.load().sc_batch_status(self._h, _p(act), _p(it), _p(res)))
+        return act.astype(bool), it, res
+
+    def set_graph(self, enable: bool):
+        self._check(_lib.load().sc_batch_set_graph(self._h, int(bool(enable))))
+
+    def config(self, log_groups: int, minb: int):
+        self._check(_lib.load().sc_batch_config(self._h, int(log_groups), int(minb)))
+
+    def get_config(self):
+        v = [ctypes.c_int() for _ in range(3)]
+        self._check(_lib.load().sc_batch_get_config(self._h, *[ctypes.byref(x) for x in v]))
+        return tuple(x.value for x in v)
+
+    def autotune(self):
+        lg, mb, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        self._check(_lib.load().sc_batch_autotune(self._h, ctypes.byref(lg), ctypes.byref(mb), ctypes.byref(ms)))
+        return lg.value, mb.value, ms.value
+
+    def time_sweeps(self, repeats: int = 3) -> float:
+        ms = ctypes.c_double()
+        self._check(_lib.load().sc_batch_time_sweeps(self._h, int(repeats), ctypes.byref(ms)))
+        return ms.value
+
+    def launch_count(self) -> int:
+        k = ctypes.c_longlong()
+        self._check(_lib.load().sc_batch_launch_count(self._h, ctypes.byref(k)))
+        return k.value
+
+    def site_updates(self) -> np.ndarray:
+        return np.array([g.site_updates() for g in self.grains], np.int64)

@@ -130,6 +130,48 @@ def c5() -> dict:
     return cfg
 
 
+def c3_grains(n: int = 128, seed: int = 3, ppxi: float = 10.0):
+    """The batched workload: n seeded grains, half discs of radius U(4, 20) xi0
+    and half squares of side U(8, 40) xi0 at ppxi points/xi0; s- or
+    d_{x2-y2}-wave 50/50; T ~ U(0.1, 0.9); b ~ U(0, 0.1) B0 (flux from the
+    geometric area); kappa = 2; clip(32 round(w / 10 xi0), 32, 128) angles for a
+    grain of width w; Ozaki poles at the 16 pi T_c cutoff.  Returns the
+    configurations and their seeded initial states
+    Delta = Delta_bulk (1 + 0.01 N(0,1)) (no phase), A = 0."""
+    rng = np.random.default_rng(seed)
+    cfgs, states = [], []
+    for i in range(n):
+        disc = i < n // 2
+        size = rng.uniform(4.0, 20.0) if disc else rng.uniform(8.0, 40.0)
+        width = 2.0 * size if disc else size
+        sym = "s" if rng.uniform() < 0.5 else "dx2-y2"
+        t = float(rng.uniform(0.1, 0.9))
+        b = float(rng.uniform(0.0, 0.1))
+        na = int(min(128, max(32, 32 * round(width / 10.0))))
+        cfg = _base(t, ppxi, na, 2.0, 0.0)
+        if disc:
+            cfg["geometry"] = [{"disc": {"add": True, "radius": size, "center_x": 0.0, "center_y": 0.0}}]
+            area = math.pi * size * size
+        else:
+            cfg["geometry"] = [{"regular_polygon": {"add": True, "num_edges": 4, "side_length": size,
+                                                    "rotation": 0.0, "center_x": 0.0, "center_y": 0.0}}]
+            area = size * size
+        cfg["physics"]["order_parameter"] = {sym: {"critical_temperature": 1.0}}
+        cfg["physics"]["external_flux_quanta"] = b * area / math.pi
+        cfg["numerics"]["num_iterations_max"] = 400
+        cfgs.append(cfg)
+        states.append((sym, t, int(rng.integers(0, 2**31 - 1))))
+    return cfgs, states
+
+
+def c3_initial_state(cfg: dict, state: tuple, n0: int):
+    sym, t, s = state
+    rng = np.random.default_rng(s)
+    d = np.zeros((1, 2, n0, n0))
+    d[0, 0] = delta_bulk(t, sym) * (1.0 + 0.01 * rng.standard_normal((n0, n0)))
+    return d, np.zeros((2, n0, n0))
+
+
 WORKLOADS = {"c1": c1, "c2": c2, "c2p": c2p, "c4": c4, "c5": c5}
 SEEDS = {"c1": 1, "c2": 2, "c2p": 2, "c4": 4, "c5": 5}
 

@@ -1,0 +1,121 @@
+"""Batched grains: the persistent multi-grain sweep, the CUDA-graph replay and
+the autotuner give the results of the grains run one by one, and every grain
+converges on its own."""
+import numpy as np
+import pytest
+
+from tests import configs
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    scale = max(np.max(np.abs(b)), 1e-300)
+    return float(np.max(np.abs(np.asarray(a) - np.asarray(b))) / scale)
+
+
+def _grains():
+    cfgs = [configs.small_disc(), configs.small_square_d(), configs.chiral_annulus(),
+            configs.golden_disc("picard")]
+    states = []
+    from oracle import oracle as O
+    for i, c in enumerate(cfgs):
+        s = O.make_setup(c)
+        db = O.delta_bulk(s.temperature, s.symmetries[0])
+        states.append(configs.seeded_state(s.n_comp, s.n0, db, 10 + i, 0.05, True, 0.02))
+    return cfgs, states
+
+
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+def test_batch_matches_single(engine_lib, mode):
+    import superconga_b200 as sb
+    cfgs, states = _grains()
+    b = sb.Batch(cfgs, mode=mode)
+    singles = []
+    for c, (d, a), g in zip(cfgs, states, b.grains):
+        g.set_state(d, a)
+        e = sb.Context(c, mode=mode)
+        e.set_state(d, a)
+        e.compute(4)
+        singles.append(e)
+    b.compute(4)  # iteration 1 eager, 2-4 graph replays
+    tol = 1e-11 if mode == "fp64" else 1e-4
+    for g, e in zip(b.grains, singles):
+        d_b, j_b, a_b = g.results()
+        d_s, j_s, a_s = e.results()
+        assert _rel(d_b, d_s) < tol
+        assert _rel(j_b, j_s) < 100 * tol
+        assert abs(g.scalars()["free_energy"] - e.scalars()["free_energy"]) <= tol * abs(e.scalars()["free_energy"])
+    act, it, _ = b.status()
+    assert np.all(it == 4)
+    b.close()
+
+
+def test_batch_graph_equals_eager(engine_lib):
+    import superconga_b200 as sb
+    cfgs, states = _grains()
+    out = []
+    for graph in (True, False):
+        b = sb.Batch(cfgs, mode="fp64")
+        b.set_graph(graph)
+        for g, (d, a) in zip(b.grains, states):
+            g.set_state(d, a)
+        b.compute(3)
+        out.append([g.results()[0] for g in b.grains])
+        b.close()
+    for x, y in zip(*out):
+        assert np.array_equal(x, y)
+
+
+def test_batch_autotune(engine_lib):
+    import superconga_b200 as sb
+    cfgs, states = _grains()
+    b = sb.Batch(cfgs, mode="fp64")
+    for g, (d, a) in zip(b.grains, states):
+        g.set_state(d, a)
+    b.compute(1)
+    lg, mb, ms = b.autotune()
+    assert 1 <= lg <= 3 and mb in (1, 4) and ms > 0
+    assert b.get_config()[:2] == (lg, mb)
+    b.compute(2)
+    ref = []
+    for c, (d, a) in zip(cfgs, states):
+        e = sb.Context(c, mode="fp64")
+        e.set_state(d, a)
+        e.compute(3)
+        ref.append(e.results()[0])
+    for g, r in zip(b.grains, ref):
+        assert _rel(g.results()[0], r) < 1e-11
+    b.close()
+
+
+def test_batch_converges_independently(engine_lib):
+    """Grains leave the batch when they converge; the golden disc reaches the
+    reference's known free energy with two accelerators."""
+    import superconga_b200 as sb
+    from oracle import oracle as O
+    cfgs = [configs.golden_disc("congacc"), configs.golden_disc("barzilai-borwein")]
+    capped = configs.small_disc()
+    capped["numerics"]["num_iterations_max"] = 5
+    cfgs.append(capped)
+    for c in cfgs[:2]:
+        c["numerics"]["num_iterations_max"] = 100
+    b = sb.Batch(cfgs, mode="fp64")
+    for g in b.grains[:2]:
+        n0 = g.dims.n0
+        d = np.zeros((1, 2, n0, n0))
+        d[0, 0] = O.delta_bulk(0.5, "s")
+        g.set_state(d, np.zeros((2, n0, n0)))
+    s = O.make_setup(capped)
+    d, a = configs.seeded_state(1, s.n0, O.delta_bulk(0.5, "s"), 1, 0.01, False, 0.0)
+    b.grains[2].set_state(d, a)
+    left = b.compute(200)
+    assert left == 0
+    act, it, res = b.status()
+    assert not act.any()
+    assert it[2] == 5
+    for k in range(2):
+        assert res[k] < 1e-5 and it[k] < 100
+        fe = b.grains[k].scalars()["free_energy_per_area"]
+        assert abs(fe - configs.GOLDEN_FREE_ENERGY_PER_AREA) <= 1e-3 * abs(configs.GOLDEN_FREE_ENERGY_PER_AREA)
+    b.close()

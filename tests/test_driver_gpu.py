@@ -66,3 +66,61 @@ def test_driver_bad_config(engine_lib, tmp_path):
     r = _run(cfg, tmp_path)
     assert r.returncode != 0
     assert "norm" in r.stderr
+
+
+PP_EXE = os.path.join(ROOT, "superconga_b200", "bin", "postprocess_b200")
+
+
+def test_postprocess_driver(engine_lib, tmp_path):
+    """simulation_b200 writes a run, postprocess_b200 reads it back
+    (src/postprocess.cu:86-360) and writes ldos.csv; the LDOS agrees with the
+    oracle's postprocess of the same files."""
+    import numpy as np
+    from oracle import oracle as O
+    cfg = configs.small_disc()
+    cfg["physics"]["order_parameter"]["s"].update({"initial_noise_stddev": 0.0,
+                                                  "initial_phase_shift": 0.0, "vortices": []})
+    cfg["numerics"].update({"num_iterations_burnin": 0, "num_iterations_min": 0,
+                            "num_iterations_max": 4})
+    sim_out = tmp_path / "sim"
+    cfg["misc"] = {"save_path": str(sim_out), "save_frequency": -1, "load_path": "",
+                   "verbose": False, "data_format": "csv"}
+    r = _run(cfg, tmp_path)
+    assert r.returncode == 0, r.stderr
+    db = O.delta_bulk(0.5, "s")
+    pp = configs.ldos_postprocess(db, n_energies=6, per_block=4, n_angles=16, crit=1e-6)
+    pp["misc"] = {"data_format": "csv", "load_path": str(sim_out), "save_path": str(tmp_path / "pp"),
+                  "verbose": False}
+    ppath = tmp_path / "postprocess_config.json"
+    ppath.write_text(json.dumps(pp))
+    r = subprocess.run([PP_EXE, str(ppath)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    for name in ("ldos.csv", "postprocess_config.json", "postprocess_convergence.csv"):
+        assert (tmp_path / "pp" / name).exists(), name
+    rows = list(csv.reader(open(tmp_path / "pp" / "ldos.csv")))
+    assert rows[0] == ["x_idx", "y_idx", "e_idx", "ldos"]
+    vals = np.array([float(r[3]) for r in rows[1:]])
+    # The oracle on the state read from the written files.
+    sim_cfg = json.loads((sim_out / "simulation_config.json").read_text())
+    L = O.LdosOracle(sim_cfg, pp)
+    n0 = L.n0
+    assert len(vals) == 6 * n0 * n0
+    op = list(csv.reader(open(sim_out / "order_parameter.csv")))[1:]
+    vp = list(csv.reader(open(sim_out / "vector_potential.csv")))[1:]
+    d = np.zeros((1, 2, n0, n0))
+    d[0, 0] = np.array([float(r[2]) for r in op]).reshape(n0, n0)
+    d[0, 1] = np.array([float(r[3]) for r in op]).reshape(n0, n0)
+    lam2 = cfg["physics"]["penetration_depth"] ** 2
+    a = np.zeros((2, n0, n0))
+    a[0] = np.array([float(r[2]) for r in vp]).reshape(n0, n0) * lam2
+    a[1] = np.array([float(r[3]) for r in vp]).reshape(n0, n0) * lam2
+    L.set_state(d, a)
+    for b in range(L.n_blocks):
+        L.begin_block(b)
+        for _ in range(2):
+            L.burn_in()
+        for _ in range(60):
+            if L.iterate()[0] < 1e-6:
+                break
+    want = L.ldos.reshape(-1)
+    assert np.max(np.abs(vals - want)) <= 1e-7 * np.max(np.abs(want))
