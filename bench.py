@@ -172,8 +172,7 @@ def run_reference(args):
         "unit": "site-updates/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": {"workload": "c2: d-wave square 30 xi0 @20/xi0, 256 angles, T=0.1, 14 Ozaki poles, kappa=2",
-                   "sample": sample},
+        "config": {"workload": WORKLOAD_DESC.get(args.workload, args.workload), "sample": sample},
         "cpu_baseline": {"value": value, "unit": "site-updates/s", "cores": threads,
                          "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "site-updates/s", "h2d_bytes_per_step": 0,
@@ -182,8 +181,206 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def run_engine(args):
+WORKLOAD_DESC = {
+    "c2": "c2: d_x2-y2 square 30 xi0 @20/xi0 (N0=606, N1=858), axes 45 deg, 256 angles, "
+          "T=0.1 (14 Ozaki poles), kappa=2, zero field",
+}
+
+
+def _time_context(ctx, stream, steps, warmup, world):
+    """Device-timed self-consistency iterations of one context (inputs resident)."""
+    import torch
+    for _ in range(warmup):
+        ctx.compute(1)
+    ctx.profile(True)
+    launches0 = ctx.launch_count()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    ctx.compute(steps)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    launches = ctx.launch_count() - launches0
+    prof = {k: ctx.profile_read(i) for i, k in enumerate(("sweep", "rotate_back", "poisson", "boundary"))}
+    ctx.profile(False)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms, launches, prof
+
+
+def _e2e(ctx, steps, world):
+    """Same metric through the public API with host buffers: every step the
+    host sends x (pinned memory) and reads x back."""
+    import torch
+    n0, nc = ctx.dims.n0, ctx.dims.n_comp
+    host_d = torch.empty((nc, 2, n0, n0), dtype=torch.float64, pin_memory=True).numpy()
+    host_a = torch.empty((2, n0, n0), dtype=torch.float64, pin_memory=True).numpy()
+    xd, xa = ctx.state()
+    host_d[...] = xd
+    host_a[...] = xa
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        ctx.set_state(host_d, host_a)
+        ctx.compute(1)
+        xd, xa = ctx.state()
+        host_d[...] = xd
+        host_a[...] = xa
+    torch.cuda.synchronize()
+    sec = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([sec], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        sec = float(t.item())
+    return sec, (nc * 2 * n0 * n0 + 2 * n0 * n0) * 8
+
+
+def _curl(a, h):
+    """B = curl A on the reference grid (curl_kernel, GridFunctions_GPU.h:326-352)."""
     import numpy as np
+    n = a.shape[-1]
+    idx = np.arange(n)
+    xn, xp = np.minimum(idx + 1, n - 1), np.maximum(idx - 1, 0)
+    day = (a[1][:, xn] - a[1][:, xp]) / (xn - xp)[None, :]
+    dax = (a[0][xn, :] - a[0][xp, :]) / (xn - xp)[:, None]
+    return (day - dax) / h
+
+
+def converge_c1(max_it: int, max_s: float):
+    """Time to converge (residual 1e-6) of the C1 disc in both precisions from
+    the same seeded start, and the distance of the mixed solution from the FP64
+    one in Delta, j, B and Omega."""
+    import numpy as np
+    import superconga_b200 as sb
+    from superconga_b200 import workloads
+    cfg = workloads.c1()
+    out, sol = {}, {}
+    for mode in ("fp64", "mixed"):
+        ctx = sb.Context(cfg, mode=mode)
+        d0, a0 = workloads.initial_state("c1", cfg, ctx.dims.n0)
+        ctx.set_state(d0, a0)
+        import torch
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        it, ok, res = 0, False, None
+        while it < max_it and time.perf_counter() - t0 < max_s:
+            res, ok = ctx.compute(1)
+            it += 1
+            if ok:
+                break
+        sec = time.perf_counter() - t0
+        out[mode] = {"seconds": sec, "iterations": it, "converged": bool(ok), "final_residual": res,
+                     "criterion": 1e-6}
+        d, j, _ = ctx.results()
+        _, a = ctx.state()
+        sol[mode] = (d, j, a, ctx.scalars()["free_energy"])
+        ctx.close()
+    lam2 = cfg["physics"]["penetration_depth"] ** 2
+    h = 1.0 / cfg["numerics"]["points_per_coherence_length"]
+    db = workloads.delta_bulk(cfg["physics"]["temperature"], "s")
+    (d64, j64, a64, f64), (d32, j32, a32, f32) = sol["fp64"], sol["mixed"]
+    b64, b32 = _curl(a64 / lam2, h), _curl(a32 / lam2, h)
+    out["mixed_vs_fp64"] = {
+        "delta_max_abs_over_delta_bulk": float(np.max(np.abs(d32 - d64)) / db),
+        "j_max_abs_over_max_j": float(np.max(np.abs(j32 - j64)) / max(np.max(np.abs(j64)), 1e-300)),
+        "b_max_abs_over_max_b": float(np.max(np.abs(b32 - b64)) / max(np.max(np.abs(b64)), 1e-300)),
+        "omega_rel": float(abs(f32 - f64) / abs(f64)),
+    }
+    out["speedup_mixed_over_fp64"] = out["fp64"]["seconds"] / out["mixed"]["seconds"]
+    out["workload"] = "c1: s-wave disc R=10 xi0 @10/xi0, 64 angles, T=0.5, b=0.02 B0, kappa=2"
+    return out
+
+
+def batched_c3(n_grains: int, iters: int, max_s: float):
+    """The C3 batch (n seeded grains) in both precisions: device-timed batch
+    iterations (CUDA-graph replays) after autotuning, then every grain run to
+    its own convergence (bounded)."""
+    import numpy as np
+    import torch
+    import superconga_b200 as sb
+    from superconga_b200 import workloads
+    cfgs, states = workloads.c3_grains(n_grains)
+    res = {"workload": f"c3: {n_grains} seeded grains (discs R~U(4,20), squares w~U(8,40) xi0 @10/xi0, "
+                       "s/d, T~U(0.1,0.9), b~U(0,0.1), kappa=2)"}
+    for mode in ("mixed", "fp64"):
+        b = sb.Batch(cfgs, mode=mode)
+        for g, c, st in zip(b.grains, cfgs, states):
+            d, a = workloads.c3_initial_state(c, st, g.dims.n0)
+            g.set_state(d, a)
+        su = int(b.site_updates().sum())
+        t0 = time.perf_counter()
+        b.compute(1)
+        lg, mb, _ = b.autotune()
+        b.compute(1)  # graph capture
+        torch.cuda.synchronize()
+        l0 = b.launch_count()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        b.compute(iters)
+        ev1.record()
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1) / iters
+        launches = (b.launch_count() - l0) / iters
+        act, it, r = b.status()
+        full = bool(act.all())
+        while b.compute(1) > 0 and time.perf_counter() - t0 < max_s:
+            pass
+        act, it, r = b.status()
+        conv = [bool(r[k] < 1e-6) for k in range(len(cfgs))]
+        res[mode] = {"site_updates_per_s": su / (ms * 1e-3) if full else None,
+                     "ms_per_iteration": ms, "site_updates_per_iteration": su,
+                     "all_grains_active_while_timed": full,
+                     "kernel_launches_per_iteration": launches,
+                     "sweep_mapping": {"threads_per_column": 1 << lg, "min_blocks_per_sm": mb},
+                     "seconds_all_grains": time.perf_counter() - t0,
+                     "grains_converged": int(sum(conv)), "grains_at_iteration_cap": int(np.sum(~act) - sum(conv)),
+                     "grains_still_running": int(np.sum(act)),
+                     "median_iterations": float(np.median(it))}
+        b.close()
+    return res
+
+
+def ldos_c5(iters: int):
+    """LDOS postprocess throughput on the C5 grain: one block of 32 real
+    energies in [-2 Delta0, 2 Delta0], broadening 0.02 Delta0, on the seeded
+    nine-vortex state (device-timed LDOS iterations after one burn-in)."""
+    import torch
+    import superconga_b200 as sb
+    from superconga_b200 import workloads
+    cfg = workloads.c5()
+    d0 = workloads.S_WAVE_BULK
+    pp = {"spectroscopy": {"energy_min": -2 * d0, "energy_max": 2 * d0, "num_energies": 512,
+                           "energy_broadening": 0.02 * d0},
+          "numerics": {"convergence_criterion": 1e-6, "norm": "l2", "num_energies_per_block": 32,
+                       "num_fermi_momenta": 128}}
+    out = {"workload": "c5 LDOS: s square 100 xi0 @16/xi0 (N0=1606), 128 angles, 32 energies per block"}
+    for mode in ("mixed", "fp64"):
+        e = sb.LdosContext(cfg, pp, mode=mode)
+        d, a = workloads.initial_state("c5", cfg, e.dims.n0)
+        e.set_state(d, a)
+        e.begin_block(0)
+        e.burn_in(1)
+        su = e.site_updates()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e.iterate(iters)
+        torch.cuda.synchronize()
+        sec = (time.perf_counter() - t0) / iters
+        out[mode] = {"site_updates_per_s": su / sec, "s_per_iteration": sec, "site_updates_per_iteration": su}
+        e.close()
+    return out
+
+
+def run_engine(args):
     import torch
 
     world, rank, local = _dist()
@@ -196,8 +393,7 @@ def run_engine(args):
     if rank == 0:
         build.build()
     if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+        torch.distributed.barrier()
     import superconga_b200 as sb
     from superconga_b200 import workloads
     from superconga_b200.engine import fma_peak
@@ -206,134 +402,73 @@ def run_engine(args):
     hbm, hbm_kind = _peaks()
     results = {}
     modes = args.modes.split(",")
+    sampler = ClockSampler(local)
+    sampler.__enter__()
     for mode in modes:
         ctx = sb.Context(cfg, mode=mode)
         stream = torch.cuda.Stream()
         ctx.set_stream(stream.cuda_stream)
-        n0, nc = ctx.dims.n0, ctx.dims.n_comp
         su = ctx.site_updates()
-        d0, a0 = workloads.initial_state(args.workload, cfg, n0)
+        d0, a0 = workloads.initial_state(args.workload, cfg, ctx.dims.n0)
         ctx.set_state(d0, a0)
-        for _ in range(args.warmup):
-            ctx.compute(1)
-        # device-timed region: K iterations, inputs resident in HBM
-        ctx.profile(True)
-        launches0 = ctx.launch_count()
-        if world > 1:
-            torch.distributed.barrier()
-        torch.cuda.synchronize()
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev1 = torch.cuda.Event(enable_timing=True)
-        with ClockSampler(local) as clk:
-            ev0.record(stream)
-            ctx.compute(args.steps)
-            ev1.record(stream)
-            torch.cuda.synchronize()
-        ms = ev0.elapsed_time(ev1)
-        launches = ctx.launch_count() - launches0
-        sweep_ms, sweep_n = ctx.profile_read(0)
-        rb_ms, _ = ctx.profile_read(1)
-        pois_ms, _ = ctx.profile_read(2)
-        bc_ms, _ = ctx.profile_read(3)
-        ctx.profile(False)
-        clocks = clk.summary()
-        if world > 1:
-            t = torch.tensor([ms], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ms = float(t.item())
-        per_step = ms / args.steps
+        ms, launches, prof = _time_context(ctx, stream, args.steps, args.warmup, world)
         value = world * su * args.steps / (ms * 1e-3)
-        # end to end through the public API with host buffers: every step the
-        # host sends x (pinned) and reads x back.
-        nd = nc * 2 * n0 * n0
-        host_d = torch.empty((nc, 2, n0, n0), dtype=torch.float64, pin_memory=True).numpy()
-        host_a = torch.empty((2, n0, n0), dtype=torch.float64, pin_memory=True).numpy()
-        xd, xa = ctx.state()
-        host_d[...] = xd
-        host_a[...] = xa
-        if world > 1:
-            torch.distributed.barrier()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for _ in range(args.steps):
-            ctx.set_state(host_d, host_a)
-            ctx.compute(1)
-            xd, xa = ctx.state()
-            host_d[...] = xd
-            host_a[...] = xa
-        torch.cuda.synchronize()
-        e2e_s = time.perf_counter() - t0
-        if world > 1:
-            t = torch.tensor([e2e_s], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            e2e_s = float(t.item())
-        e2e = world * su * args.steps / e2e_s
-        bytes_io = (nd + 2 * n0 * n0) * 8
-        # roofline of the dominant kernel, the sweep
+        e2e_s, bytes_io = _e2e(ctx, args.steps, world)
+        sweep_ms, sweep_n = prof["sweep"]
         sweep_avg_s = (sweep_ms / max(sweep_n, 1)) * 1e-3
-        sweeps_per_step = max(sweep_n, 1) / args.steps
-        su_per_launch = su / sweeps_per_step
+        su_per_launch = su / (max(sweep_n, 1) / args.steps)
         achieved_gbs = su_per_launch * BYTES_PER_SU[mode] / sweep_avg_s / 1e9
         pipe_peak = fma_peak(64 if mode == "fp64" else 32)
         achieved_flops = su_per_launch * FLOPS_PER_SU / sweep_avg_s
-        traffic = _traffic(mode)
+        tr = _traffic(mode)
         results[mode] = {
-            "value": value, "ms_per_step": per_step, "site_updates_per_step": su,
-            "gpu_launches": launches, "clocks": clocks,
-            "e2e": {"value": e2e, "unit": "site-updates/s", "h2d_bytes_per_step": bytes_io,
-                    "d2h_bytes_per_step": bytes_io},
+            "value": value, "ms_per_step": ms / args.steps, "site_updates_per_step": su,
+            "gpu_launches": launches,
+            "e2e": {"value": world * su * args.steps / e2e_s, "unit": "site-updates/s",
+                    "h2d_bytes_per_step": bytes_io, "d2h_bytes_per_step": bytes_io},
             "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved_gbs / hbm, "traffic": traffic,
-                         "peak_kind": hbm_kind,
-                         "kernel": "k_sweep", "kernel_ms_per_launch": sweep_avg_s * 1e3,
+                         "frac": achieved_gbs / hbm,
+                         "traffic": None if tr is None else tr * su_per_launch,
+                         "peak_kind": hbm_kind, "kernel": "k_sweep",
+                         "kernel_ms_per_launch": sweep_avg_s * 1e3,
+                         "algorithmic_bytes_per_launch": su_per_launch * BYTES_PER_SU[mode],
                          "pipe": {"precision": "fp64" if mode == "fp64" else "fp32",
                                   "achieved_tflops": achieved_flops / 1e12,
                                   "peak_tflops": pipe_peak / 1e12,
                                   "frac": achieved_flops / pipe_peak,
                                   "peak_kind": "measured FMA loop"}},
-            "kernel_ms_per_step": {"sweep": sweep_ms / args.steps, "rotate_back": rb_ms / args.steps,
-                                   "poisson": pois_ms / args.steps, "boundary": bc_ms / args.steps},
+            "kernel_ms_per_step": {k: v[0] / args.steps for k, v in prof.items()},
         }
-        # time to converge (residual 1e-6) from the seeded start, bounded
-        conv = None
-        if not args.no_converge:
-            ctx2 = sb.Context(cfg, mode=mode)
-            ctx2.set_stream(stream.cuda_stream)
-            ctx2.set_state(d0, a0)
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            it, ok, res = 0, False, None
-            while it < args.converge_max_it and time.perf_counter() - t0 < args.converge_max_s:
-                res, ok = ctx2.compute(1)
-                it += 1
-                if ok:
-                    break
-            conv = {"seconds": time.perf_counter() - t0, "iterations": it, "converged": bool(ok),
-                    "final_residual": res, "criterion": 1e-6}
-            ctx2.close()
-        results[mode]["time_to_converge"] = conv
         ctx.close()
         del stream
+    extra = {}
+    if rank == 0 and world == 1 and not args.no_converge:
+        extra["time_to_converge"] = converge_c1(args.converge_max_it, args.converge_max_s)
+    if rank == 0 and world == 1 and not args.no_batch:
+        extra["batched"] = batched_c3(args.batch_grains, args.batch_iters, args.converge_max_s)
+    if rank == 0 and world == 1 and args.ldos:
+        extra["ldos"] = ldos_c5(2)
+    sampler.__exit__(None, None, None)
+    clocks = sampler.summary()
 
     m = results[modes[0]]
     line = {
         "metric": "riccati_site_updates_per_s", "value": m["value"], "unit": "site-updates/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32 stepping / f64 accumulation", "data": "synthetic (seeded)",
-        "config": {"workload": "c2: d_x2-y2 square 30 xi0 @20/xi0 (N0=606, N1=858), axes 45 deg, "
-                               "256 angles, T=0.1 (14 Ozaki poles), kappa=2, zero field",
+        "vs_baseline": None,
+        "dtype": "f32 stepping / f64 accumulation" if modes[0] == "mixed" else "f64",
+        "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD_DESC.get(args.workload, args.workload + " (profiling case, not the benchmark workload)"),
                    "global_batch": 1, "seq_len": None, "parallelism": "replicas" if world > 1 else "single",
                    "mode": modes[0], "l2": "inputs larger than L2 (multi-GB sweep scratch per step)"},
         "e2e": m["e2e"], "gpu_launches": m["gpu_launches"], "roofline": m["roofline"],
-        "clocks": m["clocks"], "kernel_ms_per_step": m["kernel_ms_per_step"],
-        "time_to_converge": m["time_to_converge"],
+        "clocks": clocks, "kernel_ms_per_step": m["kernel_ms_per_step"],
     }
     if "fp64" in results and modes[0] != "fp64":
         line["fp64"] = results["fp64"]
         line["mixed_over_fp64"] = m["value"] / results["fp64"]["value"]
-    if args.workload != WORKLOAD:
-        line["config"]["workload"] = args.workload + " (profiling case, not the benchmark workload)"
+    line.update(extra)
     if rank == 0 and world == 1 and not args.no_cpu:
         v, sec, threads, sample = cpu_reference(2, 1, workload=args.workload)
         line["cpu_baseline"] = {"value": v, "unit": "site-updates/s", "cores": threads,
@@ -357,6 +492,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--converge-max-it", type=int, default=400)
     ap.add_argument("--converge-max-s", type=float, default=60.0)
+    ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--batch-grains", type=int, default=128)
+    ap.add_argument("--batch-iters", type=int, default=5)
+    ap.add_argument("--ldos", action="store_true", help="also time the C5 LDOS postprocess")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -1782,6 +1782,18 @@ void orc_angle_greens(void *h, int a, double *fre, double *fim, double *gre, dou
   std::memcpy(dre, vdre.data(), nn * 8);
   std::memcpy(dim, vdim.data(), nn * 8);
 }
+// One frozen-boundary evaluation (the sweeps and compute objects of one
+// Context::compute without the accelerator step and the boundary update):
+// g(x), j and the free energy of the current state.
+void orc_evaluate(void *h) {
+  Oracle *o = (Oracle *)h;
+  if (!o->boundary_initialized) o->set_boundary_initial();
+  o->integrate_all();
+}
+
+// External flux quanta (the field enters the energy shift through the gauge).
+void orc_set_flux(void *h, double flux_quanta) { ((Oracle *)h)->p.flux_quanta = flux_quanta; }
+
 // Real parts of the sweep energies (LDOS energies E_k; the imaginary parts,
 // the broadening, are those given to orc_create).  Starts a new energy block:
 // fresh boundary values and LDOS history.

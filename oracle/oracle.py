@@ -494,6 +494,14 @@ class Oracle:
     def burn_in(self):
         lib().orc_burn_in(self.h)
 
+    def evaluate(self) -> float:
+        """Frozen-boundary evaluation; returns the free energy."""
+        lib().orc_evaluate(self.h)
+        return self.scalars()["free_energy"]
+
+    def set_flux(self, flux_quanta: float):
+        lib().orc_set_flux(self.h, ctypes.c_double(flux_quanta))
+
     def state(self):
         n = self.n0
         d = np.zeros((self.setup.n_comp, 2, n, n))

@@ -68,6 +68,11 @@ SIGNATURES = {
     "sc_batch_autotune": (ctypes.c_int, [ctypes.c_void_p, _c_int_p, _c_int_p, ctypes.POINTER(ctypes.c_double)]),
     "sc_batch_time_sweeps": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "sc_batch_launch_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]),
+    "sc_set_external_field": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
+    "sc_get_external_field": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
+    "sc_evaluate": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
+    "sc_adjoint": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _c_double_p, _c_double_p, _c_double_p,
+                                  ctypes.POINTER(ctypes.c_double)]),
     "sc_measure_fma_peak": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "sc_setup_create": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p)]),
     "sc_setup_last_error": (ctypes.c_char_p, []),

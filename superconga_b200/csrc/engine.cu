@@ -1143,6 +1143,11 @@ struct DevArray {
   }
 };
 
+struct AdjBuffers;  // adjoint work buffers (adjoint.cuh)
+struct AdjDeleter {
+  void operator()(AdjBuffers *p) const;
+};
+
 struct Chunk {
   int a_begin, a_end;   // angles [a_begin, a_end)
   int item_begin, item_end;
@@ -1196,8 +1201,14 @@ struct sc_ctx {
   // Work buffers of the sweep (scratch, fields, frame buffers): the
   // context's own arrays, or a batch's shared pool (batch_member).
   bool batch_member = false;
+  // Frame buffers hold zeros wherever the sweep and the extension do not
+  // write; with one chunk every slot always holds the same angle, so they are
+  // cleared once instead of before every sweep.
+  bool frames_zeroed = false;
   double *w_scratch = nullptr, *w_scratch2 = nullptr, *w_fg = nullptr, *w_gi = nullptr;
   size_t need_scratch = 0, need_scratch2 = 0, need_frame = 0;  // bytes of each (frame: fg and gi each)
+
+  std::unique_ptr<AdjBuffers, AdjDeleter> adj;  // allocated by the first sc_adjoint
 
   // LDOS postprocess: frame buffer, block accumulator, all energies.
   DevArray<double> ldf, ldos_acc, ldos_all;
@@ -1492,11 +1503,13 @@ void run_chunks(sc_ctx *c, int burn_in) {
     run_chunks_ldos<R>(c, burn_in);
     return;
   }
+  const bool clear = c->chunks.size() > 1 || !c->frames_zeroed;
   for (const Chunk &ch : c->chunks) {
     const int nslots = ch.a_end - ch.a_begin;
-    if (!burn_in) {
+    if (!burn_in && clear) {
       CUDA_TRY(cudaMemsetAsync(c->w_fg, 0, (size_t)nslots * nn1 * sizeof(double2), c->stream));
       CUDA_TRY(cudaMemsetAsync(c->w_gi, 0, (size_t)nslots * nn1 * sizeof(double2), c->stream));
+      c->frames_zeroed = c->chunks.size() == 1;
     }
     launch_sweep<R>(c, ch, burn_in);
     if (burn_in) continue;
@@ -2323,6 +2336,7 @@ int sc_angle_greens(sc_ctx *ctx, int angle, double *f, double *g_re, double *i_r
   }
   const size_t nn1 = (size_t)S.n1 * S.n1;
   extend_reference(ctx);
+  ctx->frames_zeroed = false;  // slot 0 now holds this angle
   CUDA_TRY(cudaMemsetAsync(ctx->w_fg, 0, nn1 * sizeof(double2), ctx->stream));
   CUDA_TRY(cudaMemsetAsync(ctx->w_gi, 0, nn1 * sizeof(double2), ctx->stream));
   if (!cols.empty()) {
@@ -2478,8 +2492,18 @@ struct sc_batch {
   long long graph_launches = 0;     // kernel launches in the captured iteration
   long long replayed_launches = 0;  // launches executed through graph replays
   long long captured_launches = 0;  // launches recorded into graphs (not run at capture)
+  // Side streams for the grains' own kernels, forked from and joined back
+  // into the batch stream around every phase (graph branches once captured).
+  static constexpr int K_SIDE = 8;
+  cudaStream_t side[K_SIDE] = {};
+  cudaEvent_t ev_fork = nullptr, ev_join[K_SIDE] = {};
   ~sc_batch() {
     if (exec) cudaGraphExecDestroy(exec);
+    for (int k = 0; k < K_SIDE; ++k) {
+      if (side[k]) cudaStreamDestroy(side[k]);
+      if (ev_join[k]) cudaEventDestroy(ev_join[k]);
+    }
+    if (ev_fork) cudaEventDestroy(ev_fork);
     for (sc_ctx *c : grains) delete c;
     if (stream) cudaStreamDestroy(stream);
   }
@@ -2519,6 +2543,7 @@ void batch_plan(sc_batch *b) {
     }
     sc_ctx *c = b->grains[g];
     char *base = (char *)b->pool.p + used[w];
+    c->frames_zeroed = false;  // new place in the pool
     c->w_scratch = (double *)base;
     base += align256(c->need_scratch);
     c->w_scratch2 = (double *)base;
@@ -2594,38 +2619,67 @@ void launch_batch_sweep(sc_batch *b, sc_batch::Wave &w, int wi) {
   if (e != cudaSuccess) throw EngineError(SC_ERR_CUDA, std::string("batch sweep launch: ") + cudaGetErrorString(e));
 }
 
+void batch_fork(sc_batch *b) {
+  CUDA_TRY(cudaEventRecord(b->ev_fork, b->stream));
+  for (int k = 0; k < sc_batch::K_SIDE; ++k) CUDA_TRY(cudaStreamWaitEvent(b->side[k], b->ev_fork, 0));
+}
+void batch_join(sc_batch *b) {
+  for (int k = 0; k < sc_batch::K_SIDE; ++k) {
+    CUDA_TRY(cudaEventRecord(b->ev_join[k], b->side[k]));
+    CUDA_TRY(cudaStreamWaitEvent(b->stream, b->ev_join[k], 0));
+  }
+}
+// Grain g's kernels go to side stream (rank of g among the active grains) mod K.
+void batch_assign_streams(sc_batch *b, bool to_side) {
+  int k = 0;
+  for (size_t g = 0; g < b->grains.size(); ++g)
+    b->grains[g]->stream = (to_side && b->active[g]) ? b->side[(k++) % sc_batch::K_SIDE] : b->stream;
+}
+
 // The sweeps of all waves (with the per-grain frame fields before and the
 // frame rotation after each wave's launch).
 template <typename R>
 void batch_sweeps(sc_batch *b) {
   const int nw = (int)b->waves.size();
+  batch_assign_streams(b, true);
   for (int wi = 0; wi < nw; ++wi) {
     sc_batch::Wave &w = *b->waves[wi];
+    batch_fork(b);
     for (int g : w.grains) {
       sc_ctx *c = b->grains[g];
       const Chunk &ch = c->chunks[0];
       const size_t nn1 = (size_t)c->S.n1 * c->S.n1;
       const int nslots = ch.a_end - ch.a_begin;
-      CUDA_TRY(cudaMemsetAsync(c->w_fg, 0, (size_t)nslots * nn1 * sizeof(double2), b->stream));
-      CUDA_TRY(cudaMemsetAsync(c->w_gi, 0, (size_t)nslots * nn1 * sizeof(double2), b->stream));
+      if (!c->frames_zeroed) {
+        CUDA_TRY(cudaMemsetAsync(c->w_fg, 0, (size_t)nslots * nn1 * sizeof(double2), c->stream));
+        CUDA_TRY(cudaMemsetAsync(c->w_gi, 0, (size_t)nslots * nn1 * sizeof(double2), c->stream));
+        c->frames_zeroed = true;
+      }
       launch_frame_fields<R>(c, ch, sweep_args<R>(c, &ch, 0));
     }
+    batch_join(b);
     launch_batch_sweep<R>(b, w, wi);
+    batch_fork(b);
     for (int g : w.grains) frame_to_reference(b->grains[g], b->grains[g]->chunks[0]);
+    batch_join(b);
   }
+  batch_assign_streams(b, false);
 }
 
 template <typename R>
 void batch_iteration(sc_batch *b) {
+  batch_assign_streams(b, true);
+  batch_fork(b);
   for (size_t g = 0; g < b->grains.size(); ++g)
     if (b->active[g]) compute_pre<R>(b->grains[g]);
+  batch_join(b);
   batch_sweeps<R>(b);
-  int n = 0;
+  batch_assign_streams(b, true);
+  batch_fork(b);
   for (size_t g = 0; g < b->grains.size(); ++g)
-    if (b->active[g]) {
-      compute_post<R>(b->grains[g]);
-      ++n;
-    }
+    if (b->active[g]) compute_post<R>(b->grains[g]);
+  batch_join(b);
+  batch_assign_streams(b, false);
   k_gather_scalars<<<grid1(b->grains.size(), 128), 128, 0, b->stream>>>((int)b->grains.size(), b->scalar_src.p,
                                                                           b->scalars.p);
   b->launches++;
@@ -2710,6 +2764,11 @@ int sc_batch_create(const char *const *configs, int n, int mode, sc_batch **out)
   b->mode = mode;
   try {
     CUDA_TRY(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    for (int k = 0; k < sc_batch::K_SIDE; ++k) {
+      CUDA_TRY(cudaStreamCreateWithFlags(&b->side[k], cudaStreamNonBlocking));
+      CUDA_TRY(cudaEventCreateWithFlags(&b->ev_join[k], cudaEventDisableTiming));
+    }
+    CUDA_TRY(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
     int dev = 0;
     CUDA_TRY(cudaGetDevice(&dev));
     CUDA_TRY(cudaDeviceGetAttribute(&b->n_sm, cudaDevAttrMultiProcessorCount, dev));
@@ -2719,7 +2778,14 @@ int sc_batch_create(const char *const *configs, int n, int mode, sc_batch **out)
       b->grains.push_back(c);
       c->mode = mode;
       c->batch_member = true;
-      const std::string e = build_setup(configs[i], c->S);
+    }
+    // Host set-up of the grains in parallel (pure host work).
+    std::vector<std::string> errs(n);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int i = 0; i < n; ++i) errs[i] = build_setup(configs[i], b->grains[i]->S);
+    for (int i = 0; i < n; ++i) {
+      sc_ctx *c = b->grains[i];
+      const std::string &e = errs[i];
       if (!e.empty()) throw EngineError(SC_ERR_ARG, "grain " + std::to_string(i) + ": " + e);
       if (c->S.nc > MAX_COMP) throw EngineError(SC_ERR_ARG, "at most 4 order-parameter components");
       if (c->S.ne > 32) throw EngineError(SC_ERR_ARG, "grain " + std::to_string(i) + ": at most 32 Ozaki energies in a batch");
@@ -2935,3 +3001,5 @@ int sc_batch_autotune(sc_batch *b, int *log_groups, int *minb, double *best_ms) 
 }
 
 }  // extern "C"
+
+#include "adjoint.cuh"

@@ -125,6 +125,35 @@ class Context:
             if (conv and i >= it_min) or (it_max >= 0 and i >= it_max):
                 return i, conv
 
+    def set_external_field(self, b: float):
+        """External field B_ext = pi Phi / area in units of B0 (RiccatiSolver.h:137-139)."""
+        self._check(_lib.load().sc_set_external_field(self._h, float(b)))
+
+    def external_field(self) -> float:
+        v = ctypes.c_double()
+        self._check(_lib.load().sc_get_external_field(self._h, ctypes.byref(v)))
+        return v.value
+
+    def evaluate(self) -> float:
+        """Frozen-boundary evaluation of the current state (no accelerator
+        step, no boundary update); returns the free energy.  g(x) and j are
+        then available from ``results``."""
+        v = ctypes.c_double()
+        self._check(_lib.load().sc_evaluate(self._h, ctypes.byref(v)))
+        return v.value
+
+    def adjoint(self, w_omega: float = 1.0, beta_j: np.ndarray | None = None):
+        """Gradients of L = w_omega * Omega + sum(beta_j * j) at frozen boundary
+        values: dL/dDelta [Nc][2][N0][N0] (d/dRe, d/dIm), dL/dA [2][N0][N0]
+        (internal units), dL/dB_ext."""
+        gd = np.zeros(self._shape_delta())
+        ga = np.zeros(self._shape_vec())
+        gb = ctypes.c_double()
+        bj = None if beta_j is None else np.ascontiguousarray(beta_j, np.float64).reshape(self._shape_vec())
+        self._check(_lib.load().sc_adjoint(self._h, float(w_omega), _p(bj) if bj is not None else None,
+                                           _p(gd), _p(ga), ctypes.byref(gb)))
+        return gd, ga, gb.value
+
     def results(self):
         """g(x): new order parameter, current density, new vector potential."""
         d = np.zeros(self._shape_delta())
