@@ -218,8 +218,9 @@ int sc_batch_status(const sc_batch *b, int *active, int *iterations, double *res
 int sc_batch_set_graph(sc_batch *b, int enable);
 /* Mapping of the persistent sweep: 2^log_groups threads per trajectory column
  * and the resident-block variant minb (1: up to 255 registers per thread,
- * 4: at most 128).  sc_batch_autotune times every feasible choice on the
- * current state (after at least one iteration) and keeps the fastest. */
+ * 4: at most 128, 6: at most 80 with at most two energies per thread).
+ * sc_batch_autotune times every feasible choice on the current state (after
+ * at least one iteration) and keeps the fastest. */
 int sc_batch_config(sc_batch *b, int log_groups, int minb);
 int sc_batch_get_config(const sc_batch *b, int *log_groups, int *minb, int *n_waves);
 int sc_batch_autotune(sc_batch *b, int *log_groups, int *minb, double *best_ms);

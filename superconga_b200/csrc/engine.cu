@@ -764,48 +764,73 @@ __global__ void k_subtract_mean(int n0, const double *__restrict__ j, const doub
 // One Toeplitz correlation pass of the separable Poisson solve for every
 // filter (cvp_internal::crossCorrelate1DTranspose, ComputeVectorPotential.h:437-499):
 //   out[k][d][x][y] = sum_i filt_k[i + n - 1 - y] * src[k or 0][d][i][x].
-// Tiled 32 x 32 in (x, y), 32 source rows at a time through shared memory.
-constexpr int PT = 32;
-__global__ void __launch_bounds__(PT * 8) k_toeplitz(int n, int nk, const double *__restrict__ filt,
-                                                     const double *__restrict__ src, size_t src_kstride,
-                                                     double *__restrict__ dst) {
-  __shared__ double s_src[PT][PT + 1];
-  __shared__ double s_f[2 * PT];
+// A block computes a 64 x 64 tile of (x, y); each of its 128 threads a 4 x 8
+// register tile (x strided by 16, 8 consecutive y).  Source rows come through
+// shared memory 32 at a time; for consecutive y the filter taps f[i + n - 1 - y]
+// form a window that slides by one per source row, so each row costs four
+// source loads and one filter load for 32 FMAs.  The sum over i runs in
+// ascending order as in the reference.
+constexpr int PT_X = 64, PT_Y = 64, PT_R = 32;
+__global__ void __launch_bounds__(128) k_toeplitz(int n, int nk, const double *__restrict__ filt,
+                                                  const double *__restrict__ src, size_t src_kstride,
+                                                  double *__restrict__ dst) {
+  __shared__ double s_src[PT_R][PT_X];
+  __shared__ double s_f[PT_R + PT_Y];
   const int k = blockIdx.z / 2, d = blockIdx.z % 2;
-  const int x0 = blockIdx.x * PT, y0 = blockIdx.y * PT;
-  const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+  const int x0 = blockIdx.x * PT_X, y0 = blockIdx.y * PT_Y;
+  const int t = threadIdx.x, tx = t & 15, ty = t >> 4;  // 16 x 8 threads
   const size_t nn = (size_t)n * n;
   const double *S = src + (size_t)k * src_kstride + (size_t)d * nn;
   const double *F = filt + (size_t)k * (2 * n - 1);
-  double acc[4] = {0, 0, 0, 0};
-  for (int i0 = 0; i0 < n; i0 += PT) {
-    for (int r = ty; r < PT; r += 8) {
-      const int i = i0 + r, xx = x0 + tx;
-      s_src[r][tx] = (i < n && xx < n) ? S[(size_t)i * n + xx] : 0.0;
+  double acc[4][8];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 8; ++b) acc[a][b] = 0.0;
+  for (int i0 = 0; i0 < n; i0 += PT_R) {
+    for (int e = t; e < PT_R * PT_X; e += 128) {
+      const int r = e / PT_X, c = e % PT_X;
+      const int i = i0 + r, xx = x0 + c;
+      s_src[r][c] = (i < n && xx < n) ? S[(size_t)i * n + xx] : 0.0;
     }
-    // filter window: f[i + n - 1 - y] for i in [i0, i0+32), y in [y0, y0+32)
-    const int t = ty * 32 + tx;
-    if (t < 2 * PT) {
-      const int fi = i0 + n - 1 - y0 - (PT - 1) + t;
-      s_f[t] = (fi >= 0 && fi < 2 * n - 1) ? F[fi] : 0.0;
+    // taps f[i + n - 1 - y], i in [i0, i0 + 32), y in [y0, y0 + 64):
+    // s_f[q] = f[i0 + n - 1 - y0 - (PT_Y - 1) + q]
+    for (int q = t; q < PT_R + PT_Y; q += 128) {
+      const int fi = i0 + n - 1 - y0 - (PT_Y - 1) + q;
+      s_f[q] = (fi >= 0 && fi < 2 * n - 1) ? F[fi] : 0.0;
     }
     __syncthreads();
-    for (int r = 0; r < PT; ++r) {
-      const double sv = s_src[r][tx];
+    // y = y0 + 8 ty + b uses s_f[r - 8 ty - b + PT_Y - 1]
+    const int base = PT_Y - 1 - 8 * ty;
+    double w[8];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int yl = ty + 8 * u;
-        acc[u] += s_f[r - yl + PT - 1] * sv;
+    for (int b = 0; b < 8; ++b) w[b] = s_f[base - b];
+#pragma unroll
+    for (int r = 0; r < PT_R; ++r) {
+      double sv[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) sv[a] = s_src[r][tx + 16 * a];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 8; ++b) acc[a][b] += w[b] * sv[a];
+      if (r + 1 < PT_R) {
+#pragma unroll
+        for (int b = 7; b > 0; --b) w[b] = w[b - 1];
+        w[0] = s_f[base + r + 1];
       }
     }
     __syncthreads();
   }
-  const int xx = x0 + tx;
-  if (xx < n) {
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int yy = y0 + ty + 8 * u;
-      if (yy < n) dst[(size_t)k * 2 * nn + (size_t)n * (d * n + xx) + yy] = acc[u];
+  for (int a = 0; a < 4; ++a) {
+    const int xx = x0 + tx + 16 * a;
+    if (xx >= n) continue;
+    double *o = dst + (size_t)k * 2 * nn + (size_t)n * (d * n + xx);
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      const int yy = y0 + 8 * ty + b;
+      if (yy < n) o[yy] = acc[a][b];
     }
   }
 }
@@ -1182,6 +1207,7 @@ struct sc_ctx {
   DevArray<int> onode_a_g, onode_x_g, onode_y_g, onode_a_gt, onode_x_gt, onode_y_gt;
   std::vector<Chunk> chunks;
   int groups = 1, log_groups = 0, ept = 1;
+  bool emax2 = false;  // two-energies-per-thread sweep variant (tuning)
   int pair = 0;  // > 0: mixed mode sweeps angles [0, n/2) and mirrors them onto [n/2, n)
 
   // state: x = [delta | avec], g = [delta_new | a_new]
@@ -1329,13 +1355,17 @@ void launch_sweep(sc_ctx *c, const Chunk &ch, int burn_in) {
   ProfScope prof(c, 0);
   // FP64 runs best with four resident blocks per SM (measured on B200).
   static const char *minb_env = std::getenv("SCB_SWEEP_MINB");
-  const int variant = minb_env ? std::atoi(minb_env) : (sizeof(R) == 8 ? 4 : 1);
+  const int variant = minb_env ? std::atoi(minb_env) : (sizeof(R) == 8 ? 4 : (c->emax2 ? 6 : 1));
   if (c->S.keldysh) {
     if (c->ept <= 4) k_sweep<R, 4, 1, true><<<blocks, 128, 0, c->stream>>>(A);
     else if (c->ept <= 8) k_sweep<R, 8, 1, true><<<blocks, 128, 0, c->stream>>>(A);
     else k_sweep<R, 16, 1, true><<<blocks, 128, 0, c->stream>>>(A);
+  } else if (c->ept <= 2 && c->emax2) {
+    if (variant >= 6) k_sweep<R, 2, 6, false><<<blocks, 128, 0, c->stream>>>(A);
+    else k_sweep<R, 2, 4, false><<<blocks, 128, 0, c->stream>>>(A);
   } else if (c->ept <= 4) {
     if (variant == 4) k_sweep<R, 4, 4, false><<<blocks, 128, 0, c->stream>>>(A);
+    else if (variant == 5) k_sweep<R, 4, 5, false><<<blocks, 128, 0, c->stream>>>(A);
     else k_sweep<R, 4, 1, false><<<blocks, 128, 0, c->stream>>>(A);
   } else if (c->ept <= 8) {
     k_sweep<R, 8, 1, false><<<blocks, 128, 0, c->stream>>>(A);
@@ -1415,8 +1445,8 @@ void poisson(sc_ctx *c, const double *j, double *a_out, int mean_from_scalars) {
   } else {
     CUDA_TRY(cudaMemcpyAsync(c->pois_s.p, j, nn2 * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
   }
-  dim3 blk(PT, 8);
-  dim3 grid((n + PT - 1) / PT, (n + PT - 1) / PT, 2 * nk);
+  dim3 blk(128);
+  dim3 grid((n + PT_X - 1) / PT_X, (n + PT_Y - 1) / PT_Y, 2 * nk);
   ProfScope prof(c, 2);
   k_toeplitz<<<grid, blk, 0, c->stream>>>(n, nk, c->filters.p, c->pois_s.p, 0, c->pois_t0.p);
   check_launch(c);
@@ -1820,18 +1850,22 @@ void upload_static(sc_ctx *c) {
   c->groups = 1;
   c->log_groups = 0;
   const char *eg = std::getenv("SCB_ENERGY_GROUPS");
-  // Default: the fewest threads per column that keep at most four energies per
-  // thread (the fastest split measured on B200 for 7-14 Ozaki energies).
+  // Default (fastest measured on B200 for 7-14 Ozaki energies): FP64 the fewest
+  // threads per column that keep at most four energies per thread; mixed
+  // precision at most two, so that six blocks fit on an SM.
+  const bool fp32_sweep = c->mode == SC_MODE_MIXED && !S.keldysh;
+  const int per_thread = fp32_sweep ? 2 : 4;
   int want = 1;
   if (eg) want = std::atoi(eg);
   else
-    while ((S.ne + want - 1) / want > 4 && want < 8) want *= 2;
+    while ((S.ne + want - 1) / want > per_thread && want < 8) want *= 2;
   while (c->groups < want && c->groups < 8) {
     c->groups *= 2;
     c->log_groups++;
   }
   c->ept = (S.ne + c->groups - 1) / c->groups;
   if (c->ept > 16) throw EngineError(SC_ERR_ARG, "too many Ozaki energies per thread");
+  c->emax2 = fp32_sweep ? !std::getenv("SCB_SWEEP_EMAX4") : std::getenv("SCB_SWEEP_EMAX2") != nullptr;
 
   // State and work buffers.
   const size_t nn = c->nn0();
@@ -2606,7 +2640,9 @@ void launch_batch_sweep(sc_batch *b, sc_batch::Wave &w, int wi) {
     const int blocks = std::max(1, per_sm) * b->n_sm;
     kernel<<<blocks, 128, 0, b->stream>>>(args, w.units.p, w.n_units, counter, b->log_groups);
   };
-  if (ept <= 4) {
+  if (ept <= 2 && b->minb == 6) {
+    run(k_sweep_batch<R, 2, 6>);
+  } else if (ept <= 4) {
     if (b->minb == 4) run(k_sweep_batch<R, 4, 4>);
     else run(k_sweep_batch<R, 4, 1>);
   } else if (ept <= 8) {
@@ -2898,7 +2934,7 @@ int sc_batch_set_graph(sc_batch *b, int enable) {
 }
 
 int sc_batch_config(sc_batch *b, int log_groups, int minb) {
-  if (!b || log_groups < 0 || log_groups > 3 || (minb != 1 && minb != 4)) return SC_ERR_ARG;
+  if (!b || log_groups < 0 || log_groups > 3 || (minb != 1 && minb != 4 && minb != 6)) return SC_ERR_ARG;
   int ne_max = 1;
   for (sc_ctx *c : b->grains) ne_max = std::max(ne_max, c->S.ne);
   if (((ne_max + (1 << log_groups) - 1) >> log_groups) > 16) return SC_ERR_ARG;
@@ -2977,8 +3013,9 @@ int sc_batch_autotune(sc_batch *b, int *log_groups, int *minb, double *best_ms) 
   for (int lg = 1; lg <= 3; ++lg) {
     const int ept = (ne_max + (1 << lg) - 1) >> lg;
     if (ept > 16) continue;
-    for (int mb : {1, 4}) {
+    for (int mb : {1, 4, 6}) {
       if (mb == 4 && ept > 4) continue;  // the 128-register variant only for <= 4 energies per thread
+      if (mb == 6 && ept > 2) continue;  // the 80-register variant only for <= 2 energies per thread
       int st = sc_batch_config(b, lg, mb);
       if (st != SC_OK) return st;
       double ms = 0.0;
