@@ -408,13 +408,8 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
         const size_t fi = (size_t)y * n1 + x;
         fg[fi] = make_double2(sfr, sfi);
         gi[fi] = make_double2(sg, -si);
-        if (A.pair) {
-          // Partner angle at the mirrored site: gamma' = conj(gammaTilde),
-          // gammaTilde' = conj(gamma) give F' = F, Re g' = -Re g, Re I' = Re I.
-          const size_t pf = (size_t)A.pair * nn1 + (size_t)(n1 - 1 - y) * n1 + (n1 - 1 - x);
-          fg[pf] = make_double2(sfr, sfi);
-          gi[pf] = make_double2(-sg, -si);
-        }
+        // The mirrored partner angle is not stored: k_rotate_back reads it
+        // from this frame at the mirrored site.
       }
     }
   }
@@ -488,8 +483,13 @@ __global__ void k_halo(int n_entries, int entry0, int n1, const int *__restrict_
 // Rotation of the frame Green sums back to the reference grid, accumulated in
 // angle order (ComputeOrderParameter.h:174-210, ComputeCurrent.h:142-173,
 // ComputeFreeEnergy.h:260-279).
+// With pair > 0 (mixed precision, mirrored angles) the frames hold only the
+// angles [a_begin, a_end) of the first half; angle a + pair is read from the
+// frame of a at the mirrored site (n1-1-x, n1-1-y) with gamma' = conj(gammaTilde),
+// gammaTilde' = conj(gamma): F' = F, Re g' = -Re g, Re I' = Re I.  The angles
+// are then accumulated in the order a, a + pair, a + 1, ...
 __global__ void __launch_bounds__(256) k_rotate_back(int n0, int n1, int nc, int a_begin,
-                                                     int a_end, const AngleParams *__restrict__ ang,
+                                                     int a_end, int pair, const AngleParams *__restrict__ ang,
                                                      const double2 *__restrict__ fg,
                                                      const double2 *__restrict__ gi,
                                                      double *acc_d, double *acc_j, double *acc_fe) {
@@ -504,13 +504,27 @@ __global__ void __launch_bounds__(256) k_rotate_back(int n0, int n1, int nc, int
     di[c] = acc_d[(size_t)(2 * c + 1) * nn0 + i];
   }
   double jx = acc_j[i], jy = acc_j[nn0 + i], fe = acc_fe[i];
-  for (int a = a_begin; a < a_end; ++a) {
+  const int last = (pair ? 2 : 1) * (a_end - a_begin);
+  for (int k = 0; k < last; ++k) {
+    const int a0 = a_begin + (pair ? k >> 1 : k);
+    const bool mirrored = pair && (k & 1);
+    const int a = mirrored ? a0 + pair : a0;
     const AngleParams &P = ang[a];
     Bilinear b;
     if (!rotated_lookup(x, y, n0, n1, P.cB, P.sB, b)) continue;
-    const size_t base = (size_t)(a - a_begin) * nn1 + b.i00;
-    const double2 f00 = fg[base], f01 = fg[base + 1], f10 = fg[base + n1], f11 = fg[base + n1 + 1];
-    const double2 q00 = gi[base], q01 = gi[base + 1], q10 = gi[base + n1], q11 = gi[base + n1 + 1];
+    double2 f00, f01, f10, f11, q00, q01, q10, q11;
+    const size_t slot = (size_t)(a0 - a_begin) * nn1;
+    if (!mirrored) {
+      const size_t base = slot + b.i00;
+      f00 = fg[base]; f01 = fg[base + 1]; f10 = fg[base + n1]; f11 = fg[base + n1 + 1];
+      q00 = gi[base]; q01 = gi[base + 1]; q10 = gi[base + n1]; q11 = gi[base + n1 + 1];
+    } else {
+      // corner (xi + dx, yi + dy) of angle a is site nn1 - 1 - i00 - dx - n1 dy of angle a0
+      const size_t m = slot + (nn1 - 1 - (size_t)b.i00);
+      f00 = fg[m]; f01 = fg[m - 1]; f10 = fg[m - n1]; f11 = fg[m - n1 - 1];
+      q00 = gi[m]; q01 = gi[m - 1]; q10 = gi[m - n1]; q11 = gi[m - n1 - 1];
+      q00.x = -q00.x; q01.x = -q01.x; q10.x = -q10.x; q11.x = -q11.x;
+    }
     const double fre = bilerp(f00.x, f01.x, f10.x, f11.x, b.xf, b.yf);
     const double fim = bilerp(f00.y, f01.y, f10.y, f11.y, b.xf, b.yf);
     for (int c = 0; c < nc; ++c) {
@@ -1483,9 +1497,19 @@ void accelerate(sc_ctx *c) {
 }
 
 // Frame extension and rotation back of one swept chunk.
+int chunk_pair(const sc_ctx *c, const Chunk &ch) {
+  return (c->pair && ch.a_begin == 0 && ch.a_end == c->S.n_angles) ? c->pair : 0;
+}
+// Frame slots of a chunk: with mirrored pairs only the first half is stored.
+int chunk_slots(const sc_ctx *c, const Chunk &ch) {
+  return chunk_pair(c, ch) ? c->pair : ch.a_end - ch.a_begin;
+}
+
 void frame_to_reference(sc_ctx *c, const Chunk &ch) {
   const HostSetup &S = c->S;
-  const int h0 = S.halo_angle_off[ch.a_begin], h1 = S.halo_angle_off[ch.a_end];
+  const int pair = chunk_pair(c, ch);
+  const int a_stored = ch.a_begin + chunk_slots(c, ch);
+  const int h0 = S.halo_angle_off[ch.a_begin], h1 = S.halo_angle_off[a_stored];
   if (h1 > h0) {
     k_halo<<<grid1(h1 - h0, 128), 128, 0, c->stream>>>(h1 - h0, h0, S.n1, c->halo_angle.p, ch.a_begin,
                                                         c->halo_site.p, c->halo_off.p, c->halo_src.p,
@@ -1494,7 +1518,7 @@ void frame_to_reference(sc_ctx *c, const Chunk &ch) {
   }
   dim3 blk(32, 8), grid((S.n0 + 31) / 32, (S.n0 + 7) / 8);
   ProfScope prof(c, 1);
-  k_rotate_back<<<grid, blk, 0, c->stream>>>(S.n0, S.n1, S.nc, ch.a_begin, ch.a_end, c->ang.p,
+  k_rotate_back<<<grid, blk, 0, c->stream>>>(S.n0, S.n1, S.nc, ch.a_begin, a_stored, pair, c->ang.p,
                                              (const double2 *)c->w_fg, (const double2 *)c->w_gi,
                                              c->acc_d.p, c->acc_j.p, c->acc_fe.p);
   check_launch(c);
@@ -1535,7 +1559,7 @@ void run_chunks(sc_ctx *c, int burn_in) {
   }
   const bool clear = c->chunks.size() > 1 || !c->frames_zeroed;
   for (const Chunk &ch : c->chunks) {
-    const int nslots = ch.a_end - ch.a_begin;
+    const int nslots = chunk_slots(c, ch);
     if (!burn_in && clear) {
       CUDA_TRY(cudaMemsetAsync(c->w_fg, 0, (size_t)nslots * nn1 * sizeof(double2), c->stream));
       CUDA_TRY(cudaMemsetAsync(c->w_gi, 0, (size_t)nslots * nn1 * sizeof(double2), c->stream));
@@ -1699,7 +1723,7 @@ void plan_chunks(sc_ctx *c, std::vector<int4> &items) {
       ch.kmax = std::max(ch.kmax, kmax[b]);
     }
     ch.item_end = (int)items.size();
-    const double need = (double)items.size() * ch.kmax * per_row + (double)na * frame_slot;
+    const double need = (double)items.size() * ch.kmax * per_row + (double)(na / 2) * frame_slot;
     if (need <= budget) {
       c->chunks.push_back(ch);
       return;
@@ -1894,7 +1918,7 @@ void upload_static(sc_ctx *c) {
     const size_t ni = (size_t)(ch.item_end - ch.item_begin);
     scr = std::max(scr, ni * ch.kmax * S.ne * c->esize());
     scr2 = std::max(scr2, ni * ch.kmax * 3);
-    max_slots = std::max(max_slots, ch.a_end - ch.a_begin);
+    max_slots = std::max(max_slots, chunk_slots(c, ch));
   }
   c->need_scratch = scr + 8;
   c->need_scratch2 = (scr2 + 1) * sizeof(double);
@@ -2685,7 +2709,7 @@ void batch_sweeps(sc_batch *b) {
       sc_ctx *c = b->grains[g];
       const Chunk &ch = c->chunks[0];
       const size_t nn1 = (size_t)c->S.n1 * c->S.n1;
-      const int nslots = ch.a_end - ch.a_begin;
+      const int nslots = chunk_slots(c, ch);
       if (!c->frames_zeroed) {
         CUDA_TRY(cudaMemsetAsync(c->w_fg, 0, (size_t)nslots * nn1 * sizeof(double2), c->stream));
         CUDA_TRY(cudaMemsetAsync(c->w_gi, 0, (size_t)nslots * nn1 * sizeof(double2), c->stream));
