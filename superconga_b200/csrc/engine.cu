@@ -168,6 +168,32 @@ __device__ __forceinline__ void group_sum(double &v, int groups, unsigned mask) 
   for (int o = groups >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
 }
 
+// Sum of four values over the G threads of a group, scattered: afterwards the
+// thread whose group index has bits (b1 b0) in the two highest positions holds
+// the total of value 2 b1 + b0 (G >= 4), or of values {2 b0, 2 b0 + 1} in v[0],
+// v[1] (G = 2).  Halving the exchanged set in each of the first two rounds
+// takes 3 (G = 2: 2, G = 8: 4) shuffles instead of 4 log2(G).
+__device__ __forceinline__ void group_sum4_scatter(double v[4], int g, int log_groups, unsigned mask) {
+  if (log_groups == 0) return;
+  int o = 1 << (log_groups - 1);
+  {  // keep two of four
+    const bool up = (g & o) != 0;
+    const double s0 = up ? v[0] : v[2], s1 = up ? v[1] : v[3];
+    const double r0 = __shfl_xor_sync(mask, s0, o), r1 = __shfl_xor_sync(mask, s1, o);
+    v[0] = (up ? v[2] : v[0]) + r0;
+    v[1] = (up ? v[3] : v[1]) + r1;
+  }
+  o >>= 1;
+  if (!o) return;
+  {  // keep one of two
+    const bool up = (g & o) != 0;
+    const double sv = up ? v[0] : v[1];
+    const double r = __shfl_xor_sync(mask, sv, o);
+    v[0] = (up ? v[1] : v[0]) + r;
+  }
+  for (o >>= 1; o > 0; o >>= 1) v[0] += __shfl_xor_sync(mask, v[0], o);
+}
+
 // Rotated order parameter and Doppler shift of every site of every trajectory
 // column of a chunk, written to scratch2[row][3][item] for the sweep.
 template <typename R>
@@ -398,18 +424,24 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
             si += rr * (double)iim;
           }
       }
-      if (A.groups > 1) {
-        group_sum(sfr, A.groups, gmask);
-        group_sum(sfi, A.groups, gmask);
-        group_sum(sg, A.groups, gmask);
-        group_sum(si, A.groups, gmask);
-      }
-      if (g == 0) {
-        const size_t fi = (size_t)y * n1 + x;
-        fg[fi] = make_double2(sfr, sfi);
-        gi[fi] = make_double2(sg, -si);
-        // The mirrored partner angle is not stored: k_rotate_back reads it
-        // from this frame at the mirrored site.
+      // The mirrored partner angle is not stored: k_rotate_back reads it
+      // from this frame at the mirrored site.
+      const size_t fi = (size_t)y * n1 + x;
+      double v[4] = {sfr, sfi, sg, -si};
+      const int lg = A.log_groups;
+      group_sum4_scatter(v, g, lg, gmask);
+      if (lg == 0) {
+        fg[fi] = make_double2(v[0], v[1]);
+        gi[fi] = make_double2(v[2], v[3]);
+      } else if (lg == 1) {
+        (g ? gi : fg)[fi] = make_double2(v[0], v[1]);
+      } else {
+        const int sh = lg - 2;  // low bits below the two value bits
+        if ((g & ((1 << sh) - 1)) == 0) {
+          const int k = g >> sh;  // value index 0..3
+          double *dst = (double *)((k < 2 ? fg : gi) + fi);
+          dst[k & 1] = v[0];
+        }
       }
     }
   }
