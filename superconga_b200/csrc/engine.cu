@@ -1913,8 +1913,18 @@ void upload_static(sc_ctx *c) {
   const int per_thread = fp32_sweep ? 2 : 4;
   int want = 1;
   if (eg) want = std::atoi(eg);
-  else
+  else {
     while ((S.ne + want - 1) / want > per_thread && want < 8) want *= 2;
+    // Small grains: too few trajectory columns to fill the GPU twice over,
+    // so spread the energies over more threads per column.
+    int dev = 0, n_sm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    const double resident = (double)n_sm * (fp32_sweep ? 6 : 4) * 128;
+    size_t max_items = 0;
+    for (const Chunk &ch : c->chunks) max_items = std::max(max_items, (size_t)(ch.item_end - ch.item_begin));
+    while ((double)max_items * want < 2.0 * resident && want < 8 && (S.ne + want - 1) / want > 1) want *= 2;
+  }
   while (c->groups < want && c->groups < 8) {
     c->groups *= 2;
     c->log_groups++;

@@ -8,7 +8,13 @@ from tests import configs
 
 pytestmark = pytest.mark.gpu
 
-EPS = 1e-6
+# Central differences along random directions whose entries are of order
+# Delta_bulk (order-parameter part), 0.05 (vector potential) and 0.01 (field).
+# The step 1e-4 perturbs each site by ~3e-5 Delta_bulk: small enough that the
+# truncation error stays below 1e-7 relative, large enough that the rounding
+# error of the free energy (a sum over the whole grain) does not swamp small
+# directional derivatives, as it does for steps of 1e-6 and below.
+EPS = 1e-4
 TOL = 1e-6  # relative agreement of directional derivatives
 
 
