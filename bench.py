@@ -380,6 +380,67 @@ def ldos_c5(iters: int):
     return out
 
 
+def adjoint_c4(n_dirs: int = 64, eps: float = 1e-4):
+    """The adjoint on C4 (chiral d + i d_xy disc R = 15 xi0 @15/xi0, 128 angles,
+    T = 0.3, b = 0.05, kappa = 2), FP64, frozen boundary after 5 burn-in
+    iterations: device time of one frozen-boundary evaluation and of one
+    adjoint, and the largest relative difference between the adjoint's
+    directional derivatives and central differences (step eps) along n_dirs
+    seeded random directions, for the free energy and for the total azimuthal
+    current in a 2 xi0 ring at the edge."""
+    import numpy as np
+    import torch
+    import superconga_b200 as sb
+    from superconga_b200 import workloads
+    from superconga_b200.autograd import edge_current_weights
+    cfg = workloads.c4()
+    e = sb.Context(cfg, mode="fp64")
+    n0 = e.dims.n0
+    d, a = workloads.initial_state("c4", cfg, n0)
+    a = 0.05 * np.random.default_rng(44).standard_normal((2, n0, n0))
+    e.set_state(d, a)
+    e.burn_in(5)
+    dom = e.domain() > 0
+    d = d * dom
+    h = 1.0 / cfg["numerics"]["points_per_coherence_length"]
+    beta = edge_current_weights(e.domain(), h, 2.0)
+    b0 = e.external_field()
+    db = workloads.delta_bulk(0.3, "dx2-y2")
+
+    def f(dd, aa, bb, loss):
+        e.set_state(dd, aa)
+        e.set_external_field(bb)
+        fe = e.evaluate()
+        return fe if loss == "omega" else float(np.sum(beta * e.results()[1]))
+
+    out = {"workload": "c4: chiral d+id disc R=15 xi0 @15/xi0 (N0=%d), 128 angles, T=0.3, b=0.05, kappa=2" % n0,
+           "directions": n_dirs, "fd_step": eps}
+    for loss in ("omega", "edge_current"):
+        f(d, a, b0, loss)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        gd, ga, gb = e.adjoint(1.0, None) if loss == "omega" else e.adjoint(0.0, beta)
+        t_adj = time.perf_counter() - t0
+        rng = np.random.default_rng(4)
+        worst = 0.0
+        t_eval = []
+        for _ in range(n_dirs):
+            vd = rng.standard_normal(d.shape) * db * dom
+            va = rng.standard_normal(a.shape) * 0.05
+            vb = float(rng.standard_normal()) * 0.01
+            t0 = time.perf_counter()
+            fp = f(d + eps * vd, a + eps * va, b0 + eps * vb, loss)
+            t_eval.append(time.perf_counter() - t0)
+            fm = f(d - eps * vd, a - eps * va, b0 - eps * vb, loss)
+            fd = (fp - fm) / (2 * eps)
+            ad = float(np.sum(gd * vd) + np.sum(ga * va) + gb * vb)
+            worst = max(worst, abs(fd - ad) / max(abs(fd), abs(ad), 1e-300))
+        out[loss] = {"adjoint_s": t_adj, "evaluation_s": float(np.median(t_eval)),
+                     "max_rel_diff_vs_fd": worst}
+    e.close()
+    return out
+
+
 def run_engine(args):
     import torch
 
@@ -445,9 +506,11 @@ def run_engine(args):
     if rank == 0 and world == 1 and not args.no_converge:
         extra["time_to_converge"] = converge_c1(args.converge_max_it, args.converge_max_s)
     if rank == 0 and world == 1 and not args.no_batch:
-        extra["batched"] = batched_c3(args.batch_grains, args.batch_iters, args.converge_max_s)
+        extra["batched"] = batched_c3(args.batch_grains, args.batch_iters, args.batch_max_s)
     if rank == 0 and world == 1 and args.ldos:
         extra["ldos"] = ldos_c5(2)
+    if rank == 0 and world == 1 and not args.no_adjoint:
+        extra["adjoint"] = adjoint_c4()
     sampler.__exit__(None, None, None)
     clocks = sampler.summary()
 
@@ -496,6 +559,8 @@ def main():
     ap.add_argument("--batch-grains", type=int, default=128)
     ap.add_argument("--batch-iters", type=int, default=5)
     ap.add_argument("--ldos", action="store_true", help="also time the C5 LDOS postprocess")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--batch-max-s", type=float, default=120.0)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

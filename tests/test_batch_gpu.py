@@ -119,3 +119,35 @@ def test_batch_converges_independently(engine_lib):
         fe = b.grains[k].scalars()["free_energy_per_area"]
         assert abs(fe - configs.GOLDEN_FREE_ENERGY_PER_AREA) <= 1e-3 * abs(configs.GOLDEN_FREE_ENERGY_PER_AREA)
     b.close()
+
+
+def test_batch_vs_oracle(engine_lib):
+    """Seeded grains of the batched workload (coarsened to 3 points/xi0 so the
+    CPU oracle runs them in seconds), advanced together in one FP64 batch,
+    against the oracle run grain by grain: two iterations within 1e-10."""
+    import superconga_b200 as sb
+    from oracle import oracle as O
+    from superconga_b200 import workloads
+    cfgs, states = workloads.c3_grains(128, ppxi=3.0)
+    pick = [0, 1, 64, 65]  # two discs, two squares
+    cfgs = [cfgs[i] for i in pick]
+    states = [states[i] for i in pick]
+    b = sb.Batch(cfgs, mode="fp64")
+    oracles = []
+    for g, c, st in zip(b.grains, cfgs, states):
+        d, a = workloads.c3_initial_state(c, st, g.dims.n0)
+        g.set_state(d, a)
+        o = O.Oracle(c)
+        o.set_state(d, a)
+        oracles.append(o)
+    for it in range(2):
+        b.compute(1)
+        for o in oracles:
+            o.compute()
+        for g, o in zip(b.grains, oracles):
+            d_b, j_b, _ = g.results()
+            d_o, j_o, _ = o.results()
+            assert _rel(d_b, d_o) < 1e-10, it
+            assert _rel(j_b, j_o) < 1e-10, it
+            assert abs(g.scalars()["free_energy"] - o.scalars()["free_energy"]) <= 1e-10 * abs(o.scalars()["free_energy"])
+    b.close()
