@@ -340,7 +340,7 @@ def batched_c3(n_grains: int, iters: int, max_s: float):
                      "ms_per_iteration": ms, "site_updates_per_iteration": su,
                      "all_grains_active_while_timed": full,
                      "kernel_launches_per_iteration": launches,
-                     "sweep_mapping": {"threads_per_column": 1 << lg, "min_blocks_per_sm": mb},
+                     "sweep_mapping": {"max_energies_per_thread": lg, "min_blocks_per_sm": mb},
                      "seconds_all_grains": time.perf_counter() - t0,
                      "grains_converged": int(sum(conv)), "grains_at_iteration_cap": int(np.sum(~act) - sum(conv)),
                      "grains_still_running": int(np.sum(act)),

@@ -216,14 +216,15 @@ int sc_batch_compute(sc_batch *b, int n, int *n_active);
 int sc_batch_status(const sc_batch *b, int *active, int *iterations, double *residual);
 /* CUDA-graph replay of the iteration on (default) or off. */
 int sc_batch_set_graph(sc_batch *b, int enable);
-/* Mapping of the persistent sweep: 2^log_groups threads per trajectory column
- * and the resident-block variant minb (1: up to 255 registers per thread,
- * 4: at most 128, 6: at most 80 with at most two energies per thread).
- * sc_batch_autotune times every feasible choice on the current state (after
- * at least one iteration) and keeps the fastest. */
-int sc_batch_config(sc_batch *b, int log_groups, int minb);
-int sc_batch_get_config(const sc_batch *b, int *log_groups, int *minb, int *n_waves);
-int sc_batch_autotune(sc_batch *b, int *log_groups, int *minb, double *best_ms);
+/* Mapping of the persistent sweep: each grain takes the fewest threads per
+ * trajectory column (1, 2, 4 or 8) that keep at most energies_per_thread
+ * energies on a thread, and minb selects the resident-block variant (1: up
+ * to 255 registers per thread, 4: at most 128, 6: at most 80 with at most two
+ * energies per thread).  sc_batch_autotune times the feasible choices on the
+ * current state (after at least one iteration) and keeps the fastest. */
+int sc_batch_config(sc_batch *b, int energies_per_thread, int minb);
+int sc_batch_get_config(const sc_batch *b, int *energies_per_thread, int *minb, int *n_waves);
+int sc_batch_autotune(sc_batch *b, int *energies_per_thread, int *minb, double *best_ms);
 /* Device time of the sweeps of all waves (average of `repeats`), state unchanged. */
 int sc_batch_time_sweeps(sc_batch *b, int repeats, double *ms);
 int sc_batch_launch_count(const sc_batch *b, long long *count);

@@ -45,9 +45,20 @@ __device__ __forceinline__ double rcp_(double x) {
   return fma(r, e, r);
 }
 __device__ __forceinline__ float rcp_(float x) { return __fdividef(1.0f, x); }
-__device__ __forceinline__ double rsqrt_(double x) { return rsqrt(x); }
+// FP64 reciprocal square root of a positive normal argument: the hardware
+// approximation refined by two Newton-Raphson steps r <- r + r (1 - x r^2) / 2.
+__device__ __forceinline__ double rsqrt_(double x) {
+  double r;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+  double e = fma(-x * r, r, 1.0);
+  r = fma(0.5 * r, e, r);
+  e = fma(-x * r, r, 1.0);
+  return fma(0.5 * r, e, r);
+}
 __device__ __forceinline__ float rsqrt_(float x) { return rsqrtf(x); }
-__device__ __forceinline__ double sqrt_(double x) { return x > 0.0 ? x * rsqrt(x) : 0.0; }
+__device__ __forceinline__ double sqrt_(double x) {
+  return x >= 2.2250738585072014e-308 ? x * rsqrt_(x) : 0.0;  // 0 below the smallest normal
+}
 __device__ __forceinline__ float sqrt_(float x) { return x > 0.0f ? x * rsqrtf(x) : 0.0f; }
 
 // Principal square root, branch cut on the negative real axis, through one

@@ -466,16 +466,13 @@ __global__ void __launch_bounds__(128, MINB) k_sweep(const SweepArgs<R> A) {
 // warp's worth of trajectory columns (32 / G of them) of one grain; warps take
 // units from a global counter, longest columns first (the unit list is sorted
 // by the host), so ragged grains share the GPU without a tail per grain.  All
-// grains of a batch use the same G = 2^log_groups threads per column.
+// grain has its own G = 2^log_groups threads per column (the warp's unit
+// belongs to one grain, so the mapping is uniform within a warp).
 template <typename R, int EMAX, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_sweep_batch(const SweepArgs<R> *__restrict__ args,
                                                            const int2 *__restrict__ units, int n_units,
-                                                           int *counter, int log_groups) {
+                                                           int *counter) {
   const int lane = threadIdx.x & 31;
-  const int groups = 1 << log_groups;
-  const int g = lane & (groups - 1);
-  const int sub = lane >> log_groups;
-  const unsigned gmask = ((groups == 32) ? 0xffffffffu : ((1u << groups) - 1u)) << (lane & ~(groups - 1));
   for (;;) {
     int u = 0;
     if (lane == 0) u = atomicAdd(counter, 1);
@@ -483,6 +480,10 @@ __global__ void __launch_bounds__(128, MINB) k_sweep_batch(const SweepArgs<R> *_
     if (u >= n_units) break;
     const int2 wu = units[u];
     const SweepArgs<R> &A = args[wu.x];
+    const int lg = A.log_groups, groups = 1 << lg;
+    const int g = lane & (groups - 1);
+    const int sub = lane >> lg;
+    const unsigned gmask = ((groups == 32) ? 0xffffffffu : ((1u << groups) - 1u)) << (lane & ~(groups - 1));
     const int item = wu.y + sub;
     if (item < A.n_items) sweep_column<R, EMAX, false>(A, A.res, item, g, gmask);
   }
@@ -2567,7 +2568,7 @@ struct sc_batch {
   int mode = SC_MODE_FP64;
   cudaStream_t stream = nullptr;
   std::string err;
-  int log_groups = 2;  // threads per trajectory column: 2^log_groups
+  int ept_max = 4;     // at most this many energies per thread; each grain the fewest threads per column that allow it
   int minb = 1;        // resident-block variant of the persistent sweep
   int n_sm = 148;
   std::vector<char> active;
@@ -2655,7 +2656,7 @@ void batch_plan(sc_batch *b) {
     members[w].push_back(g);
   }
   b->waves.clear();
-  const int G = 1 << b->log_groups, per_warp = 32 >> b->log_groups;
+
   for (auto &m : members) {
     auto wv = std::make_unique<sc_batch::Wave>();
     wv->grains = m;
@@ -2663,9 +2664,12 @@ void batch_plan(sc_batch *b) {
     std::vector<std::pair<int, int2>> keyed;  // (column length, unit)
     for (int k = 0; k < (int)m.size(); ++k) {
       sc_ctx *c = b->grains[m[k]];
-      c->groups = G;
-      c->log_groups = b->log_groups;
-      c->ept = (c->S.ne + G - 1) / G;
+      c->log_groups = 0;
+      while (((c->S.ne + (1 << c->log_groups) - 1) >> c->log_groups) > b->ept_max && c->log_groups < 3)
+        c->log_groups++;
+      c->groups = 1 << c->log_groups;
+      c->ept = (c->S.ne + c->groups - 1) / c->groups;
+      const int per_warp = 32 >> c->log_groups;
       const Chunk &ch = c->chunks[0];
       args.push_back(sweep_args<R>(c, &ch, 0));
       const int n = ch.item_end - ch.item_begin;
@@ -2704,7 +2708,7 @@ void launch_batch_sweep(sc_batch *b, sc_batch::Wave &w, int wi) {
     int per_sm = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 128, 0);
     const int blocks = std::max(1, per_sm) * b->n_sm;
-    kernel<<<blocks, 128, 0, b->stream>>>(args, w.units.p, w.n_units, counter, b->log_groups);
+    kernel<<<blocks, 128, 0, b->stream>>>(args, w.units.p, w.n_units, counter);
   };
   if (ept <= 2 && b->minb == 6) {
     run(k_sweep_batch<R, 2, 6>);
@@ -2918,12 +2922,9 @@ int sc_batch_create(const char *const *configs, int n, int mode, sc_batch **out)
     b->scalar_src.upload(src, b->stream);
     b->scalars.alloc(n);
     b->host_scalars.resize(n);
-    // Threads per column: enough that no thread integrates more than four
-    // energies of the grain with the most energies.
-    int ne_max = 1;
-    for (sc_ctx *c : b->grains) ne_max = std::max(ne_max, c->S.ne);
-    b->log_groups = 0;
-    while (((ne_max + (1 << b->log_groups) - 1) >> b->log_groups) > 4 && b->log_groups < 3) b->log_groups++;
+    // Threads per column, per grain: the fewest that keep at most four (FP64)
+    // or two (mixed) energies per thread.
+    b->ept_max = mode == SC_MODE_FP64 ? 4 : 2;
     b->minb = mode == SC_MODE_FP64 ? 4 : 1;
     if (mode == SC_MODE_FP64) batch_plan<double>(b);
     else batch_plan<float>(b);
@@ -2999,14 +3000,16 @@ int sc_batch_set_graph(sc_batch *b, int enable) {
   return SC_OK;
 }
 
-int sc_batch_config(sc_batch *b, int log_groups, int minb) {
-  if (!b || log_groups < 0 || log_groups > 3 || (minb != 1 && minb != 4 && minb != 6)) return SC_ERR_ARG;
+int sc_batch_config(sc_batch *b, int energies_per_thread, int minb) {
+  const int e = energies_per_thread;
+  if (!b || !(e == 1 || e == 2 || e == 4 || e == 8 || e == 16) || (minb != 1 && minb != 4 && minb != 6))
+    return SC_ERR_ARG;
   int ne_max = 1;
   for (sc_ctx *c : b->grains) ne_max = std::max(ne_max, c->S.ne);
-  if (((ne_max + (1 << log_groups) - 1) >> log_groups) > 16) return SC_ERR_ARG;
+  if ((ne_max + 7) / 8 > 16) return SC_ERR_ARG;
   try {
     CUDA_TRY(cudaStreamSynchronize(b->stream));
-    b->log_groups = log_groups;
+    b->ept_max = e;
     b->minb = minb;
     if (b->mode == SC_MODE_FP64) batch_plan<double>(b);
     else batch_plan<float>(b);
@@ -3016,9 +3019,9 @@ int sc_batch_config(sc_batch *b, int log_groups, int minb) {
   return SC_OK;
 }
 
-int sc_batch_get_config(const sc_batch *b, int *log_groups, int *minb, int *n_waves) {
+int sc_batch_get_config(const sc_batch *b, int *energies_per_thread, int *minb, int *n_waves) {
   if (!b) return SC_ERR_ARG;
-  if (log_groups) *log_groups = b->log_groups;
+  if (energies_per_thread) *energies_per_thread = b->ept_max;
   if (minb) *minb = b->minb;
   if (n_waves) *n_waves = (int)b->waves.size();
   return SC_OK;
@@ -3065,39 +3068,33 @@ int sc_batch_launch_count(const sc_batch *b, long long *count) {
 
 extern "C" {
 
-// Autotuner of the persistent batch sweep: tries every feasible mapping of
-// trajectory columns to threads (2, 4 or 8 threads per column, i.e. 16, 8 or 4
-// columns per warp) and both resident-block variants (register budget of 255
-// or 128 per thread), times the sweeps of all waves for each on the current
-// state, keeps the fastest and returns it.
-int sc_batch_autotune(sc_batch *b, int *log_groups, int *minb, double *best_ms) {
+// Autotuner of the persistent batch sweep: tries the mappings of trajectory
+// columns to threads (at most 1, 2, 4 or 8 energies per thread, each grain
+// taking the fewest threads per column that allow it, up to 8) with the
+// resident-block variants that fit them (registers capped at 80, 128 or 255
+// per thread), times the sweeps of all waves for each on the current state,
+// keeps the fastest and returns it.
+int sc_batch_autotune(sc_batch *b, int *energies_per_thread, int *minb, double *best_ms) {
   if (!b) return SC_ERR_ARG;
-  int ne_max = 1;
-  for (sc_ctx *c : b->grains) ne_max = std::max(ne_max, c->S.ne);
-  int best_lg = b->log_groups, best_mb = b->minb;
+  const int cand[][2] = {{1, 6}, {2, 6}, {2, 1}, {4, 4}, {4, 1}, {8, 1}};
+  int best_e = b->ept_max, best_mb = b->minb;
   double best = 1e300;
-  for (int lg = 1; lg <= 3; ++lg) {
-    const int ept = (ne_max + (1 << lg) - 1) >> lg;
-    if (ept > 16) continue;
-    for (int mb : {1, 4, 6}) {
-      if (mb == 4 && ept > 4) continue;  // the 128-register variant only for <= 4 energies per thread
-      if (mb == 6 && ept > 2) continue;  // the 80-register variant only for <= 2 energies per thread
-      int st = sc_batch_config(b, lg, mb);
-      if (st != SC_OK) return st;
-      double ms = 0.0;
-      st = sc_batch_time_sweeps(b, 1, &ms);  // warm-up
-      if (st == SC_OK) st = sc_batch_time_sweeps(b, 2, &ms);
-      if (st != SC_OK) return st;
-      if (ms < best) {
-        best = ms;
-        best_lg = lg;
-        best_mb = mb;
-      }
+  for (const auto &cd : cand) {
+    int st = sc_batch_config(b, cd[0], cd[1]);
+    if (st != SC_OK) return st;
+    double ms = 0.0;
+    st = sc_batch_time_sweeps(b, 1, &ms);  // warm-up
+    if (st == SC_OK) st = sc_batch_time_sweeps(b, 2, &ms);
+    if (st != SC_OK) return st;
+    if (ms < best) {
+      best = ms;
+      best_e = cd[0];
+      best_mb = cd[1];
     }
   }
-  const int st = sc_batch_config(b, best_lg, best_mb);
+  const int st = sc_batch_config(b, best_e, best_mb);
   if (st != SC_OK) return st;
-  if (log_groups) *log_groups = best_lg;
+  if (energies_per_thread) *energies_per_thread = best_e;
   if (minb) *minb = best_mb;
   if (best_ms) *best_ms = best;
   return SC_OK;

@@ -443,8 +443,10 @@ class Batch:
     def set_graph(self, enable: bool):
         self._check(_lib.load().sc_batch_set_graph(self._h, int(bool(enable))))
 
-    def config(self, log_groups: int, minb: int):
-        self._check(_lib.load().sc_batch_config(self._h, int(log_groups), int(minb)))
+    def config(self, energies_per_thread: int, minb: int):
+        """Each grain takes the fewest threads per column that keep at most
+        ``energies_per_thread`` energies on a thread; ``minb`` the register variant."""
+        self._check(_lib.load().sc_batch_config(self._h, int(energies_per_thread), int(minb)))
 
     def get_config(self):
         v = [ctypes.c_int() for _ in range(3)]
@@ -452,6 +454,7 @@ class Batch:
         return tuple(x.value for x in v)
 
     def autotune(self):
+        """Returns the chosen (energies per thread, minb) and the sweep time in ms."""
         lg, mb, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
         self._check(_lib.load().sc_batch_autotune(self._h, ctypes.byref(lg), ctypes.byref(mb), ctypes.byref(ms)))
         return lg.value, mb.value, ms.value

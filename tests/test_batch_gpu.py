@@ -74,9 +74,9 @@ def test_batch_autotune(engine_lib):
     for g, (d, a) in zip(b.grains, states):
         g.set_state(d, a)
     b.compute(1)
-    lg, mb, ms = b.autotune()
-    assert 1 <= lg <= 3 and mb in (1, 4, 6) and ms > 0
-    assert b.get_config()[:2] == (lg, mb)
+    ept, mb, ms = b.autotune()
+    assert ept in (1, 2, 4, 8) and mb in (1, 4, 6) and ms > 0
+    assert b.get_config()[:2] == (ept, mb)
     b.compute(2)
     ref = []
     for c, (d, a) in zip(cfgs, states):
