@@ -90,9 +90,9 @@ struct SweepArgs {
   const double *avec;  // [2][n0*n0]
   const double *e_re, *e_im, *res;
   Cx<R> *scratch;   // [row][energy][item]
-  double *scratch2; // [row][3][item]: Re D, Im D, energy shift
+  R *scratch2;      // [row][3][item]: Re D, Im D, energy shift (in R: the sweep steps in R)
   double2 *fg, *gi; // frame buffers [slot][n1*n1]: (Re F, Im F), (Re G, Re I)
-  double *ldf;      // LDOS frame buffer [slot][energy][n1*n1]: Im g per real energy
+  double *ldf;      // LDOS frame buffer [slot][n1*n1][energy]: Im g per real energy
 };
 
 // Gauges, include/conga/riccati/energy_shift/Gauges.h:25-62.
@@ -209,10 +209,10 @@ __global__ void __launch_bounds__(128) k_frame_fields(const SweepArgs<R> A, int 
   for (int r = r0; r < r1; ++r) {
     double dre, dim, es;
     frame_fields(A, P, x, lo + r, dre, dim, es);
-    double *s2 = A.scratch2 + (size_t)r * 3 * ni + item;
-    s2[0] = dre;
-    s2[ni] = dim;
-    s2[2 * ni] = es;
+    R *s2 = A.scratch2 + (size_t)r * 3 * ni + item;
+    s2[0] = (R)dre;
+    s2[ni] = (R)dim;
+    s2[2 * ni] = (R)es;
   }
 }
 
@@ -259,7 +259,7 @@ __device__ __forceinline__ void site_step(uint8_t l, uint8_t l_entry, uint8_t l_
 // scratch; gamma then runs up and the Green sums over all energies are formed
 // site by site (RiccatiSolverConfined.h:129-312, GreensFunctionStatic.h:92-157,
 // ComputeFreeEnergy.h:106-160).  The frame order parameter and the energies come
-// from scratch2 (FP64); the coherence functions are integrated in R.
+// from scratch2; the coherence functions are integrated in R.
 // KEL: real energies e_re + i e_im (the LDOS path, IntegrationIteratorKeldysh.h
 // :219-389); instead of the energy sums, Im g of every energy is written to the
 // LDOS frame buffer (GreensFunctionStatic.h:66-90, ComputeLDOS.h:123-144).
@@ -301,8 +301,8 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
 #pragma unroll
     for (int j = 0; j < EMAX; ++j) coh[j] = Cx<R>{R(0), R(0)};
     uint8_t l_nx = lab[(size_t)hi * n1 + x];
-    const double *s2 = A.scratch2 + (size_t)(hi - lo) * 3 * ni + item;
-    double f0 = s2[0], f1 = s2[ni], f2 = s2[2 * ni];
+    const R *s2 = A.scratch2 + (size_t)(hi - lo) * 3 * ni + item;
+    R f0 = s2[0], f1 = s2[ni], f2 = s2[2 * ni];
     for (int y = hi; y >= lo; --y) {
       const int r = y - lo;
       const uint8_t l = l_nx;
@@ -310,7 +310,7 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
       const R dre = (R)(-f0), dim = (R)f1, es = (R)f2;
       if (y > lo) {
         l_nx = lab[(size_t)(y - 1) * n1 + x];
-        const double *s2n = A.scratch2 + (size_t)(r - 1) * 3 * ni + item;
+        const R *s2n = A.scratch2 + (size_t)(r - 1) * 3 * ni + item;
         f0 = s2n[0];
         f1 = s2n[ni];
         f2 = s2n[2 * ni];
@@ -352,7 +352,7 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
     double2 *fg = A.fg + (size_t)(a - A.slot_base) * nn1;
     double2 *gi = A.gi + (size_t)(a - A.slot_base) * nn1;
     uint8_t l_nx = lab[(size_t)lo * n1 + x];
-    double f0 = A.scratch2[item], f1 = A.scratch2[ni + item], f2 = A.scratch2[2 * ni + item];
+    R f0 = A.scratch2[item], f1 = A.scratch2[ni + item], f2 = A.scratch2[2 * ni + item];
     Cx<R> gt_nx[EMAX];
     if (!A.burn_in) {
       const Cx<R> *sc = A.scratch + (size_t)e0 * ni + item;
@@ -369,7 +369,7 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
       for (int j = 0; j < EMAX; ++j) gt[j] = gt_nx[j];
       if (y < hi) {
         l_nx = lab[(size_t)(y + 1) * n1 + x];
-        const double *s2n = A.scratch2 + (size_t)(r + 1) * 3 * ni + item;
+        const R *s2n = A.scratch2 + (size_t)(r + 1) * 3 * ni + item;
         f0 = s2n[0];
         f1 = s2n[ni];
         f2 = s2n[2 * ni];
@@ -402,10 +402,10 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
       if (A.burn_in) continue;
       if constexpr (KEL) {
         if (l != 0) {
-          double *o = A.ldf + ((size_t)(a - A.slot_base) * ne + e0) * nn1 + (size_t)y * n1 + x;
+          double *o = A.ldf + ((size_t)(a - A.slot_base) * nn1 + (size_t)y * n1 + x) * ne + e0;
 #pragma unroll
           for (int j = 0; j < EMAX; ++j)
-            if (j < ecount) o[(size_t)j * nn1] = (double)greens_g_im<R>(coh[j], gt[j]);
+            if (j < ecount) o[j] = (double)greens_g_im<R>(coh[j], gt[j]);
         }
         continue;
       }
@@ -584,38 +584,53 @@ __global__ void k_halo_ldos(int n_entries, int entry0, int n1, int ne,
                             const int *__restrict__ entry_angle, int slot_base,
                             const int *__restrict__ site, const int *__restrict__ off,
                             const int *__restrict__ src, double *ldf) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n_entries) return;
+  // one thread per (entry, energy), energy fastest: the LDOS frame is
+  // [slot][site][energy]
+  const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (t >= (size_t)n_entries * ne) return;
+  const int k = (int)(t / ne), en_ = (int)(t % ne);
   const int e = entry0 + k;
-  const size_t nn1 = (size_t)n1 * n1;
-  double *f = ldf + ((size_t)(entry_angle[e] - slot_base) * ne + blockIdx.y) * nn1;
+  double *f = ldf + (size_t)(entry_angle[e] - slot_base) * n1 * n1 * ne + en_;
   const int b = off[e], en = off[e + 1];
-  double v = f[src[b]];
-  for (int i = b + 1; i < en; ++i) v = __dadd_rn(v, f[src[i]]);
-  f[site[e]] = __ddiv_rn(v, (double)(en - b));
+  double v = f[(size_t)src[b] * ne];
+  for (int i = b + 1; i < en; ++i) v = __dadd_rn(v, f[(size_t)src[i] * ne]);
+  f[(size_t)site[e] * ne] = __ddiv_rn(v, (double)(en - b));
 }
 
 // LDOS frames rotated back onto the reference grid and accumulated in angle
 // order, Im part weighted by the integrand factor (ComputeLDOS.h:140-144,
 // insertRotatedGridAdditive with Type::imag, GridFunctions_GPU.h:991-1054).
+// A thread takes one reference site and LDOS_E consecutive energies: one
+// lookup per angle serves all of them, and the corners' energies are
+// contiguous in the [slot][site][energy] frame.
+constexpr int LDOS_E = 8;
 __global__ void __launch_bounds__(256) k_rotate_back_ldos(int n0, int n1, int ne, int a_begin, int a_end,
                                                           const AngleParams *__restrict__ ang,
                                                           const double *__restrict__ ldf, double *acc) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int e = blockIdx.z;
+  const int e0 = blockIdx.z * LDOS_E;
   if (x >= n0 || y >= n0) return;
   const size_t nn0 = (size_t)n0 * n0, nn1 = (size_t)n1 * n1;
-  const size_t i = (size_t)e * nn0 + (size_t)y * n0 + x;
-  double v = acc[i];
+  const size_t i = (size_t)y * n0 + x;
+  const int ecount = min(LDOS_E, ne - e0);
+  double v[LDOS_E];
+#pragma unroll
+  for (int j = 0; j < LDOS_E; ++j) v[j] = (j < ecount) ? acc[(size_t)(e0 + j) * nn0 + i] : 0.0;
   for (int a = a_begin; a < a_end; ++a) {
     const AngleParams &P = ang[a];
     Bilinear b;
     if (!rotated_lookup(x, y, n0, n1, P.cB, P.sB, b)) continue;
-    const double *f = ldf + ((size_t)(a - a_begin) * ne + e) * nn1 + b.i00;
-    v += bilerp(f[0] * P.w, f[1] * P.w, f[n1] * P.w, f[n1 + 1] * P.w, b.xf, b.yf);
+    const double *f = ldf + ((size_t)(a - a_begin) * nn1 + b.i00) * ne + e0;
+    const size_t dx = (size_t)ne, dy = (size_t)n1 * ne;
+#pragma unroll
+    for (int j = 0; j < LDOS_E; ++j)
+      if (j < ecount)
+        v[j] += bilerp(f[j] * P.w, f[dx + j] * P.w, f[dy + j] * P.w, f[dy + dx + j] * P.w, b.xf, b.yf);
   }
-  acc[i] = v;
+#pragma unroll
+  for (int j = 0; j < LDOS_E; ++j)
+    if (j < ecount) acc[(size_t)(e0 + j) * nn0 + i] = v[j];
 }
 
 // ComputeLDOS::computePropertyFromGreens (ComputeLDOS.h:146-193): LDOS = -sum,
@@ -1377,7 +1392,7 @@ SweepArgs<R> sweep_args(sc_ctx *c, const Chunk *ch, int burn_in) {
   A.res = c->res.p;
   A.ldf = c->ldf.p;
   A.scratch = (Cx<R> *)c->w_scratch;
-  A.scratch2 = c->w_scratch2;
+  A.scratch2 = (R *)c->w_scratch2;
   A.fg = (double2 *)c->w_fg;
   A.gi = (double2 *)c->w_gi;
   return A;
@@ -1569,12 +1584,12 @@ void run_chunks_ldos(sc_ctx *c, int burn_in) {
     if (burn_in) continue;
     const int h0 = S.halo_angle_off[ch.a_begin], h1 = S.halo_angle_off[ch.a_end];
     if (h1 > h0) {
-      dim3 grid(grid1(h1 - h0, 128), S.ne);
-      k_halo_ldos<<<grid, 128, 0, c->stream>>>(h1 - h0, h0, S.n1, S.ne, c->halo_angle.p, ch.a_begin,
-                                               c->halo_site.p, c->halo_off.p, c->halo_src.p, c->ldf.p);
+      k_halo_ldos<<<grid1((size_t)(h1 - h0) * S.ne, 128), 128, 0, c->stream>>>(
+          h1 - h0, h0, S.n1, S.ne, c->halo_angle.p, ch.a_begin, c->halo_site.p, c->halo_off.p, c->halo_src.p,
+          c->ldf.p);
       check_launch(c);
     }
-    dim3 blk(32, 8), grid((S.n0 + 31) / 32, (S.n0 + 7) / 8, S.ne);
+    dim3 blk(32, 8), grid((S.n0 + 31) / 32, (S.n0 + 7) / 8, (S.ne + LDOS_E - 1) / LDOS_E);
     ProfScope prof(c, 1);
     k_rotate_back_ldos<<<grid, blk, 0, c->stream>>>(S.n0, S.n1, S.ne, ch.a_begin, ch.a_end, c->ang.p,
                                                     c->ldf.p, c->ldos_acc.p);
