@@ -81,6 +81,10 @@ __device__ __forceinline__ Cx<R> csqrt_dev(R x, R y) {
 //   a = i h/4 conj(D), b = 2 a g0 + i h e - 1, c = (a g0 + i h e + 1) g0 + i h D,
 //   g1 = 2 c / (-b + sqrt(b^2 - 4 a c)).
 // The products with the purely imaginary step are written out (they are exact).
+// With u = a g0 and B = i h e the discriminant reduces to
+//   b^2 - 4 a c = (B - 1)^2 + h^2 |D|^2 - 8 u,
+// because a (i h D) = -(h^2 / 4) |D|^2 is real; that form skips two complex
+// products and avoids the cancellation of b^2 against 4 a c.
 template <typename R>
 __device__ __forceinline__ Cx<R> riccati_step(R dre, R dim, R ere, R eim, Cx<R> g, R h) {
   const R q = R(0.25) * h;
@@ -91,9 +95,9 @@ __device__ __forceinline__ Cx<R> riccati_step(R dre, R dim, R ere, R eim, Cx<R> 
   const Cx<R> t{ag.re + ser + R(1), ag.im + sei};
   const Cx<R> tg = cmul(t, g);
   const Cx<R> c{tg.re - h * dim, tg.im + h * dre};
-  const Cx<R> bb = cmul(b, b);
-  const Cx<R> ac = cmul(a, c);
-  const Cx<R> disc = csqrt_dev<R>(bb.re - R(4) * ac.re, bb.im - R(4) * ac.im);
+  const R bm = ser - R(1);
+  const R hd2 = h * h * (dre * dre + dim * dim);
+  const Cx<R> disc = csqrt_dev<R>(bm * bm - sei * sei + hd2 - R(8) * ag.re, R(2) * bm * sei - R(8) * ag.im);
   const R den_re = disc.re - b.re, den_im = disc.im - b.im;
   const R inv = rcp_(den_re * den_re + den_im * den_im);
   const R c2r = R(2) * c.re, c2i = R(2) * c.im;
