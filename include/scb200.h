@@ -267,6 +267,17 @@ int sc_setup_filters(const sc_setup *s, int *n_filters, double *filters, int *po
                      double *scale);
 int sc_setup_site_updates(const sc_setup *s, long long *per_iteration);
 
+/* Load-path helpers for runs saved on another lattice (host only).
+ * sc_grid_extend: extendValuesAtBoundary (domain_ops.h:11-69) of n_fields
+ * planes [n_fields][n][n] in place, with the domain labels of that lattice.
+ * sc_grid_resample: GridFunctions::resample (GridFunctions_GPU.h:547-600,
+ * 1056-1091), bilinear onto an n_new lattice keeping the 3-site safety
+ * margin; sites that would read past the old lattice (only inside the margin
+ * when shrinking) take the nearest edge value.  Used by the drivers as the
+ * reference's CSV reader does (csv.h:180-205, 297-395). */
+int sc_grid_extend(int n, const signed char *domain, int n_fields, double *values);
+int sc_grid_resample(int n_old, int n_new, int n_fields, const double *src, double *dst);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1791,6 +1791,12 @@ void orc_evaluate(void *h) {
   o->integrate_all();
 }
 
+// extendValuesAtBoundary on a grid of side n (domain_ops.h:11-69), in place.
+void orc_extend_grid(int n, const signed char *labels, double *values) {
+  std::vector<char> lab(labels, labels + (size_t)n * n);
+  Oracle::extend(lab, n, values);
+}
+
 // External flux quanta (the field enters the energy shift through the gauge).
 void orc_set_flux(void *h, double flux_quanta) { ((Oracle *)h)->p.flux_quanta = flux_quanta; }
 

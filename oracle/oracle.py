@@ -641,6 +641,37 @@ class LdosOracle:
         return max(rl.value, rb.value), rl.value, rb.value
 
 
+def extend_grid(labels: np.ndarray, values: np.ndarray) -> np.ndarray:
+    """extendValuesAtBoundary of one plane (domain_ops.h:11-69)."""
+    n = labels.shape[0]
+    lab = np.ascontiguousarray(labels, np.int8)
+    out = np.ascontiguousarray(values, np.float64).copy()
+    lib().orc_extend_grid(ctypes.c_int(n), _ptr(lab), _ptr(out))
+    return out
+
+
+def resample_grid(src: np.ndarray, n_new: int, margin: int = 3) -> np.ndarray:
+    """GridFunctions::resample, resample_kernel (GridFunctions_GPU.h:547-600):
+    bilinear onto an n_new lattice with the safety margin mapped onto itself.
+    Reads past the old lattice (only in the margin when shrinking) are
+    clamped to the edge."""
+    n_old = src.shape[-1]
+    scale = (n_old - 1 - 2 * margin) / (n_new - 1 - 2 * margin)
+    idx = np.arange(n_new)
+    o = scale * (idx - margin).astype(np.float64) + margin
+    f = np.trunc(o).astype(np.int64)
+    fr = o - f
+    nx = (idx < n_new - 1).astype(np.int64)
+    c = lambda i: np.clip(i, 0, n_old - 1)
+    y0, y1 = c(f)[:, None], c(f + nx)[:, None]
+    x0, x1 = c(f)[None, :], c(f + nx)[None, :]
+    fx, fy = fr[None, :], fr[:, None]
+    p = np.asarray(src, np.float64)
+    a = (1.0 - fx) * p[..., y0, x0] + fx * p[..., y0, x1]
+    b = (1.0 - fx) * p[..., y1, x0] + fx * p[..., y1, x1]
+    return (1.0 - fy) * a + fy * b
+
+
 def riccati_step(delta: complex, energy: complex, g0: complex, h: float) -> complex:
     L = lib()
     d = np.array([delta.real, delta.imag]); e = np.array([energy.real, energy.imag])

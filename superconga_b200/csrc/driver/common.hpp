@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../json.hpp"
+#include "scb200.h"
 
 namespace fs = std::filesystem;
 
@@ -154,6 +155,71 @@ inline bool read_text(const fs::path &p, std::string &out) {
   buf << in.rdbuf();
   out = buf.str();
   return true;
+}
+
+// Order parameter [Nc][2][n0][n0] and vector potential [2][n0][n0] (internal
+// units, times lambda^2) of a saved run (src/simulation.cu:300-377,
+// src/postprocess.cu:286-364).  Files written on another lattice are read as
+// the reference's CSV reader does (csv.h:180-205, 297-395): the order
+// parameter is extended past its grain with the saved domain.csv, then both
+// fields are resampled onto n0.  Returns an error message, empty on success.
+inline std::string load_state(const fs::path &load, const std::vector<std::string> &comps, int n0, double lambda,
+                              std::vector<double> &delta, std::vector<double> &avec) {
+  std::map<std::string, std::vector<double>> op, vp;
+  if (!read_csv(load / "order_parameter.csv", op)) return "Could not find order parameter in " + load.string();
+  if (!read_csv(load / "vector_potential.csv", vp)) return "Could not find vector potential in " + load.string();
+  const size_t nn = (size_t)n0 * n0, nc = comps.size();
+  delta.assign(nc * 2 * nn, 0.0);
+  avec.assign(2 * nn, 0.0);
+  std::vector<signed char> dom;
+  int n_dom = 0;
+  auto side = [](size_t count) {
+    const int n = (int)std::lround(std::sqrt((double)count));
+    return (size_t)n * n == count ? n : -1;
+  };
+  for (size_t c = 0; c < nc; ++c) {
+    const auto &re = op[comps[c] + "_re"], &im = op[comps[c] + "_im"];
+    if (re.empty() || re.size() != im.size())
+      return "The file does not contain the columns, '" + comps[c] + "_re' and '" + comps[c] + "_im'.";
+    double *dst = &delta[c * 2 * nn];
+    if (re.size() == nn) {
+      std::copy(re.begin(), re.end(), dst);
+      std::copy(im.begin(), im.end(), dst + nn);
+      continue;
+    }
+    const int n = side(re.size());
+    if (n < 0) return "The data is not square.";
+    if (dom.empty()) {
+      std::map<std::string, std::vector<double>> dm;
+      if (!read_csv(load / "domain.csv", dm) || side(dm["domain"].size()) != n)
+        return "Could not read the domain of the saved lattice in " + load.string();
+      n_dom = n;
+      for (double v : dm["domain"]) dom.push_back((signed char)v);
+    }
+    if (n != n_dom) return "order-parameter and domain lattices differ";
+    std::vector<double> planes(2 * (size_t)n * n);
+    std::copy(re.begin(), re.end(), planes.begin());
+    std::copy(im.begin(), im.end(), planes.begin() + (size_t)n * n);
+    if (sc_grid_extend(n, dom.data(), 2, planes.data()) != SC_OK ||
+        sc_grid_resample(n, n0, 2, planes.data(), dst) != SC_OK)
+      return "could not resample the order parameter";
+  }
+  const auto &ax = vp["a_x"], &ay = vp["a_y"];
+  if (ax.empty() || ax.size() != ay.size()) return "The file does not contain the columns, 'a_x' and 'a_y'.";
+  if (ax.size() == nn) {
+    std::copy(ax.begin(), ax.end(), avec.begin());
+    std::copy(ay.begin(), ay.end(), avec.begin() + nn);
+  } else {
+    const int n = side(ax.size());
+    if (n < 0) return "The data is not square.";
+    std::vector<double> planes(2 * (size_t)n * n);
+    std::copy(ax.begin(), ax.end(), planes.begin());
+    std::copy(ay.begin(), ay.end(), planes.begin() + (size_t)n * n);
+    if (sc_grid_resample(n, n0, 2, planes.data(), avec.data()) != SC_OK) return "could not resample the vector potential";
+  }
+  const double s = lambda > 0.0 ? lambda * lambda : 0.0;
+  for (double &v : avec) v *= s;
+  return std::string();
 }
 
 }  // namespace drv

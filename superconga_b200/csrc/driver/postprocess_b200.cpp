@@ -51,22 +51,11 @@ int main(int argc, char *argv[]) {
     if (sim["physics"]["order_parameter"].has(s)) comps.push_back(s);
 
   // Order parameter and vector potential of the loaded run (postprocess.cu:286-364).
-  std::vector<double> delta((size_t)nc * 2 * nn, 0.0), avec(2 * nn, 0.0);
-  std::map<std::string, std::vector<double>> op, vp;
-  if (!read_csv(load / "order_parameter.csv", op)) return fail("Could not find order parameter in " + load.string());
-  if (!read_csv(load / "vector_potential.csv", vp)) return fail("Could not find vector potential in " + load.string());
-  for (int c = 0; c < nc; ++c) {
-    const auto &re = op[comps[c] + "_re"], &im = op[comps[c] + "_im"];
-    if (re.size() != nn || im.size() != nn) return fail("order parameter lattice differs from the configuration");
-    std::copy(re.begin(), re.end(), delta.begin() + (size_t)(2 * c) * nn);
-    std::copy(im.begin(), im.end(), delta.begin() + (size_t)(2 * c + 1) * nn);
-  }
-  if (vp["a_x"].size() != nn || vp["a_y"].size() != nn) return fail("vector potential lattice differs");
+  std::vector<double> delta, avec;
   const double lambda = sim["physics"]["penetration_depth"].as_double(-1.0);
-  const double s = lambda > 0.0 ? lambda * lambda : 0.0;  // internal units (postprocess.cu:352-360)
-  for (size_t i = 0; i < nn; ++i) {
-    avec[i] = vp["a_x"][i] * s;
-    avec[nn + i] = vp["a_y"][i] * s;
+  {
+    const std::string e = load_state(load, comps, n0, lambda, delta, avec);
+    if (!e.empty()) return fail(e);
   }
   if (sc_set_state(ctx, delta.data(), avec.data()) != SC_OK) return fail(sc_last_error(ctx));
 

@@ -55,24 +55,8 @@ int main(int argc, char *argv[]) {
   std::vector<double> delta((size_t)nc * 2 * nn, 0.0), avec(2 * nn, 0.0);
   const std::string load = cfg["misc"]["load_path"].as_string();
   if (!load.empty()) {
-    // src/simulation.cu:300-377 (same lattice only).
-    std::map<std::string, std::vector<double>> op, vp;
-    if (!read_csv(fs::path(load) / "order_parameter.csv", op))
-      return fail("Could not find order parameter in " + load);
-    if (!read_csv(fs::path(load) / "vector_potential.csv", vp))
-      return fail("Could not find vector potential in " + load);
-    for (int c = 0; c < nc; ++c) {
-      const auto &re = op[comps[c] + "_re"], &im = op[comps[c] + "_im"];
-      if (re.size() != nn || im.size() != nn) return fail("order parameter lattice differs from the configuration");
-      std::copy(re.begin(), re.end(), delta.begin() + (size_t)(2 * c) * nn);
-      std::copy(im.begin(), im.end(), delta.begin() + (size_t)(2 * c + 1) * nn);
-    }
-    if (vp["a_x"].size() != nn || vp["a_y"].size() != nn) return fail("vector potential lattice differs");
-    const double s = lambda > 0.0 ? lambda * lambda : 0.0;
-    for (size_t i = 0; i < nn; ++i) {
-      avec[i] = vp["a_x"][i] * s;
-      avec[nn + i] = vp["a_y"][i] * s;
-    }
+    const std::string e = load_state(load, comps, n0, lambda, delta, avec);
+    if (!e.empty()) return fail(e);
   } else {
     // Initial::perturbedPhaseWindings / Initial::random
     // (OrderParameterInitial.h:186-237, 420-427), with a fixed seed in place of

@@ -1280,4 +1280,65 @@ int sc_setup_site_updates(const sc_setup *s, long long *per_iteration) {
   return SC_OK;
 }
 
+int sc_grid_extend(int n, const signed char *domain, int n_fields, double *values) {
+  if (n < 1 || !domain || n_fields < 1 || !values) return SC_ERR_ARG;
+  // extendValuesAtBoundary_kernel (domain_ops.h:11-69): a site outside the
+  // grain with grain sites in its 5x5 window takes the mean of the nearest
+  // of them (squared distance, ties averaged); all reads from the input.
+  const size_t nn = (size_t)n * n;
+  std::vector<double> src(values, values + nn * n_fields);
+  for (int y = 0; y < n; ++y)
+    for (int x = 0; x < n; ++x) {
+      if (domain[(size_t)y * n + x] > 0) continue;
+      int best = 1000, cnt = 0;
+      std::vector<size_t> near;
+      for (int ky = std::max(y - 2, 0); ky <= std::min(y + 2, n - 1); ++ky)
+        for (int kx = std::max(x - 2, 0); kx <= std::min(x + 2, n - 1); ++kx) {
+          if (domain[(size_t)ky * n + kx] <= 0) continue;
+          const int d2 = (x - kx) * (x - kx) + (y - ky) * (y - ky);
+          if (d2 < best) {
+            best = d2;
+            near.clear();
+            cnt = 0;
+          }
+          if (d2 == best) {
+            near.push_back((size_t)ky * n + kx);
+            ++cnt;
+          }
+        }
+      if (!cnt) continue;
+      for (int f = 0; f < n_fields; ++f) {
+        double v = 0.0;
+        for (size_t k : near) v += src[f * nn + k];
+        values[f * nn + (size_t)y * n + x] = v / (double)cnt;
+      }
+    }
+  return SC_OK;
+}
+
+int sc_grid_resample(int n_old, int n_new, int n_fields, const double *src, double *dst) {
+  const int margin = 3;  // constants::GRAIN_SIZE_MARGIN (defines.h:25)
+  if (n_old <= 2 * margin + 1 || n_new <= 2 * margin + 1 || n_fields < 1 || !src || !dst) return SC_ERR_ARG;
+  // resample_kernel (GridFunctions_GPU.h:547-600): bilinear interpolation
+  // with the safety margin mapped onto itself.  Sites whose interpolation
+  // would reach past the old lattice (only in the margin when shrinking) read
+  // the nearest edge value instead.
+  const double sx = (double)(n_old - 1 - 2 * margin) / (double)(n_new - 1 - 2 * margin);
+  auto clampi = [&](int i) { return std::min(std::max(i, 0), n_old - 1); };
+  for (int z = 0; z < n_fields; ++z)
+    for (int y = 0; y < n_new; ++y)
+      for (int x = 0; x < n_new; ++x) {
+        const double xo = sx * (double)(x - margin) + margin, yo = sx * (double)(y - margin) + margin;
+        const int xf = (int)xo, yf = (int)yo;
+        const double fx = xo - (double)xf, fy = yo - (double)yf;
+        const int xn = x < n_new - 1 ? 1 : 0, yn = y < n_new - 1 ? 1 : 0;
+        const double *p = src + (size_t)z * n_old * n_old;
+        auto at = [&](int yy, int xx) { return p[(size_t)clampi(yy) * n_old + clampi(xx)]; };
+        const double x1 = (1.0 - fx) * at(yf, xf) + fx * at(yf, xf + xn);
+        const double x2 = (1.0 - fx) * at(yf + yn, xf) + fx * at(yf + yn, xf + xn);
+        dst[((size_t)z * n_new + y) * n_new + x] = (1.0 - fy) * x1 + fy * x2;
+      }
+  return SC_OK;
+}
+
 }  // extern "C"

@@ -60,6 +60,38 @@ def test_driver_golden_disc(engine_lib, tmp_path):
     assert abs(res2["free_energy_per_unit_area"] - fe) <= 1e-4 * abs(fe)
 
 
+def test_driver_load_other_lattice(engine_lib, tmp_path):
+    """A run saved at 3 points/xi0 continued at 4 points/xi0: the order
+    parameter is extended past the grain and resampled onto the finer lattice
+    (csv.h:297-395); the continued run reaches the free energy of a run started
+    afresh on the fine lattice, in fewer iterations."""
+    cfg = configs.golden_disc("congacc")
+    cfg["physics"]["order_parameter"]["s"].update({"initial_noise_stddev": 0.0,
+                                                  "initial_phase_shift": 0.0, "vortices": []})
+    cfg["numerics"].update({"num_iterations_burnin": 0, "num_iterations_min": 0,
+                            "num_iterations_max": 100})
+    coarse = tmp_path / "coarse"
+    cfg["misc"] = {"save_path": str(coarse), "save_frequency": -1, "load_path": "",
+                   "verbose": False, "data_format": "csv"}
+    assert _run(cfg, tmp_path).returncode == 0
+    fine_cfg = json.loads(json.dumps(cfg))
+    fine_cfg["numerics"]["points_per_coherence_length"] = 4.0
+    fine_cfg["misc"]["load_path"] = str(coarse)
+    fine_cfg["misc"]["save_path"] = str(tmp_path / "fine")
+    r = _run(fine_cfg, tmp_path)
+    assert r.returncode == 0, r.stderr
+    # the same fine configuration from the default start
+    fresh_cfg = json.loads(json.dumps(fine_cfg))
+    fresh_cfg["misc"]["load_path"] = ""
+    fresh_cfg["misc"]["save_path"] = str(tmp_path / "fresh")
+    assert _run(fresh_cfg, tmp_path).returncode == 0
+    fe = [json.loads((tmp_path / d / "simulation_results.json").read_text())["free_energy_per_unit_area"]
+          for d in ("fine", "fresh")]
+    assert abs(fe[0] - fe[1]) <= 1e-4 * abs(fe[1])
+    its = [len(list(csv.reader(open(tmp_path / d / "simulation_convergence.csv")))) - 1 for d in ("fine", "fresh")]
+    assert its[0] < its[1]  # the resampled state starts closer to the solution
+
+
 def test_driver_bad_config(engine_lib, tmp_path):
     cfg = configs.golden_disc()
     cfg["numerics"]["norm"] = "l7"
