@@ -2054,7 +2054,7 @@ void upload_static(sc_ctx *c) {
     c->w_gi = c->gi.p;
   }
   c->nb_fin = std::min<int>(592, (int)grid1(nn, REDUCE_THREADS));
-  c->nb_bnd = 296;
+  c->nb_bnd = std::min<int>(296, (int)grid1((size_t)std::max(S.n_in_g, S.n_in_gt) * S.ne, REDUCE_THREADS));
   c->nb_vp = std::min<int>(296, (int)grid1(2 * nn, REDUCE_THREADS));
   c->nb_acc = std::min<int>(148, (int)grid1(nn, REDUCE_THREADS));
   c->partial_fin.alloc((size_t)c->nb_fin * NQ);
