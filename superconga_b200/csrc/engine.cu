@@ -925,24 +925,25 @@ __device__ double residual_from(const double *t, size_t n_elem, int norm) {
   return numer / fmax(denom, eps);
 }
 
-__device__ void reduce_partials(const double *partial, int nblocks, int nq, int k, bool is_max,
-                                double *out) {
-  __shared__ double sh[256];
-  double v = is_max ? 0.0 : 0.0;
-  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
-    const double p = partial[(size_t)b * nq + k];
-    v = is_max ? fmax(v, p) : v + p;
-  }
-  sh[threadIdx.x] = v;
-  __syncthreads();
-  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-    if ((int)threadIdx.x < s) {
-      const double o = sh[threadIdx.x + s];
-      sh[threadIdx.x] = is_max ? fmax(sh[threadIdx.x], o) : sh[threadIdx.x] + o;
+// Sums (or maxima, for the slots set in max_mask) of nq slots over the
+// nblocks rows of block partials: warp w reduces slots w, w + nwarps, ... in a
+// fixed order (lane-strided, then a shuffle tree); results in t[0..nq).
+__device__ void reduce_slots(const double *partial, int nblocks, int nq, unsigned long long max_mask,
+                             double *t) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int k = w; k < nq; k += nw) {
+    const bool mx = (max_mask >> k) & 1ull;
+    double v = 0.0;
+    for (int b = lane; b < nblocks; b += 32) {
+      const double p = partial[(size_t)b * nq + k];
+      v = mx ? fmax(v, p) : v + p;
     }
-    __syncthreads();
+    for (int o = 16; o > 0; o >>= 1) {
+      const double u = __shfl_xor_sync(0xffffffffu, v, o);
+      v = mx ? fmax(v, u) : v + u;
+    }
+    if (lane == 0) t[k] = v;
   }
-  if (threadIdx.x == 0) *out = sh[0];
   __syncthreads();
 }
 
@@ -958,8 +959,7 @@ struct FinalizeConsts {
 // ComputeCurrent.h:184-211).
 __global__ void k_scalars_a(FinalizeConsts C, const double *partial, int nblocks, Scalars *S) {
   __shared__ double t[NQ];
-  for (int k = 0; k < NQ; ++k)
-    reduce_partials(partial, nblocks, NQ, k, (FIN_MAX_MASK >> k) & 1ull, &t[k]);
+  reduce_slots(partial, nblocks, NQ, FIN_MAX_MASK, t);
   if (threadIdx.x != 0) return;
   double rop = 0.0;
   for (int c = 0; c < C.nc; ++c) rop = fmax(rop, residual_from(&t[6 * c], C.n_elem_field, C.norm));
@@ -994,14 +994,11 @@ __global__ void k_scalars_b(int norm, size_t n_elem_g, size_t n_elem_gt, size_t 
                             int do_bc, int do_vp, int compute_mode, const double *p_bg, int nb_g,
                             const double *p_bgt, int nb_gt, const double *p_vp, int nb_vp, Scalars *S) {
   __shared__ double t[18];
-  for (int k = 0; k < 6; ++k) {
-    const bool mx = k >= 4;
-    if (do_bc) {
-      reduce_partials(p_bg, nb_g, 6, k, mx, &t[k]);
-      reduce_partials(p_bgt, nb_gt, 6, k, mx, &t[6 + k]);
-    }
-    if (do_vp) reduce_partials(p_vp, nb_vp, 6, k, mx, &t[12 + k]);
+  if (do_bc) {
+    reduce_slots(p_bg, nb_g, 6, 0x30ull, &t[0]);
+    reduce_slots(p_bgt, nb_gt, 6, 0x30ull, &t[6]);
   }
+  if (do_vp) reduce_slots(p_vp, nb_vp, 6, 0x30ull, &t[12]);
   if (threadIdx.x != 0) return;
   if (do_bc) S->res_bc = fmax(residual_from(&t[0], n_elem_g, norm), residual_from(&t[6], n_elem_gt, norm));
   if (do_vp) S->res_vp = residual_from(&t[12], n_elem_vp, norm);
@@ -1080,9 +1077,7 @@ struct AccConsts {
 __global__ void k_acc_scalars(AccConsts C, const double *partial, int nblocks, AccState *st) {
   __shared__ double t[48];
   const int nf = C.nf;
-  for (int f = 0; f < nf; ++f)
-    for (int k = 0; k < 3; ++k)
-      reduce_partials(partial + (size_t)f * nblocks * 3, nblocks, 3, k, false, &t[3 * f + k]);
+  for (int f = 0; f < nf; ++f) reduce_slots(partial + (size_t)f * nblocks * 3, nblocks, 3, 0ull, &t[3 * f]);
   if (threadIdx.x != 0) return;
   if (!st->initialized) {
     for (int f = 0; f < nf; ++f) {
