@@ -187,6 +187,17 @@ WORKLOAD_DESC = {
 }
 
 
+def max_over_ranks(value: float, world: int, device: str = "cuda") -> float:
+    """The largest value over all ranks (the replicas' timing rule); the
+    identity for one process."""
+    if world <= 1:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
 def _time_context(ctx, stream, steps, warmup, world):
     """Device-timed self-consistency iterations of one context (inputs resident)."""
     import torch
@@ -207,10 +218,7 @@ def _time_context(ctx, stream, steps, warmup, world):
     launches = ctx.launch_count() - launches0
     prof = {k: ctx.profile_read(i) for i, k in enumerate(("sweep", "rotate_back", "poisson", "boundary"))}
     ctx.profile(False)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, world)
     return ms, launches, prof
 
 
@@ -236,10 +244,7 @@ def _e2e(ctx, steps, world):
         host_a[...] = xa
     torch.cuda.synchronize()
     sec = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([sec], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        sec = float(t.item())
+    sec = max_over_ranks(sec, world)
     return sec, (nc * 2 * n0 * n0 + 2 * n0 * n0) * 8
 
 
