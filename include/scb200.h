@@ -266,6 +266,14 @@ int sc_setup_boundary_sizes(const sc_setup *s, int *sizes);
 int sc_setup_filters(const sc_setup *s, int *n_filters, double *filters, int *positive,
                      double *scale);
 int sc_setup_site_updates(const sc_setup *s, long long *per_iteration);
+/* Fermi-surface tables of the configuration (FermiSurfaceCircle.h:84-164, or
+ * FermiSurfaceTightBinding.h:384-470 with physics.fermi_surface.type =
+ * "tight_binding"): table [8][n_angles] = polar angle phi, system angle,
+ * Fermi momentum x, y, Fermi velocity x, y (divided by the mean speed),
+ * integrand factor, Riccati step h/|v_F|; info [4] = mean |p_F|, mean |v_F|
+ * (the tight-binding averages before normalisation, FermiSurfaceTightBinding
+ * .h:79-80; 1 on the circle), momentum origin x, y.  Either may be NULL. */
+int sc_setup_fermi_surface(const sc_setup *s, double *table, double *info);
 
 /* Load-path helpers for runs saved on another lattice (host only).
  * sc_grid_extend: extendValuesAtBoundary (domain_ops.h:11-69) of n_fields

@@ -188,6 +188,11 @@ struct orc_params {
   int acc_rank;
   int n_filters;
   double vp_scale;
+  /* Fermi surface: 0 circle (FermiSurfaceCircle.h), 1 square-lattice tight
+   * binding (FermiSurfaceTightBinding.h) with next- and next-next-nearest
+   * hopping and chemical potential (nearest hopping 1). */
+  int fs_type;
+  double tb_nnn, tb_nnnn, tb_mu;
 };
 
 }  // extern "C"
@@ -220,6 +225,10 @@ struct Oracle {
 
   // Fermi surface tables.
   std::vector<double> polar, system_angle;
+  // Tight-binding surface (p.fs_type == 1): per angle momentum, velocity
+  // (normalised), integrand factor and speed; momentum origin.
+  std::vector<double> tb_px, tb_py, tb_vx, tb_vy, tb_w, tb_speed;
+  double tb_ox = 0.0, tb_oy = 0.0;
 
   // Per-angle geometry, precomputed (the reference rebuilds it each time, with
   // identical results).
@@ -293,14 +302,49 @@ struct Oracle {
     return 1.0;
   }
   // FermiSurfaceCircle::getIntegrandFactor, FermiSurfaceCircle.h:159-164
-  double integrand(int k) const { return angle_weight(k) / (double)p.n_angles; }
+  // FermiSurfaceTightBinding::getIntegrandFactor, FermiSurfaceTightBinding.h:504-508
+  double integrand(int k) const {
+    if (p.fs_type == 1) return tb_w[wrap_int(k, 0, p.n_angles)];
+    return angle_weight(k) / (double)p.n_angles;
+  }
   void fermi_momentum(int k, double &px, double &py) const {
+    if (p.fs_type == 1) {
+      const int i = wrap_int(k, 0, p.n_angles);
+      px = tb_px[i];
+      py = tb_py[i];
+      return;
+    }
     const double phi = polar_angle(k);
     px = std::cos(phi);
     py = std::sin(phi);
   }
-  // BasisFunction::evaluate (circular), OrderParameterBasis.h:145-186
+  // getFermiVelocity: the momentum on the circle (FermiSurfaceCircle.h:125-138)
+  void fermi_velocity(int k, double &vx, double &vy) const {
+    if (p.fs_type == 1) {
+      const int i = wrap_int(k, 0, p.n_angles);
+      vx = tb_vx[i];
+      vy = tb_vy[i];
+      return;
+    }
+    fermi_momentum(k, vx, vy);
+  }
+  // Riccati step h / |v_F|, RiccatiSolverConfined.h:525-527
+  double step_size(int k) const {
+    if (p.fs_type == 1) return p.h / tb_speed[wrap_int(k, 0, p.n_angles)];
+    return p.h / 1.0;  // |v_F| = 1 on a circular Fermi surface
+  }
+  // BasisFunction::evaluate, OrderParameterBasis.h:145-219: polynomials of
+  // the momentum on the circle, lattice harmonics otherwise.
   double basis_raw(int s, double px, double py) const {
+    if (p.fs_type == 1) {
+      switch (s) {
+      case 0: return std::cos(px) + std::cos(py);
+      case 1: return std::cos(px) - std::cos(py);
+      case 2: return std::sin(px) * std::sin(py);
+      case 3: return std::sin(px) * std::sin(py) * (std::cos(px) - std::cos(py));
+      }
+      return 0.0;
+    }
     switch (s) {
     case 0: return 1.0;
     case 1: return px * px - py * py;
@@ -764,7 +808,7 @@ struct Oracle {
     const double b = M_PI * p.flux_quanta / area;
     const double theta = sys_angle(a);
     double vx, vy;
-    fermi_momentum(a, vx, vy);
+    fermi_velocity(a, vx, vy);
     es.assign((size_t)n1 * n1, 0.0);
     const double q = (double)p.charge_sign;
     const double off = -0.5 * (double)(n1 - 1);
@@ -806,7 +850,7 @@ struct Oracle {
   void sweep(int a, const std::vector<double> &dre, const std::vector<double> &dim,
              const std::vector<double> &es, bool store) {
     const int n = N1(), ne = p.n_energies;
-    const double step = p.h / 1.0;  // |v_F| = 1 on a circular Fermi surface
+    const double step = step_size(a);
     const AngleGeom &G = ag[a];
     const int x0 = xr0[a], x1 = xr1[a], y0 = yr0[a], y1 = yr1[a];
     for (int dir = 0; dir < 2; ++dir) {
@@ -904,9 +948,9 @@ struct Oracle {
     double mx, my;
     rotate(sysang, rpx, rpy, mx, my);
     // FermiSurface::getFractionalAngleIndex, FermiSurface.h:151-172
-    const double kx = wrap_range(mx, 0.0 - M_PI, 0.0 + M_PI);
-    const double ky = wrap_range(my, 0.0 - M_PI, 0.0 + M_PI);
-    const double phu = std::atan2(ky - 0.0, kx - 0.0) - 0.5 * M_PI;
+    const double kx = wrap_range(mx, tb_ox - M_PI, tb_ox + M_PI);
+    const double ky = wrap_range(my, tb_oy - M_PI, tb_oy + M_PI);
+    const double phu = std::atan2(ky - tb_oy, kx - tb_ox) - 0.5 * M_PI;
     const double ph = wrap_range(phu, 0.0, 2.0 * M_PI);
     const double fai = (double)na * ph / (2.0 * M_PI);
     const int ia0 = wrap_int((int)fai, 0, na), ia1 = wrap_int((int)fai + 1, 0, na);
@@ -1117,10 +1161,13 @@ struct Oracle {
           acc_d[(size_t)c * nn0 + i] = add(acc_d[(size_t)c * nn0 + i], v);
         }
       }
-      // Current (real part only reaches the result).
+      // Current (real part only reaches the result), weighted by the Fermi
+      // velocity (ComputeCurrent.h:155-160).
       extend(G.label, n1, gre.data());
+      double vx, vy;
+      fermi_velocity(a, vx, vy);
       for (int d = 0; d < 2; ++d) {
-        const double f = (d == 0 ? px : py) * w;
+        const double f = (d == 0 ? vx : vy) * w;
         for (size_t i = 0; i < tmp1.size(); ++i) tmp1[i] = gre[i] * f;
         rotate_insert(cur_re.data() + d * nn0, n0, tmp1.data(), n1, sa, true);
       }
@@ -1565,9 +1612,112 @@ struct Oracle {
   }
 };
 
+// ------------------------------------------------ tight-binding surface ----
+// DispersionTightBinding<T>::evaluate / derivative,
+// include/conga/fermi_surface/DispersionTightBinding.h:62-125.
+double tb_dispersion(double t1, double t2, double mu, double kx, double ky) {
+  const double term_nn = (-2.0 * 1.0) * (std::cos(kx) + std::cos(ky));
+  const double term_nnn = (-4.0 * t1) * std::cos(kx) * std::cos(ky);
+  const double term_nnnn = (-2.0 * t2) * (std::cos(2.0 * kx) + std::cos(2.0 * ky));
+  return term_nn + term_nnn + term_nnnn - mu;
+}
+void tb_velocity(double t1, double t2, double kx, double ky, double &vx, double &vy) {
+  vx = (2.0 * 1.0) * std::sin(kx) + (4.0 * t1) * std::sin(kx) * std::cos(ky) + (4.0 * t2) * std::sin(2.0 * kx);
+  vy = (2.0 * 1.0) * std::sin(ky) + (4.0 * t1) * std::cos(kx) * std::sin(ky) + (4.0 * t2) * std::sin(2.0 * ky);
+}
+
+// FermiSurfaceTightBinding<T>::initialize, FermiSurfaceTightBinding.h:384-470,
+// with tightbinding_internal::computeMomentumOffset (:129-151),
+// computeFermiMomentum (:167-290) and computeIntegrandFactor (:305-326).
+// table [8][n]: polar angle, system angle, momentum x, y, velocity x, y
+// (divided by the mean speed), integrand factor (normalised to sum 1), speed;
+// info: mean |p|, mean |v|, origin x, y.
+void tight_binding_tables(double t1, double t2, double mu, int n, double *table, double *info) {
+  // Origin: (0,0) if the band has the same sign at (0,pi) and (pi,pi).
+  const double e0pi = tb_dispersion(t1, t2, mu, 0.0, M_PI);
+  const double epipi = tb_dispersion(t1, t2, mu, M_PI, M_PI);
+  const double org = (sign_(e0pi) == sign_(epipi)) ? 0.0 : M_PI;
+  const double crit = 1e2 * std::numeric_limits<double>::epsilon();
+  double *phi = table, *sys = table + n, *px = table + 2 * n, *py = table + 3 * n;
+  double *vx = table + 4 * n, *vy = table + 5 * n, *w = table + 6 * n, *sp = table + 7 * n;
+  double fsum = 0.0, msum = 0.0, ssum = 0.0;
+  for (int k = 0; k < n; ++k) {
+    const double ph = wrap_range(M_PI * (double)(2 * k) / (double)n + 0.5 * M_PI, 0.0, 2.0 * M_PI);
+    const double c = std::cos(ph), s = std::sin(ph);
+    // Root of the band along the ray org + kappa (c, s).
+    double lo = 0.0, e_lo = tb_dispersion(t1, t2, mu, lo * c + org, lo * s + org);
+    double hi = M_PI / std::max(std::fabs(c), std::fabs(s));
+    double e_hi = tb_dispersion(t1, t2, mu, hi * c + org, hi * s + org);
+    double kappa = 0.5 * (lo + hi);
+    bool newton = false;
+    for (int it = 0; it < 100; ++it) {
+      const double mx = kappa * c + org, my = kappa * s + org;
+      const double e = tb_dispersion(t1, t2, mu, mx, my);
+      if (!newton && std::fabs(e) > std::sqrt(crit)) {
+        if (sign_(e) == sign_(e_lo)) {
+          e_lo = e;
+          lo = kappa;
+        } else {
+          e_hi = e;
+          hi = kappa;
+        }
+        if (sign_(e_lo) == sign_(e_hi)) break;
+        kappa = 0.5 * (lo + hi);
+        continue;
+      }
+      if (!(std::fabs(e) > crit)) break;
+      newton = true;
+      double gx, gy;
+      tb_velocity(t1, t2, mx, my, gx, gy);
+      const double d = gx * c + gy * s;
+      if (!(std::fabs(d) > 0.0)) break;
+      kappa -= e / d;
+    }
+    const double pkx = wrap_range(kappa * c + org, -M_PI, M_PI);
+    const double pky = wrap_range(kappa * s + org, -M_PI, M_PI);
+    double gx, gy;
+    tb_velocity(t1, t2, pkx, pky, gx, gy);
+    // Buchholtz et al.'s Jacobian |k.k / k.v| with k the momentum from the origin.
+    const double kx = wrap_range(pkx, org - M_PI, org + M_PI) - org;
+    const double ky = wrap_range(pky, org - M_PI, org + M_PI) - org;
+    const double f = std::fabs((kx * kx + ky * ky) / (kx * gx + ky * gy)) * [&] {
+      if (n % 4 == 0) return (k % 4 == 0) ? 28.0 / 45.0 : (k % 2 == 0) ? 24.0 / 45.0 : 64.0 / 45.0;
+      if (n % 3 == 0) return (k % 3 == 0) ? 6.0 / 8.0 : 9.0 / 8.0;
+      if (n % 2 == 0) return (k % 2 == 0) ? 2.0 / 3.0 : 4.0 / 3.0;
+      return 1.0;
+    }();
+    phi[k] = ph;
+    sys[k] = std::atan2(gy, gx) - 0.5 * M_PI;
+    px[k] = pkx;
+    py[k] = pky;
+    vx[k] = gx;
+    vy[k] = gy;
+    w[k] = f;
+    fsum += f;
+    msum += std::hypot(pkx, pky) * f;
+    ssum += std::hypot(gx, gy) * f;
+  }
+  const double avg_p = msum / fsum, avg_v = ssum / fsum;
+  for (int k = 0; k < n; ++k) {
+    vx[k] /= avg_v;
+    vy[k] /= avg_v;
+    w[k] /= fsum;
+    sp[k] = std::hypot(vx[k], vy[k]);
+  }
+  info[0] = avg_p;
+  info[1] = avg_v;
+  info[2] = org;
+  info[3] = org;
+}
+
 }  // namespace
 
 extern "C" {
+
+/* The tight-binding Fermi-surface tables alone (see tight_binding_tables). */
+void orc_tight_binding(double t1, double t2, double mu, int n, double *table, double *info) {
+  tight_binding_tables(t1, t2, mu, n, table, info);
+}
 
 void *orc_create(const orc_params *p, const double *energies_im, const double *residues,
                  const int *comp_symmetry, const double *comp_tc, int n_geom,
@@ -1598,11 +1748,29 @@ void *orc_create(const orc_params *p, const double *energies_im, const double *r
     }
     o->geom.push_back(c);
   }
-  // Fermi surface, FermiSurfaceCircle::initialize (FermiSurfaceCircle.h:84-104).
-  for (int k = 0; k < p->n_angles; ++k) {
-    const double phi = o->polar_angle(k);
-    o->polar.push_back(phi);
-    o->system_angle.push_back(phi - 0.5 * M_PI);
+  // Fermi surface, FermiSurfaceCircle::initialize (FermiSurfaceCircle.h:84-104)
+  // or FermiSurfaceTightBinding::initialize (FermiSurfaceTightBinding.h:384-470).
+  if (p->fs_type == 1) {
+    const int na = p->n_angles;
+    std::vector<double> t((size_t)8 * na);
+    double info[4];
+    tight_binding_tables(p->tb_nnn, p->tb_nnnn, p->tb_mu, na, t.data(), info);
+    o->polar.assign(t.begin(), t.begin() + na);
+    o->system_angle.assign(t.begin() + na, t.begin() + 2 * na);
+    o->tb_px.assign(t.begin() + 2 * na, t.begin() + 3 * na);
+    o->tb_py.assign(t.begin() + 3 * na, t.begin() + 4 * na);
+    o->tb_vx.assign(t.begin() + 4 * na, t.begin() + 5 * na);
+    o->tb_vy.assign(t.begin() + 5 * na, t.begin() + 6 * na);
+    o->tb_w.assign(t.begin() + 6 * na, t.begin() + 7 * na);
+    o->tb_speed.assign(t.begin() + 7 * na, t.end());
+    o->tb_ox = info[2];
+    o->tb_oy = info[3];
+  } else {
+    for (int k = 0; k < p->n_angles; ++k) {
+      const double phi = o->polar_angle(k);
+      o->polar.push_back(phi);
+      o->system_angle.push_back(phi - 0.5 * M_PI);
+    }
   }
   // BasisFunction::normalize, OrderParameterBasis.h:188-212.
   for (int c = 0; c < p->n_comp; ++c) {

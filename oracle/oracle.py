@@ -93,6 +93,8 @@ class OrcParams(ctypes.Structure):
         ("acc_step_size_min", ctypes.c_double), ("acc_drag", ctypes.c_double),
         ("acc_rank", ctypes.c_int), ("n_filters", ctypes.c_int),
         ("vp_scale", ctypes.c_double),
+        ("fs_type", ctypes.c_int), ("tb_nnn", ctypes.c_double),
+        ("tb_nnnn", ctypes.c_double), ("tb_mu", ctypes.c_double),
     ]
 
 
@@ -436,6 +438,17 @@ def make_setup(cfg: dict) -> Setup:
     p.acc_rank = int(acc.get("rank", 4))
     p.n_filters = len(filters)
     p.vp_scale = vscale
+    # Fermi surface: the circle, or the tight-binding surface that the
+    # reference sets in code (Context::set, Context.h:49-51); JSON spelling
+    # physics.fermi_surface = {"type": "tight_binding", ...}.
+    fs = phys.get("fermi_surface", {"type": "circle"})
+    if fs.get("type", "circle") == "tight_binding":
+        p.fs_type = 1
+        p.tb_nnn = float(fs.get("hopping_nnn", 0.0))
+        p.tb_nnnn = float(fs.get("hopping_nnnn", 0.0))
+        p.tb_mu = float(fs.get("chemical_potential", 1.0))
+    elif fs.get("type", "circle") != "circle":
+        raise ValueError(f"fermi_surface type {fs.get('type')!r} not understood")
     return Setup(cfg=cfg, n0=n0, n1=n1, h=h, grain_fraction=gf, grain_width=scaling,
                  temperature=temperature, n_angles=p.n_angles, poles=poles,
                  residues=residues, energies_im=energies_im, symmetries=syms,
@@ -693,3 +706,21 @@ def greens(g: complex, gt: complex):
     a = np.array([g.real, g.imag]); b = np.array([gt.real, gt.imag]); out = np.zeros(4)
     L.orc_greens(_ptr(a), _ptr(b), _ptr(out))
     return complex(out[0], out[1]), complex(out[2], out[3])
+
+
+def tight_binding(hopping_nnn: float, hopping_nnnn: float, chemical_potential: float,
+                  n_angles: int) -> dict:
+    """FermiSurfaceTightBinding<double>::initialize (FermiSurfaceTightBinding.h:
+    384-470) on its own: per-angle polar angle, system angle, Fermi momentum,
+    normalised Fermi velocity, integrand factor and speed, plus the mean |p_F|
+    and |v_F| before normalisation and the momentum origin."""
+    L = lib()
+    t = np.zeros((8, n_angles))
+    info = np.zeros(4)
+    L.orc_tight_binding(ctypes.c_double(hopping_nnn), ctypes.c_double(hopping_nnnn),
+                        ctypes.c_double(chemical_potential), ctypes.c_int(n_angles), _ptr(t), _ptr(info))
+    keys = ["phi", "theta", "px", "py", "vx", "vy", "weight", "speed"]
+    out = {k: t[i].copy() for i, k in enumerate(keys)}
+    out.update(avg_fermi_momentum=float(info[0]), avg_fermi_speed=float(info[1]),
+               origin=(float(info[2]), float(info[3])))
+    return out

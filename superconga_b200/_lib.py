@@ -82,6 +82,7 @@ SIGNATURES = {
     "sc_setup_dims": (ctypes.c_int, [ctypes.c_void_p] + [_c_int_p] * 5),
     "sc_setup_energies": (ctypes.c_int, [ctypes.c_void_p, _c_double_p, _c_double_p]),
     "sc_setup_frame": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, _c_int_p]),
+    "sc_setup_fermi_surface": (ctypes.c_int, [ctypes.c_void_p, _c_double_p, _c_double_p]),
     "sc_setup_domain": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "sc_setup_boundary_sizes": (ctypes.c_int, [ctypes.c_void_p, _c_int_p]),
     "sc_setup_filters": (ctypes.c_int, [ctypes.c_void_p, _c_int_p, _c_double_p, _c_int_p,

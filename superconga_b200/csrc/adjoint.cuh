@@ -109,7 +109,7 @@ __device__ void adjoint_column(const AdjArgs &J, const double *s_res, int item, 
   const int n1 = A.n1, ne = A.ne, len = hi - lo + 1;
   const size_t nn1 = (size_t)n1 * n1, ni = (size_t)A.n_items;
   const uint8_t *lab = A.labels + (size_t)a * nn1;
-  const double h = A.h;
+  const double h = A.ang[a].hs;
   const int e0 = g * A.ept;
   int ecount = ne - e0;
   if (ecount > A.ept) ecount = A.ept;

@@ -23,6 +23,7 @@ struct AngleParams {
   double cE, sE;  // external vector potential coordinates (double trig)
   double vx, vy;  // Fermi velocity
   double w;       // Fermi-surface integrand factor
+  double hs;      // Riccati step h / |v_F| (RiccatiSolverConfined.h:525-527)
   double sx, sy;  // vx * w, vy * w
   double eta[MAX_COMP];  // basis function of every component at this angle
 };

@@ -284,7 +284,10 @@ __device__ __forceinline__ void site_step(uint8_t l, uint8_t l_entry, uint8_t l_
 // LDOS frame buffer (GreensFunctionStatic.h:66-90, ComputeLDOS.h:123-144).
 // One trajectory column (item) for thread g of its group; s_res holds the
 // residues of the energies.
-template <typename R, int EMAX, bool KEL>
+// STEP_PER_ANGLE: the Riccati step h/|v_F| is read per angle (a non-circular
+// Fermi surface, and the batch); otherwise it is the uniform lattice spacing h
+// of the circle, which stays a kernel parameter.
+template <typename R, int EMAX, bool KEL, bool STEP_PER_ANGLE>
 __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double *s_res, int item,
                                              int g, unsigned gmask) {
   const int4 it = A.items[item];
@@ -293,7 +296,7 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
   const size_t nn1 = (size_t)n1 * n1;
   const uint8_t *lab = A.labels + (size_t)a * nn1;
   const size_t ni = (size_t)A.n_items;
-  const R h = (R)A.h;
+  const R h = STEP_PER_ANGLE ? (R)A.ang[a].hs : (R)A.h;  // h / |v_F| of this angle
   const int e0 = g * A.ept;
   int ecount = ne - e0;
   if (ecount > A.ept) ecount = A.ept;
@@ -467,7 +470,7 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
   }
 }
 
-template <typename R, int EMAX, int MINB, bool KEL>
+template <typename R, int EMAX, int MINB, bool KEL, bool STEP_PER_ANGLE = false>
 __global__ void __launch_bounds__(128, MINB) k_sweep(const SweepArgs<R> A) {
   __shared__ double s_res[64];  // residues (at most 64 energies)
   for (int e = threadIdx.x; e < A.ne && e < 64; e += blockDim.x) s_res[e] = A.res[e];
@@ -479,7 +482,7 @@ __global__ void __launch_bounds__(128, MINB) k_sweep(const SweepArgs<R> A) {
   const unsigned gmask = ((A.groups == 32) ? 0xffffffffu : ((1u << A.groups) - 1u))
                          << (lane & ~(A.groups - 1));
   if (item >= A.n_items) return;  // whole groups leave together (groups divide the warp)
-  sweep_column<R, EMAX, KEL>(A, s_res, item, g, gmask);
+  sweep_column<R, EMAX, KEL, STEP_PER_ANGLE>(A, s_res, item, g, gmask);
 }
 
 // The sweep of many grains in one persistent launch.  A work unit is one
@@ -505,7 +508,7 @@ __global__ void __launch_bounds__(128, MINB) k_sweep_batch(const SweepArgs<R> *_
     const int sub = lane >> lg;
     const unsigned gmask = ((groups == 32) ? 0xffffffffu : ((1u << groups) - 1u)) << (lane & ~(groups - 1));
     const int item = wu.y + sub;
-    if (item < A.n_items) sweep_column<R, EMAX, false>(A, A.res, item, g, gmask);
+    if (item < A.n_items) sweep_column<R, EMAX, false, true>(A, A.res, item, g, gmask);
   }
 }
 
@@ -1425,7 +1428,18 @@ void launch_sweep(sc_ctx *c, const Chunk &ch, int burn_in) {
   // FP64 runs best with four resident blocks per SM (measured on B200).
   static const char *minb_env = std::getenv("SCB_SWEEP_MINB");
   const int variant = minb_env ? std::atoi(minb_env) : (sizeof(R) == 8 ? 4 : (c->emax2 ? 6 : 1));
-  if (c->S.keldysh) {
+  if (c->S.fs_tight_binding) {
+    // Non-circular Fermi surface: per-angle step, generic mappings.
+    if (c->S.keldysh) {
+      if (c->ept <= 4) k_sweep<R, 4, 1, true, true><<<blocks, 128, 0, c->stream>>>(A);
+      else if (c->ept <= 8) k_sweep<R, 8, 1, true, true><<<blocks, 128, 0, c->stream>>>(A);
+      else k_sweep<R, 16, 1, true, true><<<blocks, 128, 0, c->stream>>>(A);
+    } else {
+      if (c->ept <= 4) k_sweep<R, 4, 1, false, true><<<blocks, 128, 0, c->stream>>>(A);
+      else if (c->ept <= 8) k_sweep<R, 8, 1, false, true><<<blocks, 128, 0, c->stream>>>(A);
+      else k_sweep<R, 16, 1, false, true><<<blocks, 128, 0, c->stream>>>(A);
+    }
+  } else if (c->S.keldysh) {
     if (c->ept <= 4) k_sweep<R, 4, 1, true><<<blocks, 128, 0, c->stream>>>(A);
     else if (c->ept <= 8) k_sweep<R, 8, 1, true><<<blocks, 128, 0, c->stream>>>(A);
     else k_sweep<R, 16, 1, true><<<blocks, 128, 0, c->stream>>>(A);
@@ -1889,6 +1903,7 @@ void upload_static(sc_ctx *c) {
     p.vx = S.vx[a];
     p.vy = S.vy[a];
     p.w = S.weight[a];
+    p.hs = S.step[a];
     p.sx = S.vx[a] * S.weight[a];
     p.sy = S.vy[a] * S.weight[a];
     for (int k = 0; k < MAX_COMP; ++k) p.eta[k] = k < S.nc ? S.eta[(size_t)a * S.nc + k] : 0.0;
@@ -1962,12 +1977,13 @@ void upload_static(sc_ctx *c) {
   c->onode_x_gt.upload(xgt, s);
   c->onode_y_gt.upload(ygt, s);
 
-  // Mirror pairing of angle a with a + n/2 (mixed mode only): every frame of
-  // the second half must be the 180-degree mirror of its partner, with entry
-  // and exit labels exchanged.  All four basis symmetries are even, so the
-  // order parameter is the same on both angles.
+  // Mirror pairing of angle a with a + n/2 (mixed mode only, circular Fermi
+  // surface): every frame of the second half must be the 180-degree mirror of
+  // its partner, with entry and exit labels exchanged.  All four basis
+  // symmetries are even, so the order parameter is the same on both angles.
   c->pair = 0;
-  if (c->mode == SC_MODE_MIXED && !S.keldysh && na % 2 == 0 && !std::getenv("SCB_NO_PAIRING")) {
+  if (c->mode == SC_MODE_MIXED && !S.keldysh && !S.fs_tight_binding && na % 2 == 0 &&
+      !std::getenv("SCB_NO_PAIRING")) {
     const int n1p = S.n1;
     const size_t nn1p = (size_t)n1p * n1p;
     bool ok = true;

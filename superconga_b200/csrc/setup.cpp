@@ -59,6 +59,136 @@ void rotate(double ang, double x, double y, double &ox, double &oy) {
   ox = x * c - y * s;
   oy = x * s + y * c;
 }
+double wrap_range(double v, double lo, double hi);
+int wrap_int(int v, int lo, int hi);
+// FermiSurface::getAngleWeight (FermiSurface.h:210-243): Boole, Simpson 3/8,
+// Simpson 1/3 or trapezoid weights by the divisibility of the angle count.
+double angle_weight(int k, int na) {
+  const int w = wrap_int(k, 0, na);
+  if (na % 4 == 0) return (w % 4 == 0) ? 28.0 / 45.0 : (w % 2 == 0) ? 24.0 / 45.0 : 64.0 / 45.0;
+  if (na % 3 == 0) return (w % 3 == 0) ? 6.0 / 8.0 : 9.0 / 8.0;
+  if (na % 2 == 0) return (w % 2 == 0) ? 2.0 / 3.0 : 4.0 / 3.0;
+  return 1.0;
+}
+
+// Square-lattice tight-binding band (DispersionTightBinding.h:62-125): hopping
+// 1 to nearest neighbours, t1 to next-nearest, t2 to next-next-nearest,
+// measured from the chemical potential mu; grad is the band velocity.
+struct TbBand {
+  double t1, t2, mu;
+  double energy(double kx, double ky) const {
+    const double nn = -2.0 * 1.0 * (std::cos(kx) + std::cos(ky));
+    const double nnn = -4.0 * t1 * std::cos(kx) * std::cos(ky);
+    const double nnnn = -2.0 * t2 * (std::cos(2.0 * kx) + std::cos(2.0 * ky));
+    return nn + nnn + nnnn - mu;
+  }
+  void grad(double kx, double ky, double &gx, double &gy) const {
+    const double a = 2.0 * 1.0, b = 4.0 * t1, c = 4.0 * t2;
+    gx = a * std::sin(kx) + b * std::sin(kx) * std::cos(ky) + c * std::sin(2.0 * kx);
+    gy = a * std::sin(ky) + b * std::cos(kx) * std::sin(ky) + c * std::sin(2.0 * ky);
+  }
+};
+
+// The Fermi momentum along the ray offset + k (cos phi, sin phi): bisection
+// between the origin and the zone edge until |e| < sqrt(tol), then Newton
+// steps along the ray until |e| < tol, at most 100 evaluations; the result is
+// wrapped into the first zone (tightbinding_internal::computeFermiMomentum,
+// FermiSurfaceTightBinding.h:167-290).
+void tb_fermi_momentum(const TbBand &band, double phi, double ox, double oy, double &px, double &py) {
+  const double tol = 1e2 * std::numeric_limits<double>::epsilon();
+  const double ux = std::cos(phi), uy = std::sin(phi);
+  double ka = 0.0;
+  double ea = band.energy(ka * ux + ox, ka * uy + oy);
+  const double umax = std::max(std::fabs(ux), std::fabs(uy));
+  double kb = M_PI / umax;
+  double eb = band.energy(kb * ux + ox, kb * uy + oy);
+  double k = 0.5 * (ka + kb);
+  bool bisect = true;
+  for (int it = 0; it < 100; ++it) {
+    const double mx = k * ux + ox, my = k * uy + oy;
+    const double e = band.energy(mx, my);
+    const double err = std::fabs(e);
+    if (err > std::sqrt(tol) && bisect) {
+      if (sgn(e) == sgn(ea)) {
+        ea = e;
+        ka = k;
+      } else {
+        eb = e;
+        kb = k;
+      }
+      if (sgn(ea) == sgn(eb)) break;
+      k = 0.5 * (ka + kb);
+    } else if (err > tol) {
+      bisect = false;
+      double gx, gy;
+      band.grad(mx, my, gx, gy);
+      const double slope = gx * ux + gy * uy;
+      if (std::fabs(slope) > 0.0) k -= e / slope;
+      else break;
+    } else {
+      break;
+    }
+  }
+  px = wrap_range(k * ux + ox, -M_PI, M_PI);
+  py = wrap_range(k * uy + oy, -M_PI, M_PI);
+}
+
+}  // namespace
+
+// FermiSurfaceTightBinding::initialize (FermiSurfaceTightBinding.h:384-470):
+// origin (0,0) or (pi,pi) by the band signs at (0,pi) and (pi,pi); per angle
+// the Fermi momentum on the uniform polar grid, the band velocity, the system
+// angle atan2(v) - pi/2 and the integrand factor |k.k / k.v| (momentum k
+// measured from the origin) times the angle weight; the velocities are then
+// divided by the weighted mean speed and the factors by their sum.
+void tight_binding_surface(HostSetup &S) {
+  const TbBand band{S.tb_hopping_nnn, S.tb_hopping_nnnn, S.tb_chemical_potential};
+  const int na = S.n_angles;
+  const double e_a = band.energy(0.0, M_PI), e_b = band.energy(M_PI, M_PI);
+  S.p_off_x = S.p_off_y = (sgn(e_a) == sgn(e_b)) ? 0.0 : M_PI;
+  S.phi.clear(), S.theta.clear(), S.px.clear(), S.py.clear();
+  S.vx.clear(), S.vy.clear(), S.speed.clear(), S.weight.clear();
+  double wsum = 0.0, psum = 0.0, vsum = 0.0;
+  for (int k = 0; k < na; ++k) {
+    const double ph = wrap_range(M_PI * (double)(2 * k) / (double)na + 0.5 * M_PI, 0.0, 2.0 * M_PI);
+    double px, py, vx, vy;
+    tb_fermi_momentum(band, ph, S.p_off_x, S.p_off_y, px, py);
+    band.grad(px, py, vx, vy);
+    const double kx = wrap_range(px, S.p_off_x - M_PI, S.p_off_x + M_PI) - S.p_off_x;
+    const double ky = wrap_range(py, S.p_off_y - M_PI, S.p_off_y + M_PI) - S.p_off_y;
+    const double jac = std::fabs((kx * kx + ky * ky) / (kx * vx + ky * vy));
+    const double w = jac * angle_weight(k, na);
+    S.phi.push_back(ph);
+    S.theta.push_back(std::atan2(vy, vx) - 0.5 * M_PI);
+    S.px.push_back(px);
+    S.py.push_back(py);
+    S.vx.push_back(vx);
+    S.vy.push_back(vy);
+    S.weight.push_back(w);
+    wsum += w;
+    psum += std::hypot(px, py) * w;
+    vsum += std::hypot(vx, vy) * w;
+  }
+  S.avg_fermi_momentum = psum / wsum;
+  S.avg_fermi_speed = vsum / wsum;
+  for (int k = 0; k < na; ++k) {
+    S.vx[k] /= S.avg_fermi_speed;
+    S.vy[k] /= S.avg_fermi_speed;
+    S.weight[k] /= wsum;
+    S.speed.push_back(std::hypot(S.vx[k], S.vy[k]));  // FermiSurfaceTightBinding::getFermiSpeed
+  }
+}
+
+double lattice_basis(int sym, double px, double py) {
+  switch (sym) {
+  case 0: return std::cos(px) + std::cos(py);
+  case 1: return std::cos(px) - std::cos(py);
+  case 2: return std::sin(px) * std::sin(py);
+  default: return std::sin(px) * std::sin(py) * (std::cos(px) - std::cos(py));
+  }
+}
+
+namespace {
 
 // ------------------------------------------------------- eigen solvers ----
 // Implicit QL iteration on a symmetric tridiagonal matrix (diagonal d,
@@ -712,6 +842,25 @@ std::string build_setup(const std::string &json, HostSetup &S, const SetupOverri
   if (S.nc == 0) return "config: no order-parameter component set";
   S.crystal_rot = 2.0 * M_PI * phys["crystal_axes_rotation"].as_double();
 
+  // Fermi surface model.  The reference selects it in code, through
+  // Context::set(std::unique_ptr<FermiSurface<T>>) (Context.h:49-51; the
+  // drivers keep the default circle, Context.h:189); here the JSON key
+  // physics.fermi_surface = {"type": "tight_binding", "hopping_nnn",
+  // "hopping_nnnn", "chemical_potential"} selects the tight-binding surface,
+  // with the defaults of its constructor (FermiSurfaceTightBinding.h:374-381).
+  {
+    const JsonValue &fs = phys["fermi_surface"];
+    const std::string fs_type = fs["type"].as_string("circle");
+    if (fs_type == "tight_binding") {
+      S.fs_tight_binding = 1;
+      S.tb_hopping_nnn = fs["hopping_nnn"].as_double(0.0);
+      S.tb_hopping_nnnn = fs["hopping_nnnn"].as_double(0.0);
+      S.tb_chemical_potential = fs["chemical_potential"].as_double(1.0);
+    } else if (fs_type != "circle") {
+      return "config: fermi_surface type '" + fs_type + "' not understood";
+    }
+  }
+
   const std::string gauge = phys["gauge"].as_string("symmetric");
   if (gauge == "landau") S.gauge = GAUGE_LANDAU;
   else if (gauge == "symmetric") S.gauge = GAUGE_SYMMETRIC;
@@ -735,24 +884,27 @@ std::string build_setup(const std::string &json, HostSetup &S, const SetupOverri
   S.acc.drag = acc["drag"].as_double(0.5);
   S.acc.rank = acc["rank"].as_int(4);
 
-  // Fermi surface (FermiSurface.h:104-250, FermiSurfaceCircle.h:84-164).
+  // Fermi surface (FermiSurface.h:104-250, FermiSurfaceCircle.h:84-164, or
+  // FermiSurfaceTightBinding.h:384-470).
   const int na = S.n_angles;
-  for (int k = 0; k < na; ++k) {
-    const double ph = wrap_range(M_PI * (double)(2 * k) / (double)na + 0.5 * M_PI, 0.0, 2.0 * M_PI);
-    S.phi.push_back(ph);
-    S.theta.push_back(ph - 0.5 * M_PI);
-    S.vx.push_back(std::cos(ph));
-    S.vy.push_back(std::sin(ph));
+  if (S.fs_tight_binding) {
+    tight_binding_surface(S);
+  } else {
+    for (int k = 0; k < na; ++k) {
+      const double ph = wrap_range(M_PI * (double)(2 * k) / (double)na + 0.5 * M_PI, 0.0, 2.0 * M_PI);
+      S.phi.push_back(ph);
+      S.theta.push_back(ph - 0.5 * M_PI);
+      S.vx.push_back(std::cos(ph));
+      S.vy.push_back(std::sin(ph));
+      S.weight.push_back(angle_weight(k, na) / (double)na);
+      S.speed.push_back(1.0);  // a circle: constant speed (FermiSurfaceCircle.h:51-52)
+    }
+    S.px = S.vx;  // momentum and velocity coincide on the circle
+    S.py = S.vy;
   }
-  for (int k = 0; k < na; ++k) {
-    const int w = wrap_int(k, 0, na);
-    double wt = 1.0;
-    if (na % 4 == 0) wt = (w % 4 == 0) ? 28.0 / 45.0 : (w % 2 == 0) ? 24.0 / 45.0 : 64.0 / 45.0;
-    else if (na % 3 == 0) wt = (w % 3 == 0) ? 6.0 / 8.0 : 9.0 / 8.0;
-    else if (na % 2 == 0) wt = (w % 2 == 0) ? 2.0 / 3.0 : 4.0 / 3.0;
-    S.weight.push_back(wt / (double)na);
-  }
-  auto basis_raw = [](int s, double px, double py) {
+  for (int k = 0; k < na; ++k) S.step.push_back(S.fs_tight_binding ? S.h / S.speed[k] : S.h);
+  auto basis_raw = [&](int s, double px, double py) {
+    if (S.fs_tight_binding) return lattice_basis(s, px, py);
     switch (s) {
     case 0: return 1.0;
     case 1: return px * px - py * py;
@@ -760,11 +912,12 @@ std::string build_setup(const std::string &json, HostSetup &S, const SetupOverri
     default: return px * py * (px * px - py * py);
     }
   };
-  // BasisFunction::normalize, OrderParameterBasis.h:188-212.
+  // BasisFunction::normalize, OrderParameterBasis.h:222-248 (the momentum is
+  // not rotated by the crystal axes here).
   for (int c = 0; c < S.nc; ++c) {
     double avg = 0.0;
     for (int k = 0; k < na; ++k) {
-      const double b = basis_raw(S.sym[c], S.vx[k], S.vy[k]);
+      const double b = basis_raw(S.sym[c], S.px[k], S.py[k]);
       avg += (b * b + 0.0 * 0.0) * S.weight[k];
     }
     S.norm_factor.push_back(1.0 / std::sqrt(avg));
@@ -774,7 +927,7 @@ std::string build_setup(const std::string &json, HostSetup &S, const SetupOverri
   for (int k = 0; k < na; ++k)
     for (int c = 0; c < S.nc; ++c) {
       double rx, ry;
-      rotate(S.crystal_rot, S.vx[k], S.vy[k], rx, ry);
+      rotate(S.crystal_rot, S.px[k], S.py[k], rx, ry);
       S.eta[(size_t)k * S.nc + c] = basis_raw(S.sym[c], rx, ry) * S.norm_factor[c];
     }
   // OrderParameterComponent::initCouplingConstant, OrderParameterComponent.h:156-181.
@@ -948,9 +1101,11 @@ std::string build_setup(const std::string &json, HostSetup &S, const SetupOverri
                          double *wt, double &wsum) {
     double mx, my;
     rotate(sysang, rpx, rpy, mx, my);
-    const double kx = wrap_range(mx, 0.0 - M_PI, 0.0 + M_PI);
-    const double ky = wrap_range(my, 0.0 - M_PI, 0.0 + M_PI);
-    const double ph = wrap_range(std::atan2(ky - 0.0, kx - 0.0) - 0.5 * M_PI, 0.0, 2.0 * M_PI);
+    // FermiSurface::getFractionalAngleIndex (FermiSurface.h:160-184).
+    const double ox = S.p_off_x, oy = S.p_off_y;
+    const double kx = wrap_range(mx, ox - M_PI, ox + M_PI);
+    const double ky = wrap_range(my, oy - M_PI, oy + M_PI);
+    const double ph = wrap_range(std::atan2(ky - oy, kx - ox) - 0.5 * M_PI, 0.0, 2.0 * M_PI);
     const double fai = (double)na * ph / (2.0 * M_PI);
     const int ia[2] = {wrap_int((int)fai, 0, na), wrap_int((int)fai + 1, 0, na)};
     const double rot_ang[2] = {sysang - S.theta[ia[0]], sysang - S.theta[ia[1]]};
@@ -1007,7 +1162,7 @@ std::string build_setup(const std::string &json, HostSetup &S, const SetupOverri
     for (int a = 0; a < na; ++a) {
       const double sa = S.theta[a];
       double px, py;
-      rotate(-sa, S.vx[a], S.vy[a], px, py);
+      rotate(-sa, S.px[a], S.py[a], px, py);  // Fermi momentum in the frame
       const std::vector<BoundaryNode> &nodes = is_g ? lab2[a] : lab3[a];
       const std::vector<int> &first = is_g ? first2[a] : first3[a];
       const std::vector<int> &cnt = is_g ? cnt2[a] : cnt3[a];
@@ -1230,6 +1385,24 @@ int sc_setup_energies(const sc_setup *s, double *e_im, double *residues) {
   for (int i = 0; i < s->S.ne; ++i) {
     if (e_im) e_im[i] = s->S.e_im[i];
     if (residues) residues[i] = s->S.residues[i];
+  }
+  return SC_OK;
+}
+
+int sc_setup_fermi_surface(const sc_setup *s, double *table, double *info) {
+  if (!s) return SC_ERR_ARG;
+  const scb::HostSetup &S = s->S;
+  const int na = S.n_angles;
+  if (table) {
+    const std::vector<double> *cols[8] = {&S.phi, &S.theta, &S.px, &S.py, &S.vx, &S.vy, &S.weight, &S.step};
+    for (int r = 0; r < 8; ++r)
+      for (int k = 0; k < na; ++k) table[(size_t)r * na + k] = (*cols[r])[k];
+  }
+  if (info) {
+    info[0] = S.avg_fermi_momentum;
+    info[1] = S.avg_fermi_speed;
+    info[2] = S.p_off_x;
+    info[3] = S.p_off_y;
   }
   return SC_OK;
 }

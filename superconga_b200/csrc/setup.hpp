@@ -69,8 +69,20 @@ struct HostSetup {
   std::vector<std::string> sym_name;
   std::vector<double> tc, norm_factor, coupling;
 
-  // Fermi surface, per angle.
+  // Fermi surface model: the circle of FermiSurfaceCircle.h (default) or the
+  // square-lattice tight-binding surface of FermiSurfaceTightBinding.h with
+  // the dispersion of DispersionTightBinding.h (nearest-neighbour hopping 1).
+  int fs_tight_binding = 0;
+  double tb_hopping_nnn = 0.0, tb_hopping_nnnn = 0.0, tb_chemical_potential = 1.0;
+  double p_off_x = 0.0, p_off_y = 0.0;                 // momentum origin (0,0) or (pi,pi)
+  double avg_fermi_speed = 1.0, avg_fermi_momentum = 1.0;  // tight binding only
+
+  // Fermi surface, per angle.  phi: polar angle of the momentum; theta: system
+  // angle (velocity angle - pi/2); px, py: Fermi momentum; vx, vy: Fermi
+  // velocity (normalised by its Fermi-surface average); speed = |v|;
+  // step = h / speed, the Riccati step (RiccatiSolverConfined.h:525-527).
   std::vector<double> theta, phi, vx, vy, weight;  // weight = integrand factor
+  std::vector<double> px, py, speed, step;
   std::vector<double> eta;                         // [a * nc + c]
   // Rotation coefficients (single-precision trigonometry promoted to double,
   // GridFunctions_GPU.h:436-489): cD/sD order parameter into the frame, cA/sA
@@ -139,5 +151,11 @@ int num_ozaki_poles(double temperature, double cutoff);
 void ozaki_poles(int n, double *poles, double *residues);
 void symmetric_eigen(int n, std::vector<double> &a, std::vector<double> &w);
 double bulk_s_wave(double temperature);
+// Tight-binding Fermi surface (FermiSurfaceTightBinding.h): fills phi, theta,
+// px, py, vx, vy, speed and weight of S for S.n_angles angles.
+void tight_binding_surface(HostSetup &S);
+// Square-lattice basis functions of a non-circular surface
+// (OrderParameterBasis.h:187-213): sym 0 s, 1 dx2-y2, 2 dxy, 3 g.
+double lattice_basis(int sym, double px, double py);
 
 }  // namespace scb

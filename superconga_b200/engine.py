@@ -309,6 +309,20 @@ class Setup:
         _lib.load().sc_setup_site_updates(self._h, ctypes.byref(v))
         return v.value
 
+    def fermi_surface(self) -> dict:
+        """Per-angle Fermi-surface tables (polar angle, system angle, momentum,
+        normalised velocity, integrand factor, Riccati step) and the
+        tight-binding averages and momentum origin."""
+        na = self.dims.n_angles
+        t = np.zeros((8, na))
+        info = np.zeros(4)
+        _lib.check(_lib.load().sc_setup_fermi_surface(self._h, _p(t), _p(info)))
+        keys = ["phi", "theta", "px", "py", "vx", "vy", "weight", "step"]
+        out = {k: t[i].copy() for i, k in enumerate(keys)}
+        out.update(avg_fermi_momentum=float(info[0]), avg_fermi_speed=float(info[1]),
+                   origin=(float(info[2]), float(info[3])))
+        return out
+
 
 class LdosContext(Context):
     """LDOS postprocess on the current CUDA device, shaped like the Context that
