@@ -60,7 +60,13 @@ __device__ __forceinline__ float rsqrt_(float x) { return rsqrtf(x); }
 __device__ __forceinline__ double sqrt_(double x) {
   return x >= 2.2250738585072014e-308 ? x * rsqrt_(x) : 0.0;  // 0 below the smallest normal
 }
-__device__ __forceinline__ float sqrt_(float x) { return x > 0.0f ? x * rsqrtf(x) : 0.0f; }
+// FP32 square root of a non-negative argument: the hardware approximation
+// (sqrt.approx; 0 for 0), one instruction.
+__device__ __forceinline__ float sqrt_(float x) {
+  float r;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
 
 // Principal square root, branch cut on the negative real axis, through one
 // square root and one reciprocal square root:

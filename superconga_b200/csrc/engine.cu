@@ -272,6 +272,20 @@ __device__ __forceinline__ void site_step(uint8_t l, uint8_t l_entry, uint8_t l_
   }
 }
 
+// The step at a grain site (label 1) between two grain sites: midpoint fields,
+// full step, no boundary bookkeeping (site_step handles the other labels).
+template <typename R, int EMAX, bool KEL>
+__device__ __forceinline__ void interior_step(R dre, R dim, R es, R pdre, R pdim, R pes,
+                                              const R *ere, const R *eim, Cx<R> *coh, int ept,
+                                              R h) {
+  const R sdre = (dre + pdre) * R(0.5);
+  const R sdim = (dim + pdim) * R(0.5);
+  const R ses = (es + pes) * R(0.5);
+#pragma unroll
+  for (int j = 0; j < EMAX; ++j)
+    if (j < ept) coh[j] = riccati_step<R>(sdre, sdim, KEL ? ses + ere[j] : ses, eim[j], coh[j], h);
+}
+
 // The fused Riccati sweep of one chunk of angles.  G = 2^log_groups threads
 // share one trajectory column (angle, x); thread g integrates Ozaki energies
 // [g*ept, g*ept + ept).  gammaTilde runs down the column first and is kept in
@@ -337,22 +351,26 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
         f1 = s2n[ni];
         f2 = s2n[2 * ni];
       }
-      const bool entry = l == 3, exit = l == 2;
-      const R din = entry ? (R)A.dist_in_gt[in_base + nin] : R(0);
-      const R dout = exit ? (R)A.dist_out_gt[out_base + nout] : R(0);
-      site_step<R, EMAX, KEL>(l, 3, 2, dre, dim, es, pdre, pdim, pes, ere, eim, coh, A.ept, ecount, h, din,
-                         A.bin_gt + (size_t)(in_base + nin) * ne + e0, dout,
-                         A.bout_gt + (size_t)(out_base + nout) * ne + e0);
-      if (A.pair && exit) {
-        // gamma of the partner angle at its exit is conj(gammaTilde) here.
-        const Cx<R> *src = A.bout_gt + (size_t)(out_base + nout) * ne + e0;
-        Cx<R> *dst = A.bout_g + (size_t)(A.idx_out_g[pax] + nout) * ne + e0;
+      if (l == 1) {
+        interior_step<R, EMAX, KEL>(dre, dim, es, pdre, pdim, pes, ere, eim, coh, A.ept, h);
+      } else {
+        const bool entry = l == 3, exit = l == 2;
+        const R din = entry ? (R)A.dist_in_gt[in_base + nin] : R(0);
+        const R dout = exit ? (R)A.dist_out_gt[out_base + nout] : R(0);
+        site_step<R, EMAX, KEL>(l, 3, 2, dre, dim, es, pdre, pdim, pes, ere, eim, coh, A.ept, ecount, h,
+                                din, A.bin_gt + (size_t)(in_base + nin) * ne + e0, dout,
+                                A.bout_gt + (size_t)(out_base + nout) * ne + e0);
+        if (A.pair && exit) {
+          // gamma of the partner angle at its exit is conj(gammaTilde) here.
+          const Cx<R> *src = A.bout_gt + (size_t)(out_base + nout) * ne + e0;
+          Cx<R> *dst = A.bout_g + (size_t)(A.idx_out_g[pax] + nout) * ne + e0;
 #pragma unroll
-        for (int j = 0; j < EMAX; ++j)
-          if (j < ecount) dst[j] = Cx<R>{src[j].re, -src[j].im};
+          for (int j = 0; j < EMAX; ++j)
+            if (j < ecount) dst[j] = Cx<R>{src[j].re, -src[j].im};
+        }
+        nin += entry;
+        nout += exit;
       }
-      nin += entry;
-      nout += exit;
       if (!A.burn_in) {
         Cx<R> *sc = A.scratch + (size_t)r * ne * ni + (size_t)e0 * ni + item;
 #pragma unroll
@@ -403,22 +421,26 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
             if (j < ecount) gt_nx[j] = sc[(size_t)j * ni];
         }
       }
-      const bool entry = l == 2, exit = l == 3;
-      const R din = entry ? (R)A.dist_in_g[in_base + nin] : R(0);
-      const R dout = exit ? (R)A.dist_out_g[out_base + nout] : R(0);
-      site_step<R, EMAX, KEL>(l, 2, 3, dre, dim, es, pdre, pdim, pes, ere, eim, coh, A.ept, ecount, h, din,
-                         A.bin_g + (size_t)(in_base + nin) * ne + e0, dout,
-                         A.bout_g + (size_t)(out_base + nout) * ne + e0);
-      if (A.pair && exit) {
-        // gammaTilde of the partner angle at its exit is conj(gamma) here.
-        const Cx<R> *src = A.bout_g + (size_t)(out_base + nout) * ne + e0;
-        Cx<R> *dst = A.bout_gt + (size_t)(A.idx_out_gt[pax] + nout) * ne + e0;
+      if (l == 1) {
+        interior_step<R, EMAX, KEL>(dre, dim, es, pdre, pdim, pes, ere, eim, coh, A.ept, h);
+      } else {
+        const bool entry = l == 2, exit = l == 3;
+        const R din = entry ? (R)A.dist_in_g[in_base + nin] : R(0);
+        const R dout = exit ? (R)A.dist_out_g[out_base + nout] : R(0);
+        site_step<R, EMAX, KEL>(l, 2, 3, dre, dim, es, pdre, pdim, pes, ere, eim, coh, A.ept, ecount, h,
+                                din, A.bin_g + (size_t)(in_base + nin) * ne + e0, dout,
+                                A.bout_g + (size_t)(out_base + nout) * ne + e0);
+        if (A.pair && exit) {
+          // gammaTilde of the partner angle at its exit is conj(gamma) here.
+          const Cx<R> *src = A.bout_g + (size_t)(out_base + nout) * ne + e0;
+          Cx<R> *dst = A.bout_gt + (size_t)(A.idx_out_gt[pax] + nout) * ne + e0;
 #pragma unroll
-        for (int j = 0; j < EMAX; ++j)
-          if (j < ecount) dst[j] = Cx<R>{src[j].re, -src[j].im};
+          for (int j = 0; j < EMAX; ++j)
+            if (j < ecount) dst[j] = Cx<R>{src[j].re, -src[j].im};
+        }
+        nin += entry;
+        nout += exit;
       }
-      nin += entry;
-      nout += exit;
       pdre = dre;
       pdim = dim;
       pes = es;
