@@ -215,17 +215,21 @@ __device__ __forceinline__ void group_sum4_scatter(double v[4], int g, int log_g
 
 // Rotated order parameter and Doppler shift of every site of every trajectory
 // column of a chunk, written to scratch2[row][3][item] for the sweep.
+// Block (FF_COLS, FF_ROWS): a warp covers 8 neighbouring columns x 4 rows, a
+// compact patch of the frame whose rotated corners fall on few cache lines of
+// the reference grid (a warp along one row touched ~20 sectors per gather).
+constexpr int FF_COLS = 8, FF_ROWS = 16;
 template <typename R>
-__global__ void __launch_bounds__(128) k_frame_fields(const SweepArgs<R> A, int rows_per_thread) {
-  const int item = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(FF_COLS * FF_ROWS) k_frame_fields(const SweepArgs<R> A, int rows_per_block) {
+  const int item = blockIdx.x * FF_COLS + threadIdx.x;
   if (item >= A.n_items) return;
   const int4 it = A.items[item];
   const int a = it.x, x = it.y, lo = it.z, hi = it.w;
   const AngleParams P = A.ang[a];
   const size_t ni = (size_t)A.n_items;
-  const int r0 = blockIdx.y * rows_per_thread;
-  const int r1 = min(r0 + rows_per_thread, hi - lo + 1);
-  for (int r = r0; r < r1; ++r) {
+  const int r0 = blockIdx.y * rows_per_block;
+  const int r1 = min(r0 + rows_per_block, hi - lo + 1);
+  for (int r = r0 + threadIdx.y; r < r1; r += FF_ROWS) {
     double dre, dim, es;
     frame_fields(A, P, x, lo + r, dre, dim, es);
     R *s2 = A.scratch2 + (size_t)r * 3 * ni + item;
@@ -590,8 +594,14 @@ __global__ void __launch_bounds__(256) k_rotate_back(int n0, int n1, int nc, int
     const bool mirrored = pair && (k & 1);
     const int a = mirrored ? a0 + pair : a0;
     const AngleParams &P = ang[a];
+    // A site whose lookup falls outside the frame adds exact zeros (weights
+    // 0, corners read at the frame origin): the same sums as skipping it, and
+    // the loop stays free of branches so that the loads of consecutive angles
+    // overlap.
     Bilinear b;
-    if (!rotated_lookup(x, y, n0, n1, P.cB, P.sB, b)) continue;
+    const bool inside = rotated_lookup(x, y, n0, n1, P.cB, P.sB, b);
+    if (!inside) b = Bilinear{0, 0.0, 0.0};
+    const double pw = inside ? P.w : 0.0, psx = inside ? P.sx : 0.0, psy = inside ? P.sy : 0.0;
     double2 f00, f01, f10, f11, q00, q01, q10, q11;
     const size_t slot = (size_t)(a0 - a_begin) * nn1;
     if (!mirrored) {
@@ -609,12 +619,12 @@ __global__ void __launch_bounds__(256) k_rotate_back(int n0, int n1, int nc, int
     const double fim = bilerp(f00.y, f01.y, f10.y, f11.y, b.xf, b.yf);
     for (int c = 0; c < nc; ++c) {
       const double et = P.eta[c];
-      dr[c] += (fre * et) * P.w;
-      di[c] += (fim * et) * P.w;
+      dr[c] += (fre * et) * pw;
+      di[c] += (fim * et) * pw;
     }
-    jx += bilerp(q00.x * P.sx, q01.x * P.sx, q10.x * P.sx, q11.x * P.sx, b.xf, b.yf);
-    jy += bilerp(q00.x * P.sy, q01.x * P.sy, q10.x * P.sy, q11.x * P.sy, b.xf, b.yf);
-    fe += bilerp(q00.y * P.w, q01.y * P.w, q10.y * P.w, q11.y * P.w, b.xf, b.yf);
+    jx += bilerp(q00.x * psx, q01.x * psx, q10.x * psx, q11.x * psx, b.xf, b.yf);
+    jy += bilerp(q00.x * psy, q01.x * psy, q10.x * psy, q11.x * psy, b.xf, b.yf);
+    fe += bilerp(q00.y * pw, q01.y * pw, q10.y * pw, q11.y * pw, b.xf, b.yf);
   }
   for (int c = 0; c < nc; ++c) {
     acc_d[(size_t)(2 * c) * nn0 + i] = dr[c];
@@ -1433,9 +1443,9 @@ SweepArgs<R> sweep_args(sc_ctx *c, const Chunk *ch, int burn_in) {
 template <typename R>
 void launch_frame_fields(sc_ctx *c, const Chunk &ch, const SweepArgs<R> &A) {
   if (!A.n_items) return;
-  const int rows = 16;
-  dim3 grid(grid1(A.n_items, 128), (unsigned)((ch.kmax + rows - 1) / rows));
-  k_frame_fields<R><<<grid, 128, 0, c->stream>>>(A, rows);
+  const int rows = 4 * FF_ROWS;  // rows per block, four per thread
+  dim3 grid(grid1(A.n_items, FF_COLS), (unsigned)((ch.kmax + rows - 1) / rows));
+  k_frame_fields<R><<<grid, dim3(FF_COLS, FF_ROWS), 0, c->stream>>>(A, rows);
   check_launch(c);
 }
 
@@ -1672,7 +1682,9 @@ void frame_to_reference(sc_ctx *c, const Chunk &ch) {
                                                         (Fr *)c->w_fg, (Fr *)c->w_gi);
     check_launch(c);
   }
-  dim3 blk(32, 8), grid((S.n0 + 31) / 32, (S.n0 + 7) / 8);
+  // A warp covers an 8 x 4 patch of the reference grid (its rotated corners
+  // share cache lines of the frame).
+  dim3 blk(8, 32), grid((S.n0 + 7) / 8, (S.n0 + 31) / 32);
   ProfScope prof(c, 1);
   k_rotate_back<<<grid, blk, 0, c->stream>>>(S.n0, S.n1, S.nc, ch.a_begin, a_stored, pair, c->ang.p,
                                              (const Fr *)c->w_fg, (const Fr *)c->w_gi,
