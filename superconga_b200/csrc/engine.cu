@@ -56,10 +56,24 @@ constexpr int NQ = 48;  // partial-sum slots of the finalize reduction
 
 // ------------------------------------------------------------------ kernels --
 
+// The reference-grid fields the frame lookups gather, one record per site:
+// rf[site * (nc + 1) + c] = (Re, Im) of order-parameter component c and
+// rf[site * (nc + 1) + nc] = (A_x, A_y) of the induced vector potential, so
+// that a bilinear corner costs one 16-byte load per field pair instead of two
+// 8-byte loads from separate planes.  k_pack_reference copies the state
+// (planar, [2 nc + 2][N0 * N0]) into it.
+__global__ void k_pack_reference(int nc, int nn, const double *__restrict__ x, double2 *__restrict__ rf) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nn) return;
+  double2 *r = rf + (size_t)i * (nc + 1);
+  for (int c = 0; c <= nc; ++c) r[c] = make_double2(x[(size_t)(2 * c) * nn + i], x[(size_t)(2 * c + 1) * nn + i]);
+}
+
 // Reference-grid extension of the order parameter (domain_ops.h:11-69):
-// out = in everywhere, except label-0 sites next to the grain, which get the
-// mean of their nearest grain sites.
-__global__ void k_extend_reference(int n_fields, int nn, int n_sites, const int *__restrict__ site,
+// the order parameter everywhere, except label-0 sites next to the grain,
+// which get the mean of their nearest grain sites; written into the records
+// of k_pack_reference (field f = 2c + part of component c).
+__global__ void k_extend_reference(int n_fields, int nn, int n_sites, int stride, const int *__restrict__ site,
                                    const int *__restrict__ off, const int *__restrict__ src,
                                    const double *__restrict__ in, double *__restrict__ out) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -69,7 +83,7 @@ __global__ void k_extend_reference(int n_fields, int nn, int n_sites, const int 
   const int b = off[k], e = off[k + 1];
   double acc = v[src[b]];
   for (int i = b + 1; i < e; ++i) acc = __dadd_rn(acc, v[src[i]]);
-  out[(size_t)f * nn + site[k]] = __ddiv_rn(acc, (double)(e - b));
+  out[((size_t)site[k] * stride + (f >> 1)) * 2 + (f & 1)] = __ddiv_rn(acc, (double)(e - b));
 }
 
 // Element of the frame buffers: the per-angle Matsubara sums are accumulated in
@@ -105,8 +119,7 @@ struct SweepArgs {
   const double *dist_in_g, *dist_out_g, *dist_in_gt, *dist_out_gt;
   const Cx<R> *bin_g, *bin_gt;
   Cx<R> *bout_g, *bout_gt;
-  const double *dext;  // [c][2][n0*n0]
-  const double *avec;  // [2][n0*n0]
+  const double2 *rf;   // [n0*n0][nc + 1]: extended order parameter per component, then A (k_pack_reference)
   const double *e_re, *e_im, *res;
   Cx<R> *scratch;   // [row][energy][item]
   R *scratch2;      // [row][3][item]: Re D, Im D, energy shift (in R: the sweep steps in R)
@@ -138,20 +151,19 @@ template <typename R>
 __device__ __forceinline__ void frame_fields(const SweepArgs<R> &A, const AngleParams &P, int x,
                                              int y, double &dre, double &dim, double &es) {
   const int n0 = A.n0;
-  const size_t nn0 = (size_t)n0 * n0;
   Bilinear b;
   dre = 0.0;
   dim = 0.0;
+  const int st = A.nc + 1;
   if (rotated_lookup(x, y, A.n1, n0, P.cD, P.sD, b)) {
     double c_re[4] = {0, 0, 0, 0}, c_im[4] = {0, 0, 0, 0};
     const int off[4] = {b.i00, b.i00 + 1, b.i00 + n0, b.i00 + n0 + 1};
     for (int c = 0; c < A.nc; ++c) {
-      const double *pr = A.dext + (size_t)(2 * c) * nn0;
-      const double *pi = pr + nn0;
       const double et = P.eta[c];
       for (int k = 0; k < 4; ++k) {
-        c_re[k] += __ldg(pr + off[k]) * et;
-        c_im[k] += __ldg(pi + off[k]) * et;
+        const double2 v = __ldg(A.rf + (size_t)off[k] * st + c);
+        c_re[k] += v.x * et;
+        c_im[k] += v.y * et;
       }
     }
     dre = bilerp(c_re[0], c_re[1], c_re[2], c_re[3], b.xf, b.yf);
@@ -168,11 +180,11 @@ __device__ __forceinline__ void frame_fields(const SweepArgs<R> &A, const AngleP
       double rx = 0.0, ry = 0.0;
       Bilinear ba;
       if (rotated_lookup(x, y, A.n1, n0, P.cA, P.sA, ba)) {
-        const double *px = A.avec, *py = A.avec + nn0;
-        rx = bilerp(__ldg(px + ba.i00), __ldg(px + ba.i00 + 1), __ldg(px + ba.i00 + n0),
-                    __ldg(px + ba.i00 + n0 + 1), ba.xf, ba.yf);
-        ry = bilerp(__ldg(py + ba.i00), __ldg(py + ba.i00 + 1), __ldg(py + ba.i00 + n0),
-                    __ldg(py + ba.i00 + n0 + 1), ba.xf, ba.yf);
+        const double2 *pa = A.rf + A.nc;
+        const double2 v00 = __ldg(pa + (size_t)ba.i00 * st), v01 = __ldg(pa + (size_t)(ba.i00 + 1) * st);
+        const double2 v10 = __ldg(pa + (size_t)(ba.i00 + n0) * st), v11 = __ldg(pa + (size_t)(ba.i00 + n0 + 1) * st);
+        rx = bilerp(v00.x, v01.x, v10.x, v11.x, ba.xf, ba.yf);
+        ry = bilerp(v00.y, v01.y, v10.y, v11.y, ba.xf, ba.yf);
       }
       rx *= A.lam_scale;
       ry *= A.lam_scale;
@@ -225,7 +237,7 @@ __global__ void __launch_bounds__(FF_COLS * FF_ROWS) k_frame_fields(const SweepA
   if (item >= A.n_items) return;
   const int4 it = A.items[item];
   const int a = it.x, x = it.y, lo = it.z, hi = it.w;
-  const AngleParams P = A.ang[a];
+  const AngleParams &P = A.ang[a];  // read in place (a local copy went to the stack)
   const size_t ni = (size_t)A.n_items;
   const int r0 = blockIdx.y * rows_per_block;
   const int r1 = min(r0 + rows_per_block, hi - lo + 1);
@@ -1310,7 +1322,7 @@ struct sc_ctx {
   int pair = 0;  // > 0: mixed mode sweeps angles [0, n/2) and mirrors them onto [n/2, n)
 
   // state: x = [delta | avec], g = [delta_new | a_new]
-  DevArray<double> xstate, gstate, dext, j_real;
+  DevArray<double> xstate, gstate, rfields, j_real;
   DevArray<double> acc_d, acc_j, acc_fe;
   DevArray<double> bnd;      // boundary storage (4 arrays), R-typed, viewed through pointers
   size_t bnd_off[4] = {0, 0, 0, 0};
@@ -1427,8 +1439,7 @@ SweepArgs<R> sweep_args(sc_ctx *c, const Chunk *ch, int burn_in) {
   A.bout_g = (Cx<R> *)c->bnd_ptr(1);
   A.bin_gt = (const Cx<R> *)c->bnd_ptr(2);
   A.bout_gt = (Cx<R> *)c->bnd_ptr(3);
-  A.dext = c->dext.p;
-  A.avec = c->xstate.p + (size_t)2 * S.nc * c->nn0();
+  A.rf = (const double2 *)c->rfields.p;
   A.e_re = c->e_re.p;
   A.e_im = c->e_im.p;
   A.res = c->res.p;
@@ -1457,9 +1468,11 @@ void launch_sweep(sc_ctx *c, const Chunk &ch, int burn_in) {
   const unsigned blocks = grid1(threads, 128);
   launch_frame_fields<R>(c, ch, A);
   ProfScope prof(c, 0);
-  // FP64 runs best with four resident blocks per SM (measured on B200).
+  // Both precisions run best with four resident blocks per SM (measured on
+  // B200: FP64 four energies per thread; mixed two, 10.5 ms on C2 against
+  // 11.2 ms with five or six blocks).
   static const char *minb_env = std::getenv("SCB_SWEEP_MINB");
-  const int variant = minb_env ? std::atoi(minb_env) : (sizeof(R) == 8 ? 4 : (c->emax2 ? 6 : 1));
+  const int variant = minb_env ? std::atoi(minb_env) : (sizeof(R) == 8 ? 4 : (c->emax2 ? 4 : 1));
   if (c->S.fs_tight_binding) {
     // Non-circular Fermi surface: per-angle step, generic mappings.
     if (c->S.keldysh) {
@@ -1477,6 +1490,7 @@ void launch_sweep(sc_ctx *c, const Chunk &ch, int burn_in) {
     else k_sweep<R, 16, 1, true><<<blocks, 128, 0, c->stream>>>(A);
   } else if (c->ept <= 2 && c->emax2) {
     if (variant >= 6) k_sweep<R, 2, 6, false><<<blocks, 128, 0, c->stream>>>(A);
+    else if (variant == 5) k_sweep<R, 2, 5, false><<<blocks, 128, 0, c->stream>>>(A);
     else k_sweep<R, 2, 4, false><<<blocks, 128, 0, c->stream>>>(A);
   } else if (c->ept <= 4) {
     if (variant == 4) k_sweep<R, 4, 4, false><<<blocks, 128, 0, c->stream>>>(A);
@@ -1492,13 +1506,14 @@ void launch_sweep(sc_ctx *c, const Chunk &ch, int burn_in) {
 
 void extend_reference(sc_ctx *c) {
   const HostSetup &S = c->S;
-  const size_t bytes = (size_t)2 * S.nc * c->nn0() * sizeof(double);
-  CUDA_TRY(cudaMemcpyAsync(c->dext.p, c->xstate.p, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  const int nn = (int)c->nn0();
+  k_pack_reference<<<grid1(nn, 256), 256, 0, c->stream>>>(S.nc, nn, c->xstate.p, (double2 *)c->rfields.p);
+  check_launch(c);
   const int ns = (int)S.rext_site.size();
   if (ns) {
     dim3 grid(grid1(ns, 128), 2 * S.nc);
-    k_extend_reference<<<grid, 128, 0, c->stream>>>(2 * S.nc, (int)c->nn0(), ns, c->rext_site.p,
-                                                    c->rext_off.p, c->rext_src.p, c->xstate.p, c->dext.p);
+    k_extend_reference<<<grid, 128, 0, c->stream>>>(2 * S.nc, nn, ns, S.nc + 1, c->rext_site.p, c->rext_off.p,
+                                                    c->rext_src.p, c->xstate.p, c->rfields.p);
     check_launch(c);
   }
 }
@@ -2046,7 +2061,7 @@ void upload_static(sc_ctx *c) {
   const char *eg = std::getenv("SCB_ENERGY_GROUPS");
   // Default (fastest measured on B200 for 7-14 Ozaki energies): FP64 the fewest
   // threads per column that keep at most four energies per thread; mixed
-  // precision at most two, so that six blocks fit on an SM.
+  // precision at most two; four resident blocks per SM in both.
   const bool fp32_sweep = c->mode == SC_MODE_MIXED && !S.keldysh;
   const int per_thread = fp32_sweep ? 2 : 4;
   int want = 1;
@@ -2058,7 +2073,7 @@ void upload_static(sc_ctx *c) {
     int dev = 0, n_sm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-    const double resident = (double)n_sm * (fp32_sweep ? 6 : 4) * 128;
+    const double resident = (double)n_sm * 4 * 128;
     size_t max_items = 0;
     for (const Chunk &ch : c->chunks) max_items = std::max(max_items, (size_t)(ch.item_end - ch.item_begin));
     while ((double)max_items * want < 2.0 * resident && want < 8 && (S.ne + want - 1) / want > 1) want *= 2;
@@ -2078,7 +2093,7 @@ void upload_static(sc_ctx *c) {
   c->gstate.alloc((size_t)(2 * S.nc + 2) * nn);
   c->xstate.zero(s);
   c->gstate.zero(s);
-  c->dext.alloc((size_t)2 * S.nc * nn);
+  c->rfields.alloc((size_t)2 * (S.nc + 1) * nn);
   c->j_real.alloc(2 * nn);
   c->j_real.zero(s);
   c->acc_d.alloc((size_t)2 * S.nc * nn);
@@ -2125,7 +2140,7 @@ void upload_static(sc_ctx *c) {
     c->w_gi = c->gi.p;
   }
   c->nb_fin = std::min<int>(592, (int)grid1(nn, REDUCE_THREADS));
-  c->nb_bnd = std::min<int>(296, (int)grid1((size_t)std::max(S.n_in_g, S.n_in_gt) * S.ne, REDUCE_THREADS));
+  c->nb_bnd = std::min<int>(592, (int)grid1((size_t)std::max(S.n_in_g, S.n_in_gt) * S.ne, REDUCE_THREADS));
   c->nb_vp = std::min<int>(296, (int)grid1(2 * nn, REDUCE_THREADS));
   c->nb_acc = std::min<int>(148, (int)grid1(nn, REDUCE_THREADS));
   c->partial_fin.alloc((size_t)c->nb_fin * NQ);
@@ -2859,6 +2874,8 @@ void launch_batch_sweep(sc_batch *b, sc_batch::Wave &w, int wi) {
   };
   if (ept <= 2 && b->minb == 6) {
     run(k_sweep_batch<R, 2, 6>);
+  } else if (ept <= 2 && b->minb == 4) {
+    run(k_sweep_batch<R, 2, 4>);
   } else if (ept <= 4) {
     if (b->minb == 4) run(k_sweep_batch<R, 4, 4>);
     else run(k_sweep_batch<R, 4, 1>);
@@ -3072,7 +3089,7 @@ int sc_batch_create(const char *const *configs, int n, int mode, sc_batch **out)
     // Threads per column, per grain: the fewest that keep at most four (FP64)
     // or two (mixed) energies per thread.
     b->ept_max = mode == SC_MODE_FP64 ? 4 : 2;
-    b->minb = mode == SC_MODE_FP64 ? 4 : 1;
+    b->minb = 4;
     if (mode == SC_MODE_FP64) batch_plan<double>(b);
     else batch_plan<float>(b);
   } catch (const EngineError &e) {
@@ -3223,7 +3240,7 @@ extern "C" {
 // keeps the fastest and returns it.
 int sc_batch_autotune(sc_batch *b, int *energies_per_thread, int *minb, double *best_ms) {
   if (!b) return SC_ERR_ARG;
-  const int cand[][2] = {{1, 6}, {2, 6}, {2, 1}, {4, 4}, {4, 1}, {8, 1}};
+  const int cand[][2] = {{1, 4}, {2, 4}, {2, 6}, {4, 4}, {4, 1}, {8, 1}};
   int best_e = b->ept_max, best_mb = b->minb;
   double best = 1e300;
   for (const auto &cd : cand) {
