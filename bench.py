@@ -307,7 +307,8 @@ def converge_c1(max_it: int, max_s: float):
 def batched_c3(n_grains: int, iters: int, max_s: float):
     """The C3 batch (n seeded grains) in both precisions: device-timed batch
     iterations (CUDA-graph replays) after autotuning, then every grain run to
-    its own convergence (bounded)."""
+    its own convergence (bounded); and the plain FP64 form, one grain at a
+    time, for the mixed-batched against plain comparison."""
     import numpy as np
     import torch
     import superconga_b200 as sb
@@ -322,8 +323,14 @@ def batched_c3(n_grains: int, iters: int, max_s: float):
             g.set_state(d, a)
         su = int(b.site_updates().sum())
         t0 = time.perf_counter()
-        b.compute(1)
+        b.compute(1)  # first iteration (initial boundary values)
+        torch.cuda.synchronize()
+        t_first = time.perf_counter() - t0
+        # Tuning is set-up, like the contexts' creation: timed apart.
+        ta = time.perf_counter()
         lg, mb, _ = b.autotune()
+        t_tune = time.perf_counter() - ta
+        t1 = time.perf_counter()
         b.compute(1)  # graph capture
         torch.cuda.synchronize()
         l0 = b.launch_count()
@@ -337,8 +344,9 @@ def batched_c3(n_grains: int, iters: int, max_s: float):
         launches = (b.launch_count() - l0) / iters
         act, it, r = b.status()
         full = bool(act.all())
-        while b.compute(1) > 0 and time.perf_counter() - t0 < max_s:
+        while b.compute(1) > 0 and time.perf_counter() - t1 < max_s:
             pass
+        t_all = t_first + time.perf_counter() - t1
         act, it, r = b.status()
         conv = [bool(r[k] < 1e-6) for k in range(len(cfgs))]
         res[mode] = {"site_updates_per_s": su / (ms * 1e-3) if full else None,
@@ -346,11 +354,42 @@ def batched_c3(n_grains: int, iters: int, max_s: float):
                      "all_grains_active_while_timed": full,
                      "kernel_launches_per_iteration": launches,
                      "sweep_mapping": {"max_energies_per_thread": lg, "min_blocks_per_sm": mb},
-                     "seconds_all_grains": time.perf_counter() - t0,
+                     "seconds_all_grains": t_all, "autotune_seconds": t_tune,
                      "grains_converged": int(sum(conv)), "grains_at_iteration_cap": int(np.sum(~act) - sum(conv)),
                      "grains_still_running": int(np.sum(act)),
                      "median_iterations": float(np.median(it))}
+        if mode == "fp64":
+            it_fp64, done_fp64 = np.asarray(it), not bool(np.any(act))
         b.close()
+    # The plain form: every grain as its own FP64 context, one after the other
+    # (the reference runs one grain per process).  Each grain's iteration time
+    # is measured (two device-timed iterations after the first); its iteration
+    # count is the FP64 batch's, which gives the same iterates (batch = single
+    # runs to 1e-11), so the total is sum_g iterations_g x ms_g.
+    plain_ms = []
+    for c, st in zip(cfgs, states):
+        ctx = sb.Context(c, mode="fp64")
+        d, a = workloads.c3_initial_state(c, st, ctx.dims.n0)
+        ctx.set_state(d, a)
+        ctx.compute(1)
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        ctx.compute(2)
+        ev1.record()
+        torch.cuda.synchronize()
+        plain_ms.append(ev0.elapsed_time(ev1) / 2)
+        ctx.close()
+    plain_ms = np.asarray(plain_ms)
+    est = float(np.sum(plain_ms * it_fp64)) / 1e3
+    res["plain_fp64_one_grain_at_a_time"] = {
+        "ms_per_iteration_all_grains": float(plain_ms.sum()),
+        "seconds_all_grains": est if done_fp64 else None,
+        "method": "per-grain device-timed FP64 iteration x that grain's FP64 iteration count"}
+    res["mixed_batched_over_plain_fp64"] = {
+        "per_iteration": float(plain_ms.sum()) / res["mixed"]["ms_per_iteration"],
+        "all_grains": (est / res["mixed"]["seconds_all_grains"]) if done_fp64 else None}
     return res
 
 

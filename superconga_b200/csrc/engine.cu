@@ -1323,6 +1323,7 @@ struct sc_ctx {
 
   // state: x = [delta | avec], g = [delta_new | a_new]
   DevArray<double> xstate, gstate, rfields, j_real;
+  std::vector<int4> h_items;  // trajectory columns (angle, x, first row, last row), host copy
   DevArray<double> acc_d, acc_j, acc_fe;
   DevArray<double> bnd;      // boundary storage (4 arrays), R-typed, viewed through pointers
   size_t bnd_off[4] = {0, 0, 0, 0};
@@ -1566,17 +1567,22 @@ void launch_scalars_b(sc_ctx *c, int do_bc, int do_vp, int compute_mode, size_t 
 // 2D FFT of the P x P array z (rows, transpose into t, rows): the spectrum
 // ends in t in transposed layout [k_col][k_row].  The inverse takes t in that
 // layout and leaves the result in z in the original layout.
-void fft2(sc_ctx *c, double2 *z, double2 *t, int inverse) {
+// 2D FFT of a P x P array: rows of `first`, transpose into `second`, rows of
+// `second` (so the spectrum is transposed; the inverse undoes it).  Only the
+// first rows_in rows of `first` can be non-zero (the transform of a zero row is
+// zero, so the others are left as they are), and only the first rows_out rows
+// of the result are needed (the transpose and the last pass stop there).
+void fft2(sc_ctx *c, double2 *z, double2 *t, int inverse, int rows_in, int rows_out) {
   const int P = c->fft_p, lg = c->fft_log2p;
   const int thr = std::min(P / 2, 512);
   const size_t smem = (size_t)P * sizeof(double2);
-  const dim3 tb(32, 8), tg(P / 32, P / 32);
+  const dim3 tb(32, 8), tg((rows_out + 31) / 32, P / 32);
   double2 *first = inverse ? t : z, *second = inverse ? z : t;
-  k_fft_rows<<<P, thr, smem, c->stream>>>(lg, (const double2 *)c->fft_tw.p, first, inverse);
+  k_fft_rows<<<rows_in, thr, smem, c->stream>>>(lg, (const double2 *)c->fft_tw.p, first, inverse);
   check_launch(c);
   k_fft_transpose<<<tg, tb, 0, c->stream>>>(P, first, second);
   check_launch(c);
-  k_fft_rows<<<P, thr, smem, c->stream>>>(lg, (const double2 *)c->fft_tw.p, second, inverse);
+  k_fft_rows<<<rows_out, thr, smem, c->stream>>>(lg, (const double2 *)c->fft_tw.p, second, inverse);
   check_launch(c);
 }
 
@@ -1598,10 +1604,10 @@ void poisson(sc_ctx *c, const double *j, double *a_out, int mean_from_scalars) {
   double2 *z = (double2 *)c->fft_z.p, *t = (double2 *)c->fft_t.p;
   k_fft_pack<<<grid1(pp, 256), 256, 0, c->stream>>>(n, P, c->pois_s.p, z);
   check_launch(c);
-  fft2(c, z, t, 0);
+  fft2(c, z, t, 0, n, P);  // the current fills rows < N0 of z
   k_fft_mul<<<grid1(pp, 256), 256, 0, c->stream>>>(pp, (const double2 *)c->fft_kf.p, t);
   check_launch(c);
-  fft2(c, z, t, 1);
+  fft2(c, z, t, 1, P, n);  // A is read from rows < N0 of z
   k_fft_unpack<<<grid1(c->nn0(), 256), 256, 0, c->stream>>>(n, P, 1.0 / ((double)P * (double)P), z, a_out);
   check_launch(c);
 }
@@ -1646,7 +1652,7 @@ void poisson_setup(sc_ctx *c) {
   CUDA_TRY(cudaMemcpyAsync(c->fft_z.p, kr.data(), 2 * pp * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   if (P * sizeof(double2) > 48 * 1024)
     CUDA_TRY(cudaFuncSetAttribute(k_fft_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(P * sizeof(double2))));
-  fft2(c, (double2 *)c->fft_z.p, (double2 *)c->fft_kf.p, 0);
+  fft2(c, (double2 *)c->fft_z.p, (double2 *)c->fft_kf.p, 0, P, P);
   CUDA_TRY(cudaStreamSynchronize(c->stream));
 }
 
@@ -2055,6 +2061,7 @@ void upload_static(sc_ctx *c) {
   std::vector<int4> items;
   plan_chunks(c, items);
   c->items.upload(items, s);
+  c->h_items = items;  // host copy: the batch plans its work units from it
   // Energy groups per column.
   c->groups = 1;
   c->log_groups = 0;
@@ -2835,9 +2842,7 @@ void batch_plan(sc_batch *b) {
       const Chunk &ch = c->chunks[0];
       args.push_back(sweep_args<R>(c, &ch, 0));
       const int n = ch.item_end - ch.item_begin;
-      std::vector<int4> items(n);
-      if (n)
-        CUDA_TRY(cudaMemcpy(items.data(), c->items.p + ch.item_begin, n * sizeof(int4), cudaMemcpyDeviceToHost));
+      const int4 *items = c->h_items.data() + ch.item_begin;
       for (int i = 0; i < n; i += per_warp) {
         int len = 0;
         for (int j = i; j < std::min(n, i + per_warp); ++j) len = std::max(len, items[j].w - items[j].z + 1);
