@@ -219,8 +219,8 @@ int sc_batch_set_graph(sc_batch *b, int enable);
 /* Mapping of the persistent sweep: each grain takes the fewest threads per
  * trajectory column (1, 2, 4 or 8) that keep at most energies_per_thread
  * energies on a thread, and minb selects the resident-block variant (1: up
- * to 255 registers per thread, 4: at most 128, 6: at most 80 with at most two
- * energies per thread).  sc_batch_autotune times the feasible choices on the
+ * to 255 registers per thread, 3: at most 168, 4: at most 128, 6: at most 80;
+ * 3 with at most four energies per thread, 6 with at most two).  sc_batch_autotune times the feasible choices on the
  * current state (after at least one iteration) and keeps the fastest. */
 int sc_batch_config(sc_batch *b, int energies_per_thread, int minb);
 int sc_batch_get_config(const sc_batch *b, int *energies_per_thread, int *minb, int *n_waves);

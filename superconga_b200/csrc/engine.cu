@@ -903,31 +903,116 @@ __global__ void k_subtract_mean(int n0, const double *__restrict__ j, const doub
 // kernel's spectrum is computed once at set-up.  O(P^2 log P) instead of
 // O(K N0^3); the results agree with the direct filter sums to rounding.
 
-// P-point FFT of every row (P = 2^log2p <= 4096) in shared memory: iterative
-// radix-2 Cooley-Tukey, bit-reversed load; tw[q] = exp(-2 pi i q / P),
-// q < P/2 (conjugated for the inverse).
-__global__ void __launch_bounds__(512) k_fft_rows(int log2p, const double2 *__restrict__ tw, double2 *data,
-                                                  int inverse) {
-  extern __shared__ double2 sm[];
-  const int P = 1 << log2p;
-  double2 *row = data + (size_t)blockIdx.x * P;
-  for (int i = threadIdx.x; i < P; i += blockDim.x) sm[__brev((unsigned)i) >> (32 - log2p)] = row[i];
-  __syncthreads();
-  for (int st = 1; st <= log2p; ++st) {
-    const int half = 1 << (st - 1), stride = P >> st;
-    for (int j = threadIdx.x; j < P / 2; j += blockDim.x) {
-      const int t = j & (half - 1);
-      const int i1 = ((j >> (st - 1)) << st) + t, i2 = i1 + half;
-      double2 w = tw[t * stride];
-      if (inverse) w.y = -w.y;
-      const double2 u = sm[i1], v0 = sm[i2];
-      const double vr = v0.x * w.x - v0.y * w.y, vi = v0.x * w.y + v0.y * w.x;
-      sm[i1] = make_double2(u.x + vr, u.y + vi);
-      sm[i2] = make_double2(u.x - vr, u.y - vi);
-    }
-    __syncthreads();
+// P-point FFT of every row in shared memory, P = 2^a 3^b 5^c <= 4096: the
+// Stockham autosort formulation (Govindaraju et al., "High performance
+// discrete Fourier transforms on graphics processors", SC 2008) with mixed
+// radices 2, 3, 4, 5, ping-ponging between two shared buffers.  Stage s with
+// radix R and Ns = product of the earlier radices: butterfly j (< P/R) reads
+// x[j + r P/R], twiddles it by w^(r k), k = j mod Ns, w = exp(-2 pi i / (Ns R)),
+// takes the R-point DFT and writes y[(j / Ns) Ns R + k + r Ns].
+// tw[q] = exp(-2 pi i q / P), q < P (conjugated for the inverse).
+struct FftPlan {
+  int n_stages;
+  int radix[16];
+};
+
+__device__ __forceinline__ double2 cmul_d2(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// (x + i y) times s i, s = +1 or -1.
+__device__ __forceinline__ double2 times_si(double2 a, double s) { return make_double2(-s * a.y, s * a.x); }
+
+// R-point DFTs with exponent sign s (-1 forward, +1 inverse); the constants
+// are cos and sin of 2 pi / 3, 2 pi / 5 and 4 pi / 5.
+template <int R>
+__device__ __forceinline__ void dft_small(double2 *v, double s) {
+  if constexpr (R == 2) {
+    const double2 a = v[0], b = v[1];
+    v[0] = make_double2(a.x + b.x, a.y + b.y);
+    v[1] = make_double2(a.x - b.x, a.y - b.y);
+  } else if constexpr (R == 4) {
+    const double2 t0 = make_double2(v[0].x + v[2].x, v[0].y + v[2].y);
+    const double2 t1 = make_double2(v[0].x - v[2].x, v[0].y - v[2].y);
+    const double2 t2 = make_double2(v[1].x + v[3].x, v[1].y + v[3].y);
+    const double2 t3 = times_si(make_double2(v[1].x - v[3].x, v[1].y - v[3].y), s);
+    v[0] = make_double2(t0.x + t2.x, t0.y + t2.y);
+    v[2] = make_double2(t0.x - t2.x, t0.y - t2.y);
+    v[1] = make_double2(t1.x + t3.x, t1.y + t3.y);
+    v[3] = make_double2(t1.x - t3.x, t1.y - t3.y);
+  } else if constexpr (R == 3) {
+    const double H3 = 0.86602540378443864676;  // sin(2 pi / 3) = sqrt(3) / 2
+    const double2 t = make_double2(v[1].x + v[2].x, v[1].y + v[2].y);
+    const double2 u = times_si(make_double2(H3 * (v[1].x - v[2].x), H3 * (v[1].y - v[2].y)), s);
+    const double2 m = make_double2(v[0].x - 0.5 * t.x, v[0].y - 0.5 * t.y);
+    v[0] = make_double2(v[0].x + t.x, v[0].y + t.y);
+    v[1] = make_double2(m.x + u.x, m.y + u.y);
+    v[2] = make_double2(m.x - u.x, m.y - u.y);
+  } else {  // R == 5
+    static_assert(R == 5, "radix 2, 3, 4 or 5");
+    const double C1 = 0.30901699437494742410;   // cos(2 pi / 5) = (sqrt(5) - 1) / 4
+    const double C2 = -0.80901699437494742410;  // cos(4 pi / 5) = -(sqrt(5) + 1) / 4
+    const double S1 = 0.95105651629515357212;   // sin(2 pi / 5)
+    const double S2 = 0.58778525229247312917;   // sin(4 pi / 5)
+    const double2 a1 = make_double2(v[1].x + v[4].x, v[1].y + v[4].y);
+    const double2 a2 = make_double2(v[2].x + v[3].x, v[2].y + v[3].y);
+    const double2 b1 = make_double2(v[1].x - v[4].x, v[1].y - v[4].y);
+    const double2 b2 = make_double2(v[2].x - v[3].x, v[2].y - v[3].y);
+    const double2 p1 = make_double2(v[0].x + C1 * a1.x + C2 * a2.x, v[0].y + C1 * a1.y + C2 * a2.y);
+    const double2 p2 = make_double2(v[0].x + C2 * a1.x + C1 * a2.x, v[0].y + C2 * a1.y + C1 * a2.y);
+    const double2 q1 = times_si(make_double2(S1 * b1.x + S2 * b2.x, S1 * b1.y + S2 * b2.y), s);
+    const double2 q2 = times_si(make_double2(S2 * b1.x - S1 * b2.x, S2 * b1.y - S1 * b2.y), s);
+    v[0] = make_double2(v[0].x + a1.x + a2.x, v[0].y + a1.y + a2.y);
+    v[1] = make_double2(p1.x + q1.x, p1.y + q1.y);
+    v[4] = make_double2(p1.x - q1.x, p1.y - q1.y);
+    v[2] = make_double2(p2.x + q2.x, p2.y + q2.y);
+    v[3] = make_double2(p2.x - q2.x, p2.y - q2.y);
   }
-  for (int i = threadIdx.x; i < P; i += blockDim.x) row[i] = sm[i];
+}
+
+// One Stockham stage of radix R (registers only: R is a template constant).
+template <int R>
+__device__ __forceinline__ void fft_stage(const double2 *a, double2 *b, int P, int ns,
+                                          const double2 *__restrict__ tw, int inverse) {
+  const int m = P / R, step = P / (ns * R);
+  const double s = inverse ? 1.0 : -1.0;
+  for (int j = threadIdx.x; j < m; j += blockDim.x) {
+    const int k = j % ns;
+    double2 v[R];
+    v[0] = a[j];
+#pragma unroll
+    for (int r = 1; r < R; ++r) {
+      double2 w = tw[r * k * step];
+      if (inverse) w.y = -w.y;
+      v[r] = cmul_d2(a[j + r * m], w);
+    }
+    dft_small<R>(v, s);
+    const int d = (j / ns) * ns * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) b[d + r * ns] = v[r];
+  }
+}
+
+__global__ void __launch_bounds__(512) k_fft_rows(FftPlan plan, int P, const double2 *__restrict__ tw,
+                                                  double2 *data, int inverse) {
+  extern __shared__ double2 sm[];
+  double2 *a = sm, *b = sm + P;
+  double2 *row = data + (size_t)blockIdx.x * P;
+  for (int i = threadIdx.x; i < P; i += blockDim.x) a[i] = row[i];
+  __syncthreads();
+  int ns = 1;
+  for (int st = 0; st < plan.n_stages; ++st) {
+    const int R = plan.radix[st];
+    if (R == 4) fft_stage<4>(a, b, P, ns, tw, inverse);
+    else if (R == 2) fft_stage<2>(a, b, P, ns, tw, inverse);
+    else if (R == 3) fft_stage<3>(a, b, P, ns, tw, inverse);
+    else fft_stage<5>(a, b, P, ns, tw, inverse);
+    __syncthreads();
+    double2 *t = a;
+    a = b;
+    b = t;
+    ns *= R;
+  }
+  for (int i = threadIdx.x; i < P; i += blockDim.x) row[i] = a[i];
 }
 
 // out = transpose(in), P x P complex, 32 x 32 tiles.
@@ -1330,8 +1415,10 @@ struct sc_ctx {
   DevArray<double> scratch, scratch2, fg, gi;
   DevArray<double> partial_fin, partial_bg, partial_bgt, partial_vp, partial_acc;
   DevArray<double> pois_s;
-  // Poisson transform: side P = 2^fft_log2p, twiddles, kernel spectrum, work arrays (complex).
-  int fft_p = 0, fft_log2p = 0;
+  // Poisson transform: side P = 32 * 2^a 3^b 5^c (radix plan), twiddles,
+  // kernel spectrum, work arrays (complex).
+  int fft_p = 0;
+  FftPlan fft_plan{};
   DevArray<double> fft_tw, fft_kf, fft_z, fft_t;
   DevArray<double> acc_m;
   DevArray<AccState> acc_state;
@@ -1469,11 +1556,12 @@ void launch_sweep(sc_ctx *c, const Chunk &ch, int burn_in) {
   const unsigned blocks = grid1(threads, 128);
   launch_frame_fields<R>(c, ch, A);
   ProfScope prof(c, 0);
-  // Both precisions run best with four resident blocks per SM (measured on
-  // B200: FP64 four energies per thread; mixed two, 10.5 ms on C2 against
-  // 11.2 ms with five or six blocks).
+  // Resident blocks per SM, fastest measured on B200: FP64 three (four
+  // energies per thread, 158 registers, no spills: 35.4 ms on C2 against 36.3
+  // with four blocks), mixed four (two energies per thread: 10.5 ms against
+  // 11.2 with five or six blocks).
   static const char *minb_env = std::getenv("SCB_SWEEP_MINB");
-  const int variant = minb_env ? std::atoi(minb_env) : (sizeof(R) == 8 ? 4 : (c->emax2 ? 4 : 1));
+  const int variant = minb_env ? std::atoi(minb_env) : (sizeof(R) == 8 ? 3 : (c->emax2 ? 4 : 1));
   if (c->S.fs_tight_binding) {
     // Non-circular Fermi surface: per-angle step, generic mappings.
     if (c->S.keldysh) {
@@ -1492,10 +1580,12 @@ void launch_sweep(sc_ctx *c, const Chunk &ch, int burn_in) {
   } else if (c->ept <= 2 && c->emax2) {
     if (variant >= 6) k_sweep<R, 2, 6, false><<<blocks, 128, 0, c->stream>>>(A);
     else if (variant == 5) k_sweep<R, 2, 5, false><<<blocks, 128, 0, c->stream>>>(A);
+    else if (variant == 3) k_sweep<R, 2, 3, false><<<blocks, 128, 0, c->stream>>>(A);
     else k_sweep<R, 2, 4, false><<<blocks, 128, 0, c->stream>>>(A);
   } else if (c->ept <= 4) {
     if (variant == 4) k_sweep<R, 4, 4, false><<<blocks, 128, 0, c->stream>>>(A);
     else if (variant == 5) k_sweep<R, 4, 5, false><<<blocks, 128, 0, c->stream>>>(A);
+    else if (variant == 3) k_sweep<R, 4, 3, false><<<blocks, 128, 0, c->stream>>>(A);
     else k_sweep<R, 4, 1, false><<<blocks, 128, 0, c->stream>>>(A);
   } else if (c->ept <= 8) {
     k_sweep<R, 8, 1, false><<<blocks, 128, 0, c->stream>>>(A);
@@ -1573,16 +1663,16 @@ void launch_scalars_b(sc_ctx *c, int do_bc, int do_vp, int compute_mode, size_t 
 // zero, so the others are left as they are), and only the first rows_out rows
 // of the result are needed (the transpose and the last pass stop there).
 void fft2(sc_ctx *c, double2 *z, double2 *t, int inverse, int rows_in, int rows_out) {
-  const int P = c->fft_p, lg = c->fft_log2p;
+  const int P = c->fft_p;
   const int thr = std::min(P / 2, 512);
-  const size_t smem = (size_t)P * sizeof(double2);
+  const size_t smem = 2 * (size_t)P * sizeof(double2);
   const dim3 tb(32, 8), tg((rows_out + 31) / 32, P / 32);
   double2 *first = inverse ? t : z, *second = inverse ? z : t;
-  k_fft_rows<<<rows_in, thr, smem, c->stream>>>(lg, (const double2 *)c->fft_tw.p, first, inverse);
+  k_fft_rows<<<rows_in, thr, smem, c->stream>>>(c->fft_plan, P, (const double2 *)c->fft_tw.p, first, inverse);
   check_launch(c);
   k_fft_transpose<<<tg, tb, 0, c->stream>>>(P, first, second);
   check_launch(c);
-  k_fft_rows<<<rows_out, thr, smem, c->stream>>>(lg, (const double2 *)c->fft_tw.p, second, inverse);
+  k_fft_rows<<<rows_out, thr, smem, c->stream>>>(c->fft_plan, P, (const double2 *)c->fft_tw.p, second, inverse);
   check_launch(c);
 }
 
@@ -1618,16 +1708,30 @@ void poisson(sc_ctx *c, const double *j, double *a_out, int mean_from_scalars) {
 void poisson_setup(sc_ctx *c) {
   const HostSetup &S = c->S;
   const int n = S.n0;
-  int P = 1, lg = 0;
-  while (P < 2 * n - 1 || P < 32) {
-    P *= 2;
-    ++lg;
-  }
+  // The smallest side P >= 2 N0 - 1 of the form 32 * 2^a 3^b 5^c (a multiple
+  // of the 32-wide transpose tiles whose rows the mixed-radix FFT handles).
+  auto smooth = [](int m) {
+    for (int f : {2, 3, 5})
+      while (m % f == 0) m /= f;
+    return m == 1;
+  };
+  int m = 1;
+  while (32 * m < 2 * n - 1 || !smooth(m)) ++m;
+  const int P = 32 * m;
   if (P > 4096) throw EngineError(SC_ERR_ARG, "lattice too large for the Poisson transform (N0 > 2048)");
   c->fft_p = P;
-  c->fft_log2p = lg;
-  std::vector<double> tw(P);  // P/2 complex twiddles
-  for (int q = 0; q < P / 2; ++q) {
+  FftPlan plan{};
+  {
+    int r = P, twos = 0;
+    while (r % 2 == 0) r /= 2, ++twos;
+    for (int k = 0; k < twos / 2; ++k) plan.radix[plan.n_stages++] = 4;
+    if (twos % 2) plan.radix[plan.n_stages++] = 2;
+    while (r % 3 == 0) r /= 3, plan.radix[plan.n_stages++] = 3;
+    while (r % 5 == 0) r /= 5, plan.radix[plan.n_stages++] = 5;
+  }
+  c->fft_plan = plan;
+  std::vector<double> tw(2 * (size_t)P);  // exp(-2 pi i q / P), q < P
+  for (int q = 0; q < P; ++q) {
     const double ang = -2.0 * M_PI * (double)q / (double)P;
     tw[2 * q] = std::cos(ang);
     tw[2 * q + 1] = std::sin(ang);
@@ -1650,8 +1754,9 @@ void poisson_setup(sc_ctx *c) {
   c->fft_t.alloc(2 * pp);
   c->fft_kf.alloc(2 * pp);
   CUDA_TRY(cudaMemcpyAsync(c->fft_z.p, kr.data(), 2 * pp * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  if (P * sizeof(double2) > 48 * 1024)
-    CUDA_TRY(cudaFuncSetAttribute(k_fft_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(P * sizeof(double2))));
+  if (2 * P * sizeof(double2) > 48 * 1024)
+    CUDA_TRY(cudaFuncSetAttribute(k_fft_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(2 * P * sizeof(double2))));
   fft2(c, (double2 *)c->fft_z.p, (double2 *)c->fft_kf.p, 0, P, P);
   CUDA_TRY(cudaStreamSynchronize(c->stream));
 }
@@ -2068,7 +2173,7 @@ void upload_static(sc_ctx *c) {
   const char *eg = std::getenv("SCB_ENERGY_GROUPS");
   // Default (fastest measured on B200 for 7-14 Ozaki energies): FP64 the fewest
   // threads per column that keep at most four energies per thread; mixed
-  // precision at most two; four resident blocks per SM in both.
+  // precision at most two; three (FP64) or four (mixed) resident blocks per SM.
   const bool fp32_sweep = c->mode == SC_MODE_MIXED && !S.keldysh;
   const int per_thread = fp32_sweep ? 2 : 4;
   int want = 1;
@@ -2080,7 +2185,7 @@ void upload_static(sc_ctx *c) {
     int dev = 0, n_sm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-    const double resident = (double)n_sm * 4 * 128;
+    const double resident = (double)n_sm * (fp32_sweep ? 4 : 3) * 128;
     size_t max_items = 0;
     for (const Chunk &ch : c->chunks) max_items = std::max(max_items, (size_t)(ch.item_end - ch.item_begin));
     while ((double)max_items * want < 2.0 * resident && want < 8 && (S.ne + want - 1) / want > 1) want *= 2;
@@ -2883,6 +2988,7 @@ void launch_batch_sweep(sc_batch *b, sc_batch::Wave &w, int wi) {
     run(k_sweep_batch<R, 2, 4>);
   } else if (ept <= 4) {
     if (b->minb == 4) run(k_sweep_batch<R, 4, 4>);
+    else if (b->minb == 3) run(k_sweep_batch<R, 4, 3>);
     else run(k_sweep_batch<R, 4, 1>);
   } else if (ept <= 8) {
     run(k_sweep_batch<R, 8, 1>);
@@ -3171,7 +3277,7 @@ int sc_batch_set_graph(sc_batch *b, int enable) {
 
 int sc_batch_config(sc_batch *b, int energies_per_thread, int minb) {
   const int e = energies_per_thread;
-  if (!b || !(e == 1 || e == 2 || e == 4 || e == 8 || e == 16) || (minb != 1 && minb != 4 && minb != 6))
+  if (!b || !(e == 1 || e == 2 || e == 4 || e == 8 || e == 16) || (minb != 1 && minb != 3 && minb != 4 && minb != 6))
     return SC_ERR_ARG;
   int ne_max = 1;
   for (sc_ctx *c : b->grains) ne_max = std::max(ne_max, c->S.ne);
@@ -3245,7 +3351,7 @@ extern "C" {
 // keeps the fastest and returns it.
 int sc_batch_autotune(sc_batch *b, int *energies_per_thread, int *minb, double *best_ms) {
   if (!b) return SC_ERR_ARG;
-  const int cand[][2] = {{1, 4}, {2, 4}, {2, 6}, {4, 4}, {4, 1}, {8, 1}};
+  const int cand[][2] = {{1, 4}, {2, 4}, {2, 6}, {4, 3}, {4, 4}, {4, 1}, {8, 1}};
   int best_e = b->ept_max, best_mb = b->minb;
   double best = 1e300;
   for (const auto &cd : cand) {
