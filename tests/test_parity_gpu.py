@@ -133,6 +133,27 @@ def test_poisson(engine_lib):
     assert _rel(e.poisson(j), o.poisson(j)) < 1e-10
 
 
+@pytest.mark.parametrize("which", ["disc_n71", "c1_n206"])
+def test_poisson_mixed_radix(engine_lib, which):
+    """The FFT Poisson solve on transform sides with radix-5 and radix-3 stages
+    (N0 = 71: P = 160 = 4*4*2*5; C1, N0 = 206: P = 480 = 4*4*2*3*5) against
+    the oracle's direct sums of the separable filters."""
+    import copy
+    from oracle import oracle as O
+    import superconga_b200 as sb
+    from superconga_b200 import workloads
+    if which == "disc_n71":
+        cfg = copy.deepcopy(configs.small_disc())
+        cfg["geometry"][0]["disc"]["radius"] = 6.5
+    else:
+        cfg = workloads.c1()
+    o = O.Oracle(cfg)
+    e = sb.Context(cfg)
+    rng = np.random.default_rng(11)
+    j = rng.standard_normal((2, o.n0, o.n0)) * (o.domain() > 0)
+    assert _rel(e.poisson(j), o.poisson(j)) < 1e-10
+
+
 @pytest.mark.parametrize("acc", ["congacc", "picard", "polyak", "barzilai-borwein"])
 def test_golden_free_energy(engine_lib, acc):
     """tests/accelerators_test.cu:45-149 on the engine: converged within 100
