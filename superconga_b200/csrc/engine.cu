@@ -4,8 +4,10 @@
 // One iteration (Context::compute, include/conga/Context.h:391-447) is a short
 // sequence of launches on the context's stream:
 //   accelerate        x <- F(x, g(x))                      (iterations >= 2)
-//   extend_reference  order parameter extended past the grain (domain_ops.h)
+//   extend_reference  order parameter extended past the grain (domain_ops.h),
+//                     packed with A into one record per reference site
 //   per angle chunk:
+//     frame_fields    order parameter and Doppler shift along every column
 //     sweep           gammaTilde down every trajectory column (stored), gamma up,
 //                     Green sums over the Ozaki energies -> frame buffers;
 //                     outgoing boundary values written in sparse order
@@ -14,7 +16,8 @@
 //   finalize          Delta, j, free energy, residuals (ComputeOrderParameter.h,
 //                     ComputeCurrent.h, ComputeFreeEnergy.h)
 //   boundary          specular reflection through precomputed gather tables
-//   poisson           separable Toeplitz filters (ComputeVectorPotential.h)
+//   poisson           the separable filters (ComputeVectorPotential.h) as one
+//                     2D FFT convolution
 // All static data (geometry in every frame, sparse indices, gather tables) is
 // built once by setup.cpp and stays resident in HBM.
 #include <cuda_runtime.h>
@@ -898,7 +901,7 @@ __global__ void k_subtract_mean(int n0, const double *__restrict__ j, const doub
 // with s = j - <j> and the translation-invariant kernel
 // K(u, v) = -h^2 scale * sum_k (+/-) f_k(u) f_k(v) built from the separable
 // filters (ComputeVectorPotential.h:212-416).  It is evaluated as one linear
-// convolution by zero-padded 2D FFTs of side P >= 2 N0 - 1 (a power of two):
+// convolution by zero-padded 2D FFTs of side P >= 2 N0 - 1 (P = 32 * 2^a 3^b 5^c):
 // both current components travel in one complex array, s_x + i s_y, the
 // kernel's spectrum is computed once at set-up.  O(P^2 log P) instead of
 // O(K N0^3); the results agree with the direct filter sums to rounding.
@@ -1556,10 +1559,10 @@ void launch_sweep(sc_ctx *c, const Chunk &ch, int burn_in) {
   const unsigned blocks = grid1(threads, 128);
   launch_frame_fields<R>(c, ch, A);
   ProfScope prof(c, 0);
-  // Resident blocks per SM, fastest measured on B200: FP64 three (four
-  // energies per thread, 158 registers, no spills: 35.4 ms on C2 against 36.3
-  // with four blocks), mixed four (two energies per thread: 10.5 ms against
-  // 11.2 with five or six blocks).
+  // Resident blocks per SM, fastest measured on B200 (606 x 606 d-wave square,
+  // 256 angles, 14 energies): FP64 three (four energies per thread, 158
+  // registers, no spills: 35.4 ms against 36.3 with four blocks), mixed four
+  // (two energies per thread: 10.5 ms against 11.2 with five or six blocks).
   static const char *minb_env = std::getenv("SCB_SWEEP_MINB");
   const int variant = minb_env ? std::atoi(minb_env) : (sizeof(R) == 8 ? 3 : (c->emax2 ? 4 : 1));
   if (c->S.fs_tight_binding) {
