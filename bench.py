@@ -224,7 +224,7 @@ def _time_context(ctx, stream, steps, warmup, world):
 
 def _e2e(ctx, steps, world):
     """Same metric through the public API with host buffers: every step the
-    host sends x (pinned memory) and reads x back."""
+    host sends x from pinned memory and reads x back into it."""
     import torch
     n0, nc = ctx.dims.n0, ctx.dims.n_comp
     host_d = torch.empty((nc, 2, n0, n0), dtype=torch.float64, pin_memory=True).numpy()
@@ -239,9 +239,7 @@ def _e2e(ctx, steps, world):
     for _ in range(steps):
         ctx.set_state(host_d, host_a)
         ctx.compute(1)
-        xd, xa = ctx.state()
-        host_d[...] = xd
-        host_a[...] = xa
+        ctx.state(host_d, host_a)
     torch.cuda.synchronize()
     sec = time.perf_counter() - t0
     sec = max_over_ranks(sec, world)

@@ -82,9 +82,15 @@ class Context:
         a = None if a_internal is None else np.ascontiguousarray(a_internal, np.float64).reshape(self._shape_vec())
         self._check(_lib.load().sc_set_state(self._h, _p(d), _p(a) if a is not None else None))
 
-    def state(self):
-        d = np.zeros(self._shape_delta())
-        a = np.zeros(self._shape_vec())
+    def state(self, delta_out: np.ndarray | None = None, a_out: np.ndarray | None = None):
+        """x as (order parameter, vector potential); into the caller's arrays
+        (C-contiguous float64 of the right shapes, e.g. pinned host memory)
+        when given, without an intermediate copy."""
+        d = np.zeros(self._shape_delta()) if delta_out is None else delta_out
+        a = np.zeros(self._shape_vec()) if a_out is None else a_out
+        for arr, shape in ((d, self._shape_delta()), (a, self._shape_vec())):
+            if arr.dtype != np.float64 or not arr.flags["C_CONTIGUOUS"] or arr.size != int(np.prod(shape)):
+                raise ValueError("state(): output arrays must be C-contiguous float64 of the state's shape")
         self._check(_lib.load().sc_get_state(self._h, _p(d), _p(a)))
         return d, a
 

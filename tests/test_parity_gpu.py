@@ -111,6 +111,22 @@ def test_iterations(engine_lib, case):
             assert _rel(e.boundary(which), o.boundary(which)) < TOL, (it, which)
 
 
+def test_state_into_caller_buffers(engine_lib):
+    """Context.state writes into the caller's (pinned) arrays and rejects
+    arrays of the wrong type or size."""
+    import torch
+    cfg, kw = CASES["small_disc"]
+    o, e, _ = _pair(cfg, **kw)
+    e.compute(1)
+    d_ref, a_ref = e.state()
+    d = torch.empty(d_ref.shape, dtype=torch.float64, pin_memory=True).numpy()
+    a = torch.empty(a_ref.shape, dtype=torch.float64, pin_memory=True).numpy()
+    e.state(d, a)
+    assert np.array_equal(d, d_ref) and np.array_equal(a, a_ref)
+    with pytest.raises(ValueError):
+        e.state(np.zeros(d_ref.shape, np.float32), a)
+
+
 def test_burn_in(engine_lib):
     cfg, kw = CASES["small_disc"]
     o, e, _ = _pair(cfg, **kw)
