@@ -1190,13 +1190,112 @@ __global__ void __launch_bounds__(REDUCE_THREADS) k_acc_sums(int nf, size_t nn, 
   block_reduce(q, 3, 0, partial + ((size_t)f * gridDim.x + blockIdx.x) * 3);
 }
 
+constexpr int AND_MAX_RANK = 16;
 struct AccState {
   double step[16];
   double inertia[16];
   double bb_step;
   int bb_iter;
   int initialized;
+  // Anderson: iterations taken, the stored residuals' squared norms and
+  // pairwise dot products (a stored pair does not change until its slot is
+  // reused), and the weights of the current step.
+  int and_iter;
+  double and_sq[AND_MAX_RANK];
+  double and_dot[AND_MAX_RANK][AND_MAX_RANK];
+  double and_w[AND_MAX_RANK];
 };
+
+// Anderson::set (Anderson.h:267-289): the iterate and its residual
+// d = g(x) - x go to slot iter mod rank (the oldest once all are used), and
+// the block partials of |d|^2 and of d . D_j with the other stored residuals.
+__global__ void __launch_bounds__(REDUCE_THREADS) k_and_store(size_t tot, int rank, const double *__restrict__ x,
+                                                              const double *__restrict__ gx, double *hx,
+                                                              double *hd, const AccState *st, double *partial) {
+  const int it = st->and_iter, slot = it % rank, m = min(it + 1, rank);
+  double q[AND_MAX_RANK];
+  for (int j = 0; j < rank; ++j) q[j] = 0.0;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < tot; k += (size_t)gridDim.x * blockDim.x) {
+    const double d = gx[k] - x[k];
+    hx[(size_t)slot * tot + k] = x[k];
+    hd[(size_t)slot * tot + k] = d;
+    for (int j = 0; j < m; ++j) q[j] += d * (j == slot ? d : hd[(size_t)j * tot + k]);
+  }
+  block_reduce(q, rank, 0, partial + (size_t)blockIdx.x * rank);
+}
+
+// Anderson::solve (Anderson.h:291-333): the bordered least-squares system
+// [A 1; 1 0] [w; l] = [0; 1] with A_ij = D_i . D_j / mean |D|^2, solved by
+// Gaussian elimination with partial pivoting; then the iteration count.
+__global__ void k_and_solve(int rank, const double *partial, int nblocks, AccState *st) {
+  __shared__ double t[AND_MAX_RANK];
+  reduce_slots(partial, nblocks, rank, 0ull, t);
+  if (threadIdx.x != 0) return;
+  const int it = st->and_iter, slot = it % rank, m = min(it + 1, rank), mt = m + 1;
+  for (int j = 0; j < m; ++j) {
+    if (j == slot) continue;
+    st->and_dot[slot][j] = t[j];
+    st->and_dot[j][slot] = t[j];
+  }
+  st->and_sq[slot] = t[slot];
+  double sr = 0.0;
+  for (int i = 0; i < m; ++i) sr += st->and_sq[i];
+  const double scale = 1.0 / (sr / (double)m);
+  double M[AND_MAX_RANK + 1][AND_MAX_RANK + 1], rhs[AND_MAX_RANK + 1];
+  for (int i = 0; i < mt; ++i) {
+    rhs[i] = (i == mt - 1) ? 1.0 : 0.0;
+    for (int j = 0; j < mt; ++j) M[i][j] = 1.0;
+  }
+  for (int i = 0; i < m; ++i) {
+    M[i][i] = st->and_sq[i] * scale;
+    for (int j = i + 1; j < m; ++j) {
+      const double v = st->and_dot[i][j] * scale;
+      M[i][j] = v;
+      M[j][i] = v;
+    }
+  }
+  M[mt - 1][mt - 1] = 0.0;
+  for (int col = 0; col < mt; ++col) {
+    int piv = col;
+    for (int r = col + 1; r < mt; ++r)
+      if (fabs(M[r][col]) > fabs(M[piv][col])) piv = r;
+    if (piv != col) {
+      for (int cc = 0; cc < mt; ++cc) {
+        const double tmp = M[col][cc];
+        M[col][cc] = M[piv][cc];
+        M[piv][cc] = tmp;
+      }
+      const double tmp = rhs[col];
+      rhs[col] = rhs[piv];
+      rhs[piv] = tmp;
+    }
+    const double dg = M[col][col];
+    for (int r = col + 1; r < mt; ++r) {
+      const double f = M[r][col] / dg;
+      for (int cc = col; cc < mt; ++cc) M[r][cc] -= f * M[col][cc];
+      rhs[r] -= f * rhs[col];
+    }
+  }
+  double w[AND_MAX_RANK + 1];
+  for (int r = mt - 1; r >= 0; --r) {
+    double v = rhs[r];
+    for (int cc = r + 1; cc < mt; ++cc) v -= M[r][cc] * w[cc];
+    w[r] = v / M[r][r];
+  }
+  for (int i = 0; i < AND_MAX_RANK; ++i) st->and_w[i] = i < m ? w[i] : 0.0;
+  st->and_iter = it + 1;
+}
+
+// Anderson::computeInternal (Anderson.h:336-355): x = sum_i w_i (X_i + step D_i).
+__global__ void k_and_update(size_t tot, int rank, double step, const double *__restrict__ hx,
+                             const double *__restrict__ hd, const AccState *st, double *x) {
+  const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (k >= tot) return;
+  const int m = min(st->and_iter, rank);  // already counts this iteration
+  double v = 0.0;
+  for (int i = 0; i < m; ++i) v += (hx[(size_t)i * tot + k] + hd[(size_t)i * tot + k] * step) * st->and_w[i];
+  x[k] = v;
+}
 
 // CongAcc::computeInertia (CongAcc.h:300-356).
 __device__ double congacc_inertia(double dn, double mn, double dot, double mincos) {
@@ -1424,6 +1523,7 @@ struct sc_ctx {
   FftPlan fft_plan{};
   DevArray<double> fft_tw, fft_kf, fft_z, fft_t;
   DevArray<double> acc_m;
+  DevArray<double> and_x, and_d;  // Anderson history [rank][fields][N0*N0] (iterates, residuals)
   DevArray<AccState> acc_state;
   DevArray<Scalars> scalars;
   DevArray<double> tmp_io;
@@ -1776,6 +1876,19 @@ void accelerate(sc_ctx *c) {
   C.smin = S.acc.step_size_min;
   C.drag = S.acc.drag;
   const size_t nn = c->nn0();
+  if (C.kind == ACC_ANDERSON) {
+    const size_t tot = (size_t)C.nf * nn;
+    const int rank = S.acc.rank;
+    k_and_store<<<c->nb_acc, REDUCE_THREADS, 0, c->stream>>>(tot, rank, c->xstate.p, c->gstate.p, c->and_x.p,
+                                                             c->and_d.p, c->acc_state.p, c->partial_acc.p);
+    check_launch(c);
+    k_and_solve<<<1, 256, 0, c->stream>>>(rank, c->partial_acc.p, c->nb_acc, c->acc_state.p);
+    check_launch(c);
+    k_and_update<<<grid1(tot, 256), 256, 0, c->stream>>>(tot, rank, C.step_size, c->and_x.p, c->and_d.p,
+                                                         c->acc_state.p, c->xstate.p);
+    check_launch(c);
+    return;
+  }
   if (C.kind == ACC_CONGACC || C.kind == ACC_BB) {
     dim3 grid(c->nb_acc, C.nf);
     k_acc_sums<<<grid, REDUCE_THREADS, 0, c->stream>>>(C.nf, nn, c->xstate.p, c->gstate.p, c->acc_m.p,
@@ -2270,6 +2383,11 @@ void upload_static(sc_ctx *c) {
   }
   c->acc_m.alloc((size_t)std::max(nf, 1) * nn);
   c->acc_m.zero(s);
+  if (S.acc.kind == ACC_ANDERSON) {
+    if (S.acc.rank < 1 || S.acc.rank > AND_MAX_RANK) throw EngineError(SC_ERR_ARG, "Anderson rank must be 1..16");
+    c->and_x.alloc((size_t)S.acc.rank * nf * nn);
+    c->and_d.alloc((size_t)S.acc.rank * nf * nn);
+  }
   c->acc_state.alloc(1);
   c->acc_state.zero(s);
   c->scalars.alloc(1);
@@ -2325,8 +2443,6 @@ int create_context(int mode, sc_ctx **out, F make) {
       throw EngineError(SC_ERR_ARG, c->S.keldysh ? "at most 64 energies per LDOS block"
                                                  : "at most 64 Ozaki energies (raise the temperature or lower the cutoff)");
     if (2 * c->S.nc + 2 > 16) throw EngineError(SC_ERR_ARG, "too many accelerator fields");
-    if (!c->S.keldysh && c->S.acc.kind == ACC_ANDERSON)
-      throw EngineError(SC_ERR_ARG, "accelerator 'anderson' is not available in this engine");
     CUDA_TRY(cudaGetDevice(&c->device));
     CUDA_TRY(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
     c->stream = c->own_stream;
@@ -3173,8 +3289,6 @@ int sc_batch_create(const char *const *configs, int n, int mode, sc_batch **out)
       if (!e.empty()) throw EngineError(SC_ERR_ARG, "grain " + std::to_string(i) + ": " + e);
       if (c->S.nc > MAX_COMP) throw EngineError(SC_ERR_ARG, "at most 4 order-parameter components");
       if (c->S.ne > 32) throw EngineError(SC_ERR_ARG, "grain " + std::to_string(i) + ": at most 32 Ozaki energies in a batch");
-      if (c->S.acc.kind == ACC_ANDERSON)
-        throw EngineError(SC_ERR_ARG, "accelerator 'anderson' is not available in this engine");
       c->device = dev;
       c->stream = b->stream;
       upload_static(c);

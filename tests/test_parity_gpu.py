@@ -170,7 +170,23 @@ def test_poisson_mixed_radix(engine_lib, which):
     assert _rel(e.poisson(j), o.poisson(j)) < 1e-10
 
 
-@pytest.mark.parametrize("acc", ["congacc", "picard", "polyak", "barzilai-borwein"])
+@pytest.mark.parametrize("case", ["small_disc", "small_square_d"])
+def test_anderson_iterations(engine_lib, case):
+    """The Anderson accelerator (Anderson.h:201-355) on the GPU against the
+    oracle over six iterations, so that its history fills (rank 4) and the
+    oldest slot is reused: x, g(x) and the free energy within 1e-10."""
+    cfg, kw = CASES[case]
+    o, e, _ = _pair(configs.with_accelerator(cfg, "anderson"), **kw)
+    for it in range(6):
+        o.compute()
+        e.compute(1)
+        assert _rel(e.state()[0], o.state()[0]) < TOL, (it, "x")
+        assert _rel(e.results()[0], o.results()[0]) < TOL, (it, "delta")
+        fo, fe = o.scalars()["free_energy"], e.scalars()["free_energy"]
+        assert abs(fe - fo) <= TOL * abs(fo), it
+
+
+@pytest.mark.parametrize("acc", ["congacc", "picard", "polyak", "barzilai-borwein", "anderson"])
 def test_golden_free_energy(engine_lib, acc):
     """tests/accelerators_test.cu:45-149 on the engine: converged within 100
     iterations to Omega/area = -0.0185386592 within 1e-3 relative."""
