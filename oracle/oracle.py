@@ -387,8 +387,11 @@ class Setup:
         return int(self.params.n_energies) if self.params is not None else len(self.poles)
 
 
-def make_setup(cfg: dict) -> Setup:
-    """Mirror of src/simulation.cu:90-463 (everything up to context.initialize)."""
+def make_setup(cfg: dict, component_order: list | None = None) -> Setup:
+    """Mirror of src/simulation.cu:90-463 (everything up to context.initialize).
+    component_order: the order-parameter components in another order than the
+    driver's (dx2-y2, dxy, g, s), as a C++ caller of OrderParameter::add may
+    add them."""
     phys, num = cfg["physics"], cfg["numerics"]
     temperature = float(phys["temperature"])
     ppxi = float(num["points_per_coherence_length"])
@@ -402,6 +405,10 @@ def make_setup(cfg: dict) -> Setup:
     geom = geometry_components(cfg, scaling, xo, yo, gf)
     ops = phys["order_parameter"]
     syms = [s for s in SYMMETRIES if s in ops]
+    if component_order is not None:
+        if sorted(component_order) != sorted(syms):
+            raise ValueError("component_order must list the configured components")
+        syms = list(component_order)
     if not syms:
         raise ValueError("no order-parameter component")
     tcs = [float(ops[s].get("critical_temperature", 1.0)) for s in syms]
@@ -460,12 +467,14 @@ def make_setup(cfg: dict) -> Setup:
 class Oracle:
     """One self-consistency context on the CPU (mirror of conga::Context)."""
 
-    def __init__(self, cfg: dict | str, energies: tuple | None = None):
+    def __init__(self, cfg: dict | str, energies: tuple | None = None,
+                 component_order: list | None = None):
         """energies: optional (imaginary parts, residues) replacing the Ozaki
-        set (the LDOS path sweeps real energies with a common broadening)."""
+        set (the LDOS path sweeps real energies with a common broadening);
+        component_order: see make_setup."""
         if isinstance(cfg, str):
             cfg = json.loads(cfg)
-        self.setup = s = make_setup(cfg)
+        self.setup = s = make_setup(cfg, component_order)
         e_im, e_res = s.energies_im, s.residues
         if energies is not None:
             e_im, e_res = (np.ascontiguousarray(v, np.float64) for v in energies)

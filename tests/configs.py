@@ -83,6 +83,52 @@ def chiral_annulus() -> dict:
     }
 
 
+def swave_disc_field() -> dict:
+    """tests/physics/swave_disc_test.cu:66-150: s-wave disc R = 20 xi0 at 2.7
+    points/xi0, 16 angles, T = 0.2, cutoff 16, five flux quanta, lambda = 5,
+    symmetric gauge, L-infinity residuals, criterion 1e-3, Barzilai-Borwein,
+    bulk start."""
+    r = 20.0
+    return {
+        "physics": {"temperature": 0.2, "external_flux_quanta": 5.0, "penetration_depth": 5.0,
+                    "charge_sign": -1, "gauge": "symmetric", "crystal_axes_rotation": 0.0,
+                    "order_parameter": {"s": {"critical_temperature": 1.0}}},
+        "geometry": [{"disc": {"add": True, "radius": r, "center_x": 0.0, "center_y": 0.0}}],
+        "numerics": {"points_per_coherence_length": 2.7, "num_fermi_momenta": 16,
+                     "energy_cutoff": 16.0, "convergence_criterion": 1e-3, "norm": "linf",
+                     "vector_potential_error": 1e-6},
+        "accelerator": {"name": "barzilai-borwein"},
+    }
+
+
+def swave_disc_free_energy(temperature: float, cutoff: float, lam: float, flux_quanta: float,
+                           radius: float, delta: float) -> float:
+    """Analytic free energy per area of a field-penetrated s-wave disc without
+    phase winding (tests/physics/swave_disc_test.cu:18-57): the bulk free
+    energy (OrderParameterBulk.h:225-246) plus the London magnetic and kinetic
+    terms with the Yoshida-renormalised penetration depth (:256-277) and the
+    modified Bessel functions I0, I1."""
+    from scipy.special import iv
+    n = int(cutoff / temperature - 0.5) + 1
+    esum, ysum = 0.0, 0.0
+    for k in range(n - 1, -1, -1):
+        e = temperature * (k + 0.5)
+        om = math.hypot(delta, e)
+        esum += 1.0 / e - 2.0 / (e + om)
+        ysum += 1.0 / om ** 3
+    f_bulk = delta * delta * (math.log(temperature) + temperature * esum)
+    yoshida = temperature * delta * delta * ysum
+    kk = lam / math.sqrt(yoshida)
+    area = math.pi * radius * radius
+    b = math.pi * flux_quanta / area
+    factor = 2.0 * math.pi * yoshida * (kk * b) ** 2 / (2.0 * area)
+    i0, i1 = iv(0, radius / kk), iv(1, radius / kk)
+    tmp = radius * i1 / i0
+    f_mag = factor * (radius * radius - 2.0 * kk * tmp - 0.5 * tmp * tmp)
+    f_kin = factor * 0.5 * radius * (-radius * i0 * i0 + 2 * kk * i0 * i1 + radius * i1 * i1) / (i0 * i0)
+    return f_bulk + f_kin + f_mag
+
+
 def with_accelerator(cfg: dict, name: str) -> dict:
     c = copy.deepcopy(cfg)
     c["accelerator"] = {"name": name}

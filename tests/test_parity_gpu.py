@@ -204,6 +204,27 @@ def test_golden_free_energy(engine_lib, acc):
     assert abs(fe - configs.GOLDEN_FREE_ENERGY_PER_AREA) <= 1e-3 * abs(configs.GOLDEN_FREE_ENERGY_PER_AREA)
 
 
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+def test_swave_disc_analytic_free_energy(engine_lib, mode):
+    """tests/physics/swave_disc_test.cu:66-174 on the engine: converged within
+    100 iterations, free energy per area within 1e-3 of the London value."""
+    from oracle import oracle as O
+    import superconga_b200 as sb
+    cfg = configs.swave_disc_field()
+    e = sb.Context(cfg, mode=mode)
+    n0 = e.dims.n0
+    db = O.delta_bulk(0.2, "s")
+    d = np.zeros((1, 2, n0, n0))
+    d[0, 0] = db
+    e.set_state(d, np.zeros((2, n0, n0)))
+    it, conv = e.run(0, 100)
+    expected = configs.swave_disc_free_energy(0.2, 16.0, 5.0, 5.0, 20.0, db)
+    fe = e.scalars()["free_energy_per_area"]
+    assert conv
+    assert abs(fe - expected) <= 1e-3 * abs(expected), (fe, expected)
+    e.close()
+
+
 def test_mixed_precision(engine_lib):
     """FP32 stepping with FP64 accumulation against the FP64 form after five
     iterations: |Delta - Delta_FP64| / Delta_bulk <= 1e-5."""

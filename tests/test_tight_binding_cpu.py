@@ -130,6 +130,26 @@ def test_engine_circle_tables():
     assert s["origin"] == (0.0, 0.0)
 
 
+@pytest.mark.parametrize("n", [7, 9, 11, 12])
+def test_engine_circle_matches_reference_tests(n):
+    # tests/fermi_surface_circle_test.cu:70-192 on the engine's tables: system
+    # angle phi - pi/2 on the uniform grid offset by pi/2, unit momentum and
+    # velocity along phi, positive integrand factors summing to 1 (10 eps).
+    from superconga_b200.engine import Setup
+    cfg = configs.small_disc()
+    cfg["numerics"]["num_fermi_momenta"] = n
+    s = Setup(cfg).fermi_surface()
+    for k in range(n):
+        ang = 2.0 * math.pi / n * k + 0.5 * math.pi
+        sys_expected = math.fmod(ang - 0.5 * math.pi + 4 * math.pi, 2 * math.pi)
+        assert math.fmod(s["theta"][k] + 4 * math.pi, 2 * math.pi) == pytest.approx(sys_expected, rel=10 * EPS, abs=10 * EPS)
+        assert s["px"][k] == pytest.approx(math.cos(ang), abs=10 * EPS)
+        assert s["py"][k] == pytest.approx(math.sin(ang), abs=10 * EPS)
+        assert math.hypot(s["vx"][k], s["vy"][k]) == pytest.approx(1.0, rel=10 * EPS)
+    assert np.all(s["weight"] > 0.0)
+    assert s["weight"].sum() == pytest.approx(1.0, rel=10 * EPS)
+
+
 def test_unknown_fermi_surface_rejected():
     from superconga_b200 import _lib
     from superconga_b200.engine import Setup
