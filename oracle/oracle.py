@@ -255,12 +255,15 @@ def geometry_components(cfg: dict, scaling: float, xo: float, yo: float, gf: flo
     return types, adds, nverts, data
 
 
-def poisson_filters(n0: int, h: float, max_error: float):
+def poisson_filters(n0: int, h: float, max_error: float, analytical: bool = True):
     """ComputeVectorPotential::makeFilter2D / initializeFilters / addFilter1D.
 
-    include/conga/compute/ComputeVectorPotential.h:212-416 with the analytical
-    matrix elements (the driver's default, ComputeVectorPotential.h:153-156).
-    Returns (filters [K, 2*n0-1], positive flags [K], scale).
+    include/conga/compute/ComputeVectorPotential.h:212-416, by default with the
+    analytical matrix elements (the driver's default,
+    ComputeVectorPotential.h:153-156); analytical=False takes the point values
+    2 log|r| and the origin value pi/2 - log 2 - 3 (:269-282) as the reference's
+    legacy comparison does.  Returns (filters [K, 2*n0-1], positive flags [K],
+    scale).
     """
     i = np.arange(n0, dtype=np.float64)
     I, J = np.meshgrid(i, i, indexing="ij")
@@ -273,17 +276,22 @@ def poisson_filters(n0: int, h: float, max_error: float):
         fac = 0.5 * ((2.0 - a + b) * (a + b) - 2.0)
         return fac * np.arctan(a / b)
 
-    Q = np.zeros((n0, n0))
-    for jsgn in (-1.0, 1.0):
-        b = 1.0 + 2.0 * (jsgn * J)
-        for isgn in (-1.0, 1.0):
-            a = 1.0 + 2.0 * (isgn * I)
-            Q += alpha(a, b) + beta(a, b) + beta(b, a)
-    Q *= 0.25
+    if analytical:
+        Q = np.zeros((n0, n0))
+        for jsgn in (-1.0, 1.0):
+            b = 1.0 + 2.0 * (jsgn * J)
+            for isgn in (-1.0, 1.0):
+                a = 1.0 + 2.0 * (isgn * I)
+                Q += alpha(a, b) + beta(a, b) + beta(b, a)
+        Q *= 0.25
+    else:
+        with np.errstate(divide="ignore"):
+            Q = 2.0 * np.log(np.hypot(I, J))
+        Q[0, 0] = 0.5 * math.pi - math.log(2.0) - 3.0
     Q = 0.5 * (Q + Q.T)
     scale = 1.0 / (4.0 * math.pi)
     Q *= scale
-    const = (2.0 * math.log(h) - math.log(2.0) - 3.0) * scale
+    const = ((2.0 * math.log(h) - math.log(2.0) - 3.0) if analytical else 2.0 * math.log(h)) * scale
     meanQ = Q.mean()
     Q -= meanQ
     const += meanQ
