@@ -129,6 +129,55 @@ def swave_disc_free_energy(temperature: float, cutoff: float, lam: float, flux_q
     return f_bulk + f_kin + f_mag
 
 
+def disc_n256() -> dict:
+    """A disc whose lattice is N0 = 256 at 10 points/xi0 (spacing 0.1), the
+    size of tests/physics/vector_potential_test.cu; four angles (only the
+    Poisson solve is used)."""
+    r = 12.475
+    return {
+        "physics": {"temperature": 0.5, "external_flux_quanta": 0.0, "penetration_depth": 2.0,
+                    "charge_sign": -1, "gauge": "symmetric", "crystal_axes_rotation": 0.0,
+                    "order_parameter": {"s": {"critical_temperature": 1.0}}},
+        "geometry": [{"disc": {"add": True, "radius": r, "center_x": 0.0, "center_y": 0.0}}],
+        "numerics": {"points_per_coherence_length": 10.0, "num_fermi_momenta": 4,
+                     "energy_cutoff": 8.0, "convergence_criterion": 1e-6, "norm": "l2",
+                     "vector_potential_error": 1e-6},
+    }
+
+
+def rotating_disc_current(n: int, h: float):
+    """tests/physics/vector_potential_test.cu:130-176: j = (-y, x) inside the
+    disc of radius R = 0.4 h (n - 1) about the lattice centre, and the
+    magnetostatic vector potential it induces, A = f(r) (-y, x) with
+    f = (2 R^2 - r^2) / 8 inside and R^4 / (8 r^2) outside."""
+    c = 0.5 * (n - 1)
+    R = h * (n - 1) * 0.4
+    y, x = np.meshgrid(h * (np.arange(n) - c), h * (np.arange(n) - c), indexing="ij")
+    r2 = x * x + y * y
+    inside = np.sqrt(r2) <= R
+    j = np.stack([np.where(inside, -y, 0.0), np.where(inside, x, 0.0)])
+    with np.errstate(divide="ignore", invalid="ignore"):
+        f = np.where(inside, 0.125 * (2.0 * R * R - r2), 0.125 * R ** 4 / r2)
+    return j, np.stack([-f * y, f * x])
+
+
+def vector_potential_symmetry_error(a: np.ndarray) -> float:
+    """Largest violation of the 90/180/270-degree rotation and transposition
+    symmetries that tests/physics/vector_potential_test.cu:56-89 requires of
+    the disc's vector potential, in doctest's Approx measure
+    |u - v| / (1 + max(|u|, |v|))."""
+    X, Y = a
+    n = X.shape[0]
+    J, I = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    def d(u, v):
+        return np.max(np.abs(u - v) / (1.0 + np.maximum(np.abs(u), np.abs(v))))
+    errs = [d(-Y, X[I, n - 1 - J]), d(X, Y[I, n - 1 - J]),
+            d(-X, X[n - 1 - J, n - 1 - I]), d(-Y, Y[n - 1 - J, n - 1 - I]),
+            d(Y, X[n - 1 - I, J]), d(-X, Y[n - 1 - I, J]),
+            d(np.hypot(X, Y), np.hypot(X[I, J], Y[I, J]))]
+    return float(max(errs))
+
+
 def with_accelerator(cfg: dict, name: str) -> dict:
     c = copy.deepcopy(cfg)
     c["accelerator"] = {"name": name}

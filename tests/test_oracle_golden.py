@@ -234,6 +234,20 @@ def test_poisson_filters_match_legacy_sum(O, current):
     assert np.abs(a - ref).max() / np.abs(ref).max() < tol
 
 
+def test_poisson_magnetostatics_disc(O):
+    """tests/physics/vector_potential_test.cu:238-245 (analytical elements,
+    error 1e-6, double): the solve of a rotating disc current on a 256 x 256
+    lattice of spacing 0.1 is within 2e-4 (relative Frobenius norm) of the
+    magnetostatic solution and has its rotation symmetries to 1e-8."""
+    o = O.Oracle(configs.disc_n256())
+    assert o.n0 == 256
+    j, expected = configs.rotating_disc_current(256, 0.1)
+    a = o.poisson(j)
+    frob = math.sqrt(np.sum((a - expected) ** 2) / np.sum(expected ** 2))
+    assert frob < 2e-4, frob
+    assert configs.vector_potential_symmetry_error(a) < 1e-8
+
+
 def test_poisson_linearity(O):
     """The separable Poisson solve is linear in the current
     (ComputeVectorPotential.h:575-745)."""

@@ -186,6 +186,25 @@ def test_anderson_iterations(engine_lib, case):
         assert abs(fe - fo) <= TOL * abs(fo), it
 
 
+def test_poisson_magnetostatics_disc(engine_lib):
+    """tests/physics/vector_potential_test.cu:238-245 on the engine's FFT solve
+    (256 x 256, spacing 0.1): within 2e-4 of the magnetostatic solution of a
+    rotating disc current, rotation symmetries to 1e-8, and the oracle's
+    filter sums to 1e-10."""
+    import math
+    from oracle import oracle as O
+    import superconga_b200 as sb
+    cfg = configs.disc_n256()
+    e = sb.Context(cfg)
+    assert e.dims.n0 == 256
+    j, expected = configs.rotating_disc_current(256, 0.1)
+    a = e.poisson(j)
+    assert math.sqrt(np.sum((a - expected) ** 2) / np.sum(expected ** 2)) < 2e-4
+    assert configs.vector_potential_symmetry_error(a) < 1e-8
+    assert _rel(a, O.Oracle(cfg).poisson(j)) < 1e-10
+    e.close()
+
+
 @pytest.mark.parametrize("acc", ["congacc", "picard", "polyak", "barzilai-borwein", "anderson"])
 def test_golden_free_energy(engine_lib, acc):
     """tests/accelerators_test.cu:45-149 on the engine: converged within 100
