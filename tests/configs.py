@@ -213,6 +213,53 @@ def ldos_postprocess(delta0: float, n_energies: int = 12, per_block: int = 8, n_
     }
 
 
+def dos_test_case(swave: bool):
+    """tests/physics/dos_test.cu:10-21,23-69: an s-wave disc or a d_{x2-y2}
+    square with axes along its edges (no pair breaking), width 5 xi0 at 2
+    points/xi0, 160 angles, T = 0.5; the LDOS of 32 energies in [0, 0.5] with
+    broadening 0.008 in one block, criterion 1e-8 (L-infinity), at most 42
+    iterations.  Returns (simulation, postprocess) configurations."""
+    geom = ({"disc": {"add": True, "radius": 2.5, "center_x": 0.0, "center_y": 0.0}} if swave else
+            {"regular_polygon": {"add": True, "num_edges": 4, "side_length": 5.0, "rotation": 0.0,
+                                 "center_x": 0.0, "center_y": 0.0}})
+    sim = {
+        "physics": {"temperature": 0.5, "external_flux_quanta": 0.0, "penetration_depth": -1.0,
+                    "charge_sign": -1, "gauge": "symmetric", "crystal_axes_rotation": 0.0,
+                    "order_parameter": {("s" if swave else "dx2-y2"): {"critical_temperature": 1.0}}},
+        "geometry": [geom],
+        "numerics": {"points_per_coherence_length": 2.0, "num_fermi_momenta": 160,
+                     "energy_cutoff": 16.0, "convergence_criterion": 1e-8, "norm": "linf"},
+    }
+    pp = {
+        "spectroscopy": {"energy_min": 0.0, "energy_max": 0.5, "num_energies": 32,
+                         "energy_broadening": 0.008},
+        "numerics": {"convergence_criterion": 1e-8, "norm": "linf", "num_energies_per_block": 32,
+                     "num_fermi_momenta": 160, "num_iterations_burnin": 0,
+                     "num_iterations_min": 0, "num_iterations_max": 42},
+        "misc": {"data_format": "csv", "load_path": "", "save_path": "", "verbose": False},
+    }
+    return sim, pp
+
+
+def bulk_dos(energy: np.ndarray, broadening: float, delta: float, swave: bool, n_angles: int) -> np.ndarray:
+    """The expected DOS of tests/physics/dos_test.cu:168-198: sum over the
+    circle's angles of w_k Im[e / sqrt(|eta_k delta|^2 - e^2)], e = E + i delta_b,
+    with the normalised basis function eta at the Fermi momentum (1 for s,
+    cos 2 phi normalised for d_{x2-y2}) and the Boole / Simpson weights."""
+    k = np.arange(n_angles)
+    phi = np.mod(2 * np.pi * k / n_angles + 0.5 * np.pi, 2 * np.pi)
+    w = np.where(k % 4 == 0, 28.0, np.where(k % 2 == 0, 24.0, 64.0)) / 45.0 if n_angles % 4 == 0 else np.ones(n_angles)
+    w = w / n_angles
+    raw = np.ones(n_angles) if swave else np.cos(phi) ** 2 - np.sin(phi) ** 2
+    eta = raw / np.sqrt(np.sum(raw * raw * w))
+    out = np.zeros(len(energy))
+    for i, e0 in enumerate(energy):
+        e = e0 + 1j * broadening
+        om = np.sqrt(np.abs(eta * delta) ** 2 - e * e + 0j)
+        out[i] = np.sum(w * (e / om).imag)
+    return out
+
+
 def bcs_dos(energy: np.ndarray, broadening: float, delta: float) -> np.ndarray:
     """Bulk s-wave density of states Re[e / sqrt(e^2 - delta^2)], e = E + i delta_b
     (retarded branch: the root with positive imaginary part times sign)."""

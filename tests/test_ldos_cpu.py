@@ -65,3 +65,28 @@ def test_particle_hole_symmetry(O):
     scale = np.max(np.abs(L.ldos))
     for k in range(n // 2):
         assert np.max(np.abs(L.ldos[k] - L.ldos[n - 1 - k])) < 1e-6 * scale, k
+
+
+@pytest.mark.parametrize("swave", [True, False], ids=["s-wave disc", "d-wave square"])
+def test_reference_dos(O, swave):
+    """tests/physics/dos_test.cu:218-240 (double): the grain-averaged LDOS of a
+    bulk s-wave disc and of a d_{x2-y2} square without pair breaking converges
+    within 42 iterations and matches the angle-averaged bulk DOS to 1e-8."""
+    sim, pp = configs.dos_test_case(swave)
+    L = O.LdosOracle(sim, pp)
+    s = L.oracle.setup
+    db = O.delta_bulk(0.5, s.symmetries[0])
+    d = np.zeros((1, 2, L.n0, L.n0))
+    d[0, 0] = db
+    L.set_state(d, np.zeros((2, L.n0, L.n0)))
+    L.begin_block(0)
+    res = 1.0
+    for _ in range(42):
+        res = L.iterate()[0]
+        if res < 1e-8:
+            break
+    assert res < 1e-8
+    dom = L.oracle.domain() > 0
+    got = np.array([L.ldos[k][dom].mean() for k in range(len(L.energies))])
+    want = configs.bulk_dos(np.asarray(L.energies), 0.008, db, swave, 160)
+    assert np.max(np.abs(got - want) / (1.0 + np.abs(want))) < 1e-8

@@ -140,3 +140,33 @@ def test_ldos_mixed(engine_lib):
         out.append(e.ldos())
         e.close()
     assert _rel(out[1], out[0]) < 1e-4
+
+
+@pytest.mark.parametrize("swave", [True, False], ids=["s-wave disc", "d-wave square"])
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+def test_reference_dos(engine_lib, swave, mode):
+    """tests/physics/dos_test.cu:211-240 on the engine: the grain-averaged LDOS
+    converges within 42 iterations and matches the bulk DOS to 1e-8 (FP64,
+    criterion 1e-8); mixed precision takes the reference's single-precision
+    case (criterion 1e-4, bound 1e-5)."""
+    from oracle import oracle as O
+    import superconga_b200 as sb
+    sim, pp = configs.dos_test_case(swave)
+    if mode == "mixed":
+        sim["numerics"]["convergence_criterion"] = 1e-4
+        pp["numerics"]["convergence_criterion"] = 1e-4
+    e = sb.LdosContext(sim, pp, mode=mode)
+    n0 = e.dims.n0
+    db = O.delta_bulk(0.5, "s" if swave else "dx2-y2")
+    d = np.zeros((1, 2, n0, n0))
+    d[0, 0] = db
+    e.set_state(d, np.zeros((2, n0, n0)))
+    conv, it = e.run(0, 0, 42)
+    assert conv
+    en, _ = e.energies()
+    ldos = e.ldos()
+    dom = e.domain() > 0
+    got = np.array([ldos[k][dom].mean() for k in range(len(en))])
+    want = configs.bulk_dos(np.asarray(en), 0.008, db, swave, 160)
+    tol = 1e-8 if mode == "fp64" else 1e-5
+    assert np.max(np.abs(got - want) / (1.0 + np.abs(want))) < tol
