@@ -275,6 +275,20 @@ int sc_setup_site_updates(const sc_setup *s, long long *per_iteration);
  * .h:79-80; 1 on the circle), momentum origin x, y.  Either may be NULL. */
 int sc_setup_fermi_surface(const sc_setup *s, double *table, double *info);
 
+/* Bulk s-wave thermodynamics (host only).
+ * sc_bulk_order_parameter_s_wave: computeOrderParameterBulkSWave
+ * (OrderParameterBulk.h:88-221), the bulk gap at temperature T/Tc in units of
+ * 2 pi k_B Tc; the reference's defaults are criterion 10 eps, 10 iterations,
+ * cutoff 100.  A d-wave (or g-wave) component's bulk amplitude is this value
+ * times D_WAVE_BULK / S_WAVE_BULK (OrderParameterComponent.h:210-235).
+ * sc_bulk_free_energy_s_wave: computeFreeEnergyBulkSWave
+ * (OrderParameterBulk.h:224-246), the bulk free energy density at that gap
+ * (reference default cutoff 100). */
+int sc_bulk_order_parameter_s_wave(double temperature, double convergence_criterion,
+                                   int max_iterations, double energy_cutoff, double *out);
+int sc_bulk_free_energy_s_wave(double temperature, double order_parameter, double energy_cutoff,
+                               double *out);
+
 /* Load-path helpers for runs saved on another lattice (host only).
  * sc_grid_extend: extendValuesAtBoundary (domain_ops.h:11-69) of n_fields
  * planes [n_fields][n][n] in place, with the domain labels of that lattice.

@@ -355,6 +355,16 @@ def bulk_s_wave(temperature: float, crit: float = 10.0 * np.finfo(np.float64).ep
     return op
 
 
+def bulk_free_energy_s_wave(temperature: float, op: float, cutoff: float = 100.0) -> float:
+    """computeFreeEnergyBulkSWave, include/conga/order_parameter/OrderParameterBulk.h:224-246."""
+    ne = int(cutoff / temperature - 0.5) + 1
+    esum = 0.0
+    for n in range(ne - 1, -1, -1):
+        e = temperature * (n + 0.5)
+        esum += 1.0 / e - 2.0 / (e + math.hypot(op, e))
+    return op * op * (math.log(temperature) + temperature * esum)
+
+
 def delta_bulk(temperature: float, symmetry: str) -> float:
     """OrderParameterComponent::deltaBulk, OrderParameterComponent.h:210-235."""
     s = bulk_s_wave(temperature)

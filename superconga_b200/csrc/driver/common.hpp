@@ -25,32 +25,11 @@ namespace drv {
 
 constexpr double EULER_GAMMA = 0.57721566490153286060651209008240243;
 
-// computeOrderParameterBulkSWave (OrderParameterBulk.h:88-221).
+// computeOrderParameterBulkSWave (OrderParameterBulk.h:88-221) with the
+// reference's defaults, from the library.
 inline double bulk_s_wave(double t) {
-  const double eps = 2.220446049250313e-16;
-  if (t >= 1.0) return 0.0;
-  const double s_bulk = 0.5 * std::exp(-EULER_GAMMA);
-  if (t < eps) return s_bulk;
-  const int ne = (int)(100.0 / t - 0.5) + 1;
-  double es = 0.0;
-  for (int n = ne - 1; n >= 0; --n) es += 1.0 / (t * ((double)n + 0.5));
-  const double coupling = 1.0 / (std::log(t) / t + es);
-  auto resid = [&](double op) {
-    double integ = 0.0;
-    for (int n = ne - 1; n >= 0; --n) integ += 1.0 / std::hypot(op, t * ((double)n + 0.5));
-    return op * (integ * coupling - 1.0);
-  };
-  double op = s_bulk * std::sqrt(1.0 - t * t * t);
-  double ops[2] = {op, std::sqrt(op)}, rs[2] = {resid(ops[0]), resid(ops[1])};
-  for (int it = 0; it < 10; ++it) {
-    const double w = 1.0 / (1.0 - (ops[0] / ops[1]) / (rs[0] / rs[1]));
-    op = (1.0 - w) * ops[0] + w * ops[1];
-    const double r = resid(op);
-    if (std::fabs(r / op) < 10.0 * eps) break;
-    const int k = std::fabs(rs[0]) > std::fabs(rs[1]) ? 0 : 1;
-    ops[k] = op;
-    rs[k] = r;
-  }
+  double op = 0.0;
+  sc_bulk_order_parameter_s_wave(t, 10.0 * 2.220446049250313e-16, 10, 100.0, &op);
   return op;
 }
 

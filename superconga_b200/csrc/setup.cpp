@@ -369,13 +369,15 @@ void ozaki_poles(int n, double *poles, double *residues) {
   }
 }
 
-// computeOrderParameterBulkSWave, OrderParameterBulk.h:88-221.
-double bulk_s_wave(double t) {
+// computeOrderParameterBulkSWave, OrderParameterBulk.h:88-221: secant
+// iteration on the bulk gap equation with the Matsubara sum cut at
+// energy_cutoff, starting from S_WAVE_BULK sqrt(1 - t^3) and its square root.
+double bulk_s_wave(double t, double crit, int max_it, double energy_cutoff) {
   const double eps = std::numeric_limits<double>::epsilon();
   if (t >= 1.0) return 0.0;
   const double s_bulk = 0.5 * std::exp(-EULER_GAMMA);
   if (t < eps) return s_bulk;
-  const int ne = (int)(100.0 / t - 0.5) + 1;
+  const int ne = (int)(energy_cutoff / t - 0.5) + 1;
   double es = 0.0;
   for (int n = ne - 1; n >= 0; --n) es += 1.0 / (t * ((double)n + 0.5));
   const double coupling = 1.0 / (std::log(t) / t + es);
@@ -386,18 +388,30 @@ double bulk_s_wave(double t) {
   };
   double op = s_bulk * std::sqrt(1.0 - t * t * t);
   double ops[2] = {op, std::sqrt(op)}, rs[2] = {resid(ops[0]), resid(ops[1])};
-  for (int it = 0; it < 10; ++it) {
+  for (int it = 0; it < max_it; ++it) {
     const double w = 1.0 / (1.0 - (ops[0] / ops[1]) / (rs[0] / rs[1]));
     op = (1.0 - w) * ops[0] + w * ops[1];
     const double r = resid(op);
     const bool small = op < 10.0 * eps;
     const double rel = small ? r : std::fabs(r / op);
-    if (rel < 10.0 * eps) break;
+    if (rel < crit) break;
     const int k = std::fabs(rs[0]) > std::fabs(rs[1]) ? 0 : 1;
     ops[k] = op;
     rs[k] = r;
   }
   return op;
+}
+
+// computeFreeEnergyBulkSWave, OrderParameterBulk.h:224-246: the bulk free
+// energy density Delta^2 (ln t + t sum_n [1/e_n - 2/(e_n + Omega_n)]).
+double bulk_free_energy_s_wave(double t, double op, double energy_cutoff) {
+  const int ne = (int)(energy_cutoff / t - 0.5) + 1;
+  double esum = 0.0;
+  for (int n = ne - 1; n >= 0; --n) {
+    const double e = t * ((double)n + 0.5);
+    esum += 1.0 / e - 2.0 / (e + std::hypot(op, e));
+  }
+  return op * op * (std::log(t) + t * esum);
 }
 
 long long HostSetup::site_updates_per_iteration() const {
@@ -1450,6 +1464,22 @@ int sc_setup_filters(const sc_setup *s, int *n_filters, double *filters, int *po
 int sc_setup_site_updates(const sc_setup *s, long long *per_iteration) {
   if (!s || !per_iteration) return SC_ERR_ARG;
   *per_iteration = s->S.site_updates_per_iteration();
+  return SC_OK;
+}
+
+int sc_bulk_order_parameter_s_wave(double temperature, double convergence_criterion,
+                                   int max_iterations, double energy_cutoff, double *out) {
+  if (!out || !(temperature >= 0.0) || !(energy_cutoff > 0.0) || max_iterations < 0 ||
+      !(convergence_criterion > 0.0))
+    return SC_ERR_ARG;
+  *out = scb::bulk_s_wave(temperature, convergence_criterion, max_iterations, energy_cutoff);
+  return SC_OK;
+}
+
+int sc_bulk_free_energy_s_wave(double temperature, double order_parameter, double energy_cutoff,
+                               double *out) {
+  if (!out || !(temperature > 0.0) || !(energy_cutoff > 0.0)) return SC_ERR_ARG;
+  *out = scb::bulk_free_energy_s_wave(temperature, order_parameter, energy_cutoff);
   return SC_OK;
 }
 

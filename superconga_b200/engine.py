@@ -252,6 +252,26 @@ def fma_peak(precision: int = 64) -> float:
     return v.value
 
 
+def bulk_order_parameter_s_wave(temperature: float, convergence_criterion: float = 10.0 * np.finfo(np.float64).eps,
+                                max_iterations: int = 10, energy_cutoff: float = 100.0) -> float:
+    """computeOrderParameterBulkSWave (OrderParameterBulk.h:88-221): the bulk
+    s-wave gap at T/Tc, in units of 2 pi k_B Tc (host only)."""
+    v = ctypes.c_double()
+    _lib.check(_lib.load().sc_bulk_order_parameter_s_wave(float(temperature), float(convergence_criterion),
+                                                         int(max_iterations), float(energy_cutoff),
+                                                         ctypes.byref(v)))
+    return v.value
+
+
+def bulk_free_energy_s_wave(temperature: float, order_parameter: float, energy_cutoff: float = 100.0) -> float:
+    """computeFreeEnergyBulkSWave (OrderParameterBulk.h:224-246): the bulk
+    free energy density at the given gap (host only)."""
+    v = ctypes.c_double()
+    _lib.check(_lib.load().sc_bulk_free_energy_s_wave(float(temperature), float(order_parameter),
+                                                     float(energy_cutoff), ctypes.byref(v)))
+    return v.value
+
+
 class Setup:
     """Host-only view of a configuration's static tables (no GPU needed)."""
 

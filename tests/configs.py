@@ -241,6 +241,26 @@ def dos_test_case(swave: bool):
     return sim, pp
 
 
+def low_temperature_bulk(swave: bool, disc: bool) -> dict:
+    """tests/physics/low_temp_free_energy_test.cu:30-60,62-160: an s-wave disc,
+    an s-wave square or a d_{x2-y2} square (axes along the edges) of width 10
+    xi0 at 1 point/xi0, T = 0.001, cutoff 32 (281 Ozaki poles), 32 (s-wave) or
+    360 (d-wave) angles, no field and no vector potential, L-infinity
+    residuals, criterion 1e-3, Barzilai-Borwein, bulk start."""
+    geom = ({"disc": {"add": True, "radius": 5.0, "center_x": 0.0, "center_y": 0.0}} if disc else
+            {"regular_polygon": {"add": True, "num_edges": 4, "side_length": 10.0, "rotation": 0.0,
+                                 "center_x": 0.0, "center_y": 0.0}})
+    return {
+        "physics": {"temperature": 0.001, "external_flux_quanta": 0.0, "penetration_depth": -1.0,
+                    "charge_sign": -1, "gauge": "symmetric", "crystal_axes_rotation": 0.0,
+                    "order_parameter": {("s" if swave else "dx2-y2"): {"critical_temperature": 1.0}}},
+        "geometry": [geom],
+        "numerics": {"points_per_coherence_length": 1.0, "num_fermi_momenta": 32 if swave else 360,
+                     "energy_cutoff": 32.0, "convergence_criterion": 1e-3, "norm": "linf"},
+        "accelerator": {"name": "barzilai-borwein"},
+    }
+
+
 def bulk_dos(energy: np.ndarray, broadening: float, delta: float, swave: bool, n_angles: int) -> np.ndarray:
     """The expected DOS of tests/physics/dos_test.cu:168-198: sum over the
     circle's angles of w_k Im[e / sqrt(|eta_k delta|^2 - e^2)], e = E + i delta_b,

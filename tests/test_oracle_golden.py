@@ -138,6 +138,48 @@ def test_swave_disc_analytic_free_energy(O):
     assert abs(fe - expected) <= 1e-3 * abs(expected), (fe, expected)
 
 
+LOW_TEMPERATURE_CASES = {"s_disc": (True, True), "s_square": (True, False), "d_square": (False, False)}
+
+
+def low_temperature_observables(delta, current, domain, free_energy_per_area):
+    """The grain averages of tests/physics/low_temp_free_energy_test.cu:162-186:
+    the order parameter and current magnitudes summed over the grain's sites
+    and divided by their number, and the free energy per area."""
+    grain = domain > 0
+    n = grain.sum()
+    mag = np.sqrt((delta ** 2).sum(axis=(0, 1)))
+    jmag = np.sqrt((current ** 2).sum(axis=0))
+    return (mag * grain).sum() / n, (jmag * grain).sum() / n, free_energy_per_area
+
+
+@pytest.mark.parametrize("case", list(LOW_TEMPERATURE_CASES))
+def test_low_temperature_bulk_values(O, case):
+    """tests/physics/low_temp_free_energy_test.cu:62-281 (double): at T =
+    0.001 a grain without pair breaking converges within 50 iterations to the
+    zero-temperature bulk gap (S_WAVE_BULK or D_WAVE_BULK, 1e-5 relative), no
+    current (machine epsilon) and the bulk free energy -Delta^2/2 per area
+    (1e-4 relative)."""
+    swave, disc = LOW_TEMPERATURE_CASES[case]
+    o = O.Oracle(configs.low_temperature_bulk(swave, disc))
+    s = o.setup
+    d = np.zeros((1, 2, s.n0, s.n0))
+    d[0, 0] = O.delta_bulk(0.001, "s" if swave else "dx2-y2")
+    o.set_state(d, np.zeros((2, s.n0, s.n0)))
+    converged = False
+    for _ in range(50):
+        o.compute()
+        if o.is_converged():
+            converged = True
+            break
+    delta, current, _ = o.results()
+    avg_d, avg_j, fe = low_temperature_observables(delta, current, o.domain(), o.scalars()["free_energy_per_area"])
+    expected = O.S_WAVE_BULK if swave else O.D_WAVE_BULK
+    assert converged
+    assert avg_d == pytest.approx(expected, rel=1e-5)
+    assert abs(avg_j) <= np.finfo(np.float64).eps * (1.0 + abs(avg_j))
+    assert fe == pytest.approx(-0.5 * expected * expected, rel=1e-4)
+
+
 def test_free_energy_component_order(O):
     """tests/free_energy_test.cu:144-169: the free energy does not depend on
     the order of the order-parameter components (s with Tc 0.1 and d_xy with

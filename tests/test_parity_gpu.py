@@ -244,6 +244,46 @@ def test_swave_disc_analytic_free_energy(engine_lib, mode):
     e.close()
 
 
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+@pytest.mark.parametrize("case", ["s_disc", "s_square", "d_square"])
+def test_low_temperature_bulk_values(engine_lib, case, mode):
+    """tests/physics/low_temp_free_energy_test.cu:62-281 on the engine (281
+    Ozaki poles, 32 or 360 angles): converged within 50 iterations, grain-
+    averaged gap within 1e-5 of the zero-temperature bulk value, no current
+    (machine epsilon of the stepping type, as the reference's float and double
+    cases), free energy per area within 1e-4 of -Delta^2/2.  FP64 also matches
+    the oracle's converged fields (1e-10)."""
+    from oracle import oracle as O
+    import superconga_b200 as sb
+    from tests.test_oracle_golden import LOW_TEMPERATURE_CASES, low_temperature_observables
+    swave, disc = LOW_TEMPERATURE_CASES[case]
+    cfg = configs.low_temperature_bulk(swave, disc)
+    e = sb.Context(cfg, mode=mode)
+    n0 = e.dims.n0
+    d = np.zeros((1, 2, n0, n0))
+    d[0, 0] = O.delta_bulk(0.001, "s" if swave else "dx2-y2")
+    e.set_state(d, np.zeros((2, n0, n0)))
+    it, conv = e.run(1, 50)
+    delta, current, _ = e.results()
+    sc = e.scalars()
+    avg_d, avg_j, fe = low_temperature_observables(delta, current, e.domain(), sc["free_energy_per_area"])
+    expected = O.S_WAVE_BULK if swave else O.D_WAVE_BULK
+    eps = np.finfo(np.float64 if mode == "fp64" else np.float32).eps
+    assert conv
+    assert avg_d == pytest.approx(expected, rel=1e-5)
+    assert abs(avg_j) <= eps * (1.0 + abs(avg_j))
+    assert fe == pytest.approx(-0.5 * expected * expected, rel=1e-4)
+    if mode == "fp64":
+        o = O.Oracle(cfg)
+        o.set_state(d, np.zeros((2, n0, n0)))
+        for _ in range(it):
+            o.compute()
+        assert _rel(delta, o.results()[0]) < TOL
+        so = o.scalars()["free_energy_per_area"]
+        assert abs(sc["free_energy_per_area"] - so) <= TOL * abs(so)
+    e.close()
+
+
 def test_mixed_precision(engine_lib):
     """FP32 stepping with FP64 accumulation against the FP64 form after five
     iterations: |Delta - Delta_FP64| / Delta_bulk <= 1e-5."""
