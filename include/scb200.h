@@ -283,11 +283,15 @@ int sc_setup_fermi_surface(const sc_setup *s, double *table, double *info);
  * times D_WAVE_BULK / S_WAVE_BULK (OrderParameterComponent.h:210-235).
  * sc_bulk_free_energy_s_wave: computeFreeEnergyBulkSWave
  * (OrderParameterBulk.h:224-246), the bulk free energy density at that gap
- * (reference default cutoff 100). */
+ * (reference default cutoff 100).
+ * sc_bulk_yoshida_s_wave: computeYoshidaBulkSWave (OrderParameterBulk.h:256-277),
+ * the Yoshida function that sets the London response j = -Y A of the bulk. */
 int sc_bulk_order_parameter_s_wave(double temperature, double convergence_criterion,
                                    int max_iterations, double energy_cutoff, double *out);
 int sc_bulk_free_energy_s_wave(double temperature, double order_parameter, double energy_cutoff,
                                double *out);
+int sc_bulk_yoshida_s_wave(double temperature, double order_parameter, double energy_cutoff,
+                           double *out);
 
 /* Load-path helpers for runs saved on another lattice (host only).
  * sc_grid_extend: extendValuesAtBoundary (domain_ops.h:11-69) of n_fields

@@ -365,6 +365,17 @@ def bulk_free_energy_s_wave(temperature: float, op: float, cutoff: float = 100.0
     return op * op * (math.log(temperature) + temperature * esum)
 
 
+def bulk_yoshida_s_wave(temperature: float, op: float, cutoff: float) -> float:
+    """computeYoshidaBulkSWave, include/conga/order_parameter/OrderParameterBulk.h:256-277."""
+    if temperature < np.finfo(np.float64).eps:
+        return 1.0
+    ne = int(cutoff / temperature - 0.5) + 1
+    esum = 0.0
+    for n in range(ne - 1, -1, -1):
+        esum += 1.0 / math.hypot(op, temperature * (n + 0.5)) ** 3
+    return temperature * op * op * esum
+
+
 def delta_bulk(temperature: float, symmetry: str) -> float:
     """OrderParameterComponent::deltaBulk, OrderParameterComponent.h:210-235."""
     s = bulk_s_wave(temperature)

@@ -7,8 +7,9 @@ face of one engine handle; ``LdosContext`` runs the LDOS postprocess and
 ``Batch`` advances many grains together.
 """
 from .engine import (Batch, Context, Dims, LdosContext, Setup,  # noqa: F401
-                     bulk_free_energy_s_wave, bulk_order_parameter_s_wave)
+                     bulk_free_energy_s_wave, bulk_order_parameter_s_wave,
+                     bulk_yoshida_s_wave)
 from ._lib import EngineError, LIB_PATH, load  # noqa: F401
 
 __all__ = ["Batch", "Context", "Dims", "LdosContext", "Setup", "bulk_order_parameter_s_wave",
-           "bulk_free_energy_s_wave", "EngineError", "LIB_PATH", "load"]
+           "bulk_free_energy_s_wave", "bulk_yoshida_s_wave", "EngineError", "LIB_PATH", "load"]

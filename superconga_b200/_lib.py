@@ -77,6 +77,8 @@ SIGNATURES = {
                                                       ctypes.c_double, _c_double_p]),
     "sc_bulk_free_energy_s_wave": (ctypes.c_int, [ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                                   _c_double_p]),
+    "sc_bulk_yoshida_s_wave": (ctypes.c_int, [ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                              _c_double_p]),
     "sc_grid_extend": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, _c_double_p]),
     "sc_grid_resample": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _c_double_p, _c_double_p]),
     "sc_measure_fma_peak": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),

@@ -414,6 +414,19 @@ double bulk_free_energy_s_wave(double t, double op, double energy_cutoff) {
   return op * op * (std::log(t) + t * esum);
 }
 
+// computeYoshidaBulkSWave, OrderParameterBulk.h:256-277: the Yoshida function
+// Y = t Delta^2 sum_n 1/Omega_n^3 (1 at zero temperature).
+double bulk_yoshida_s_wave(double t, double op, double energy_cutoff) {
+  if (t < std::numeric_limits<double>::epsilon()) return 1.0;
+  const int ne = (int)(energy_cutoff / t - 0.5) + 1;
+  double esum = 0.0;
+  for (int n = ne - 1; n >= 0; --n) {
+    const double om = std::hypot(op, t * ((double)n + 0.5));
+    esum += 1.0 / (om * om * om);
+  }
+  return t * op * op * esum;
+}
+
 long long HostSetup::site_updates_per_iteration() const {
   long long inside = 0;
   const size_t nn = (size_t)n1 * n1;
@@ -1480,6 +1493,13 @@ int sc_bulk_free_energy_s_wave(double temperature, double order_parameter, doubl
                                double *out) {
   if (!out || !(temperature > 0.0) || !(energy_cutoff > 0.0)) return SC_ERR_ARG;
   *out = scb::bulk_free_energy_s_wave(temperature, order_parameter, energy_cutoff);
+  return SC_OK;
+}
+
+int sc_bulk_yoshida_s_wave(double temperature, double order_parameter, double energy_cutoff,
+                           double *out) {
+  if (!out || !(temperature >= 0.0) || !(energy_cutoff > 0.0)) return SC_ERR_ARG;
+  *out = scb::bulk_yoshida_s_wave(temperature, order_parameter, energy_cutoff);
   return SC_OK;
 }
 

@@ -152,6 +152,7 @@ void ozaki_poles(int n, double *poles, double *residues);
 void symmetric_eigen(int n, std::vector<double> &a, std::vector<double> &w);
 double bulk_s_wave(double temperature, double criterion, int max_iterations, double energy_cutoff);
 double bulk_free_energy_s_wave(double temperature, double order_parameter, double energy_cutoff);
+double bulk_yoshida_s_wave(double temperature, double order_parameter, double energy_cutoff);
 // Tight-binding Fermi surface (FermiSurfaceTightBinding.h): fills phi, theta,
 // px, py, vx, vy, speed and weight of S for S.n_angles angles.
 void tight_binding_surface(HostSetup &S);

@@ -272,6 +272,15 @@ def bulk_free_energy_s_wave(temperature: float, order_parameter: float, energy_c
     return v.value
 
 
+def bulk_yoshida_s_wave(temperature: float, order_parameter: float, energy_cutoff: float) -> float:
+    """computeYoshidaBulkSWave (OrderParameterBulk.h:256-277): the bulk London
+    response j = -Y A at the given gap (host only)."""
+    v = ctypes.c_double()
+    _lib.check(_lib.load().sc_bulk_yoshida_s_wave(float(temperature), float(order_parameter),
+                                                 float(energy_cutoff), ctypes.byref(v)))
+    return v.value
+
+
 class Setup:
     """Host-only view of a configuration's static tables (no GPU needed)."""
 

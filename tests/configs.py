@@ -261,6 +261,169 @@ def low_temperature_bulk(swave: bool, disc: bool) -> dict:
     }
 
 
+def phase_gradient_disc() -> dict:
+    """tests/physics/current_phase_gradient_test.cu:22-78: s-wave disc of width
+    10 xi0 at 2 points/xi0, 16 angles, T = 0.9, cutoff 16, criterion 1e-5
+    (L-infinity), no field, charge sign -1, no vector potential,
+    Barzilai-Borwein."""
+    return {
+        "physics": {"temperature": 0.9, "external_flux_quanta": 0.0, "penetration_depth": -1.0,
+                    "charge_sign": -1, "gauge": "symmetric", "crystal_axes_rotation": 0.0,
+                    "order_parameter": {"s": {"critical_temperature": 1.0}}},
+        "geometry": [{"disc": {"add": True, "radius": 5.0, "center_x": 0.0, "center_y": 0.0}}],
+        "numerics": {"points_per_coherence_length": 2.0, "num_fermi_momenta": 16,
+                     "energy_cutoff": 16.0, "convergence_criterion": 1e-5, "norm": "linf"},
+        "accelerator": {"name": "barzilai-borwein"},
+    }
+
+
+def phase_winding_state(n0: int, delta_bulk: float, winding: float, phase_shift: float = 0.0,
+                        center=(0.0, 0.0)) -> np.ndarray:
+    """Initial<T>::phaseWinding without noise (OrderParameterInitial.h:187-235,
+    375-381): Delta_bulk exp(i (shift + w atan2(y, x))) on the lattice
+    normalised to [-1, 1], the winding centre taking phase 0.  Returns
+    [1][2][n0][n0]."""
+    c = np.arange(n0, dtype=np.float64)
+    u = 2.0 * c / (n0 - 1) - 1.0
+    x = u[None, :] - center[0]
+    y = u[:, None] - center[1]
+    ang = np.where(np.hypot(x, y) > 0.0, np.arctan2(y, x), 0.0)
+    phase = phase_shift + winding * ang
+    out = np.zeros((1, 2, n0, n0))
+    out[0, 0] = delta_bulk * np.cos(phase)
+    out[0, 1] = delta_bulk * np.sin(phase)
+    return out
+
+
+def complex_phase_gradient(re: np.ndarray, im: np.ndarray, h: float = 1.0) -> np.ndarray:
+    """GridFunctions::complexPhaseGradient (GridFunctions_GPU.h:209-267):
+    central differences of the phase, (f' g - f g') / (2 h |z|^2) with f = Im
+    z, g = Re z, zero on the lattice border and where 2 h |z|^2 <= 1e-5.
+    Returns [2][n][n] (x, y)."""
+    n = re.shape[0]
+    out = np.zeros((2, n, n))
+    g1, f1 = re[1:-1, 1:-1], im[1:-1, 1:-1]
+    denom = 2.0 * h * (f1 * f1 + g1 * g1)
+    ok = denom > 1e-5
+    inv = np.where(ok, 1.0 / np.where(ok, denom, 1.0), 0.0)
+    dx = ((im[1:-1, 2:] - im[1:-1, :-2]) * g1 - f1 * (re[1:-1, 2:] - re[1:-1, :-2])) * inv
+    dy = ((im[2:, 1:-1] - im[:-2, 1:-1]) * g1 - f1 * (re[2:, 1:-1] - re[:-2, 1:-1])) * inv
+    out[0, 1:-1, 1:-1] = np.where(ok, dx, 0.0)
+    out[1, 1:-1, 1:-1] = np.where(ok, dy, 0.0)
+    return out
+
+
+def penetration_depth_disc() -> dict:
+    """tests/physics/penetration_depth_test.cu:89-131: s-wave disc of width 20
+    xi0 at 5 points/xi0, 16 angles, T = 0.1, cutoff 16, half a flux quantum,
+    lambda = 1, symmetric gauge, L-infinity residuals, criterion 1e-3, CongAcc
+    with initial step 0.001, bulk start."""
+    return {
+        "physics": {"temperature": 0.1, "external_flux_quanta": 0.5, "penetration_depth": 1.0,
+                    "charge_sign": -1, "gauge": "symmetric", "crystal_axes_rotation": 0.0,
+                    "order_parameter": {"s": {"critical_temperature": 1.0}}},
+        "geometry": [{"disc": {"add": True, "radius": 10.0, "center_x": 0.0, "center_y": 0.0}}],
+        "numerics": {"points_per_coherence_length": 5.0, "num_fermi_momenta": 16,
+                     "energy_cutoff": 16.0, "convergence_criterion": 1e-3, "norm": "linf",
+                     "vector_potential_error": 1e-6},
+        "accelerator": {"name": "congacc", "step_size": 0.001},
+    }
+
+
+def curl(ax: np.ndarray, ay: np.ndarray, h: float) -> np.ndarray:
+    """GridFunctions::curl (GridFunctions_GPU.h:327-353): dAy/dx - dAx/dy by
+    central differences, one-sided on the lattice border, divided by h."""
+    n = ax.shape[0]
+    i = np.arange(n)
+    nxt, prv = np.minimum(i + 1, n - 1), np.maximum(i - 1, 0)
+    span = (nxt - prv).astype(np.float64)
+    day_dx = (ay[:, nxt] - ay[:, prv]) / span[None, :]
+    dax_dy = (ax[nxt, :] - ax[prv, :]) / span[:, None]
+    return (day_dx - dax_dy) / h
+
+
+def fit_penetration_depth(guess: float, b_ext: float, width: float, flux: float) -> float:
+    """Newton fit of the London flux through a disc, 2 pi b k ((R - k) + k
+    exp(-R/k)) with R = width / 2, to the measured flux
+    (tests/physics/penetration_depth_test.cu:15-81)."""
+    r = 0.5 * width
+    factor = 2.0 * math.pi * b_ext
+    k = guess
+    for _ in range(200):
+        res = factor * k * ((r - k) + k * math.exp(-r / k)) - flux
+        drdk = factor * ((r + 2.0 * k) * math.exp(-r / k) + r - 2.0 * k)
+        dk = res * math.copysign(1.0, drdk) / max(abs(drdk), np.finfo(np.float64).eps)
+        done = abs(dk / k) < 1e-6
+        k -= dk
+        if done:
+            return k
+    raise RuntimeError("penetration-depth fit did not converge")
+
+
+def penetration_depth_from_state(a: np.ndarray, domain: np.ndarray, h: float, flux_quanta: float,
+                                 width: float, guess: float) -> float:
+    """The fitted penetration depth of tests/physics/penetration_depth_test.cu:
+    133-150: flux = area (b_ext + <curl A>_grain) with area = sites h^2 and
+    b_ext = pi flux_quanta / area."""
+    grain = domain > 0
+    n = grain.sum()
+    area = n * h * h
+    b_ext = math.pi * flux_quanta / area
+    b = curl(a[0], a[1], h)
+    flux = area * (b_ext + (b * grain).sum() / n)
+    return fit_penetration_depth(guess, b_ext, width, flux)
+
+
+def linear_response_square(temperature: float) -> dict:
+    """tests/physics/current_linear_response_test.cu:15-120: s-wave square of
+    side 20 xi0 at 1 point/xi0, 32 angles, cutoff 16, lambda = 1, no external
+    field, bulk start; the induced vector potential is held at (0.01, 0.01)
+    for the one iteration the test runs."""
+    return {
+        "physics": {"temperature": temperature, "external_flux_quanta": 0.0, "penetration_depth": 1.0,
+                    "charge_sign": -1, "gauge": "symmetric", "crystal_axes_rotation": 0.0,
+                    "order_parameter": {"s": {"critical_temperature": 1.0}}},
+        "geometry": [{"regular_polygon": {"add": True, "num_edges": 4, "side_length": 20.0,
+                                          "rotation": 0.0, "center_x": 0.0, "center_y": 0.0}}],
+        "numerics": {"points_per_coherence_length": 1.0, "num_fermi_momenta": 32,
+                     "energy_cutoff": 16.0, "convergence_criterion": 1e-4, "norm": "l2",
+                     "vector_potential_error": 1e-6},
+        "accelerator": {"name": "congacc"},
+    }
+
+
+def solenoid_annulus(flux_quanta: float) -> dict:
+    """tests/physics/swave_annulus_solenoid_gauge_test.cu:37-134: s-wave
+    annulus with outer radius 20 xi0 and inner radius 10 xi0 at 3.5
+    points/xi0, 16 angles, T = 0.2, cutoff 16, the solenoid gauge, charge sign
+    -1, no vector potential, L-infinity residuals, criterion 1e-4,
+    Barzilai-Borwein; the initial order parameter winds once."""
+    return {
+        "physics": {"temperature": 0.2, "external_flux_quanta": flux_quanta, "penetration_depth": -1.0,
+                    "charge_sign": -1, "gauge": "solenoid", "crystal_axes_rotation": 0.0,
+                    "order_parameter": {"s": {"critical_temperature": 1.0}}},
+        "geometry": [{"disc": {"add": True, "radius": 20.0, "center_x": 0.0, "center_y": 0.0}},
+                     {"disc": {"add": False, "radius": 10.0, "center_x": 0.0, "center_y": 0.0}}],
+        "numerics": {"points_per_coherence_length": 3.5, "num_fermi_momenta": 16,
+                     "energy_cutoff": 16.0, "convergence_criterion": 1e-4, "norm": "linf"},
+        "accelerator": {"name": "barzilai-borwein"},
+    }
+
+
+def solenoid_annulus_free_energy(flux_quanta: float, bulk_gap: float, bulk_free_energy: float,
+                                 yoshida: float, charge_winding: float = -1.0) -> float:
+    """The expected free energy per area of the solenoid-gauge annulus
+    (tests/physics/swave_annulus_solenoid_gauge_test.cu:138-160): the bulk
+    value plus the kinetic term Y ln(R/r) / (4 (R^2 - r^2)) (Phi - q w)^2 with
+    R = 20 and r = 10."""
+    outer, inner = 20.0, 10.0
+    factor = 0.25 * yoshida * math.log(outer / inner) / (outer * outer - inner * inner)
+    return bulk_free_energy + factor * (flux_quanta - charge_winding) ** 2
+
+
+SOLENOID_FLUXES = (-1.5, -1.0, -0.5)
+
+
 def bulk_dos(energy: np.ndarray, broadening: float, delta: float, swave: bool, n_angles: int) -> np.ndarray:
     """The expected DOS of tests/physics/dos_test.cu:168-198: sum over the
     circle's angles of w_k Im[e / sqrt(|eta_k delta|^2 - e^2)], e = E + i delta_b,

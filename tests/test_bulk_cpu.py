@@ -75,6 +75,18 @@ def test_library_matches_oracle():
         assert abs(sb.bulk_free_energy_s_wave(t, d) - O.bulk_free_energy_s_wave(t, d)) <= 1e-13 * abs(O.bulk_free_energy_s_wave(t, d)), t
 
 
+def test_yoshida_library_matches_oracle():
+    # computeYoshidaBulkSWave: 1 at zero temperature, the oracle's sum elsewhere.
+    from oracle import oracle as O
+    import superconga_b200 as sb
+    assert sb.bulk_yoshida_s_wave(0.0, 0.3, 16.0) == 1.0
+    for t in (0.05, 0.1, 0.5, 0.9):
+        d = O.bulk_s_wave(t)
+        y = O.bulk_yoshida_s_wave(t, d, 16.0)
+        assert 0.0 < y < 1.0
+        assert abs(sb.bulk_yoshida_s_wave(t, d, 16.0) - y) <= 1e-13 * y, t
+
+
 def test_invalid_arguments_rejected():
     import superconga_b200 as sb
     from superconga_b200 import _lib

@@ -180,6 +180,120 @@ def test_low_temperature_bulk_values(O, case):
     assert fe == pytest.approx(-0.5 * expected * expected, rel=1e-4)
 
 
+def phase_gradient_signs_ok(delta_x: np.ndarray, current: np.ndarray, expected_sign: int) -> bool:
+    """tests/physics/current_phase_gradient_test.cu:80-117: the products
+    j_x d_x(phi) and j_y d_y(phi) of the current with the phase gradient of the
+    order parameter never take the sign opposite to q * sign(winding) (zero is
+    allowed)."""
+    grad = configs.complex_phase_gradient(delta_x[0, 0], delta_x[0, 1])
+    for i in range(2):
+        overlap = current[i] * grad[i]
+        if np.sign(overlap.min()) == -expected_sign or np.sign(overlap.max()) == -expected_sign:
+            return False
+    return True
+
+
+def test_current_follows_phase_gradient(O):
+    """tests/physics/current_phase_gradient_test.cu:22-122 (double): one
+    iteration from a phase winding of +1; with charge sign -1 the current runs
+    against the phase gradient at every site."""
+    cfg = configs.phase_gradient_disc()
+    o = O.Oracle(cfg)
+    s = o.setup
+    d = configs.phase_winding_state(s.n0, O.delta_bulk(0.9, "s"), 1.0)
+    o.set_state(d, np.zeros((2, s.n0, s.n0)))
+    o.compute()
+    _, current, _ = o.results()
+    x = o.state()[0]
+    assert np.max(np.abs(current)) > 0.0
+    assert phase_gradient_signs_ok(x, current, -1)
+    # A planted sign error in the current must be caught.
+    assert not phase_gradient_signs_ok(x, -current, -1)
+
+
+def test_penetration_depth(O):
+    """tests/physics/penetration_depth_test.cu:89-179 (double): the disc in
+    half a flux quantum converges within 100 iterations, and the penetration
+    depth fitted to its flux by the London expression is lambda = 1 within
+    the reference's 0.1 (doctest scale 0)."""
+    cfg = configs.penetration_depth_disc()
+    o = O.Oracle(cfg)
+    s = o.setup
+    d = np.zeros((1, 2, s.n0, s.n0))
+    d[0, 0] = O.delta_bulk(0.1, "s")
+    o.set_state(d, np.zeros((2, s.n0, s.n0)))
+    converged = False
+    for _ in range(100):
+        o.compute()
+        if o.is_converged():
+            converged = True
+            break
+    lam = configs.penetration_depth_from_state(o.state()[1], o.domain(), 0.2, 0.5, 20.0, 1.0)
+    assert converged
+    assert abs(lam - 1.0) < 0.1 * max(abs(lam), 1.0), lam
+
+
+LINEAR_RESPONSE_A = 0.01
+
+
+def linear_response_check(current: np.ndarray, temperature: float, yoshida) -> None:
+    """tests/physics/current_linear_response_test.cu:25-40,117-150: the current
+    at the middle site of the square is -Y(T) A for a uniform vector potential
+    A = (0.01, 0.01), with Y the bulk Yoshida function at the bulk gap (cutoff
+    16), within 1 % (doctest scale 0)."""
+    from oracle.oracle import bulk_s_wave
+    n = current.shape[-1]
+    mid = current[:, n // 2, n // 2]
+    expected = -yoshida(temperature, bulk_s_wave(temperature), 16.0) * LINEAR_RESPONSE_A
+    for c in range(2):
+        assert abs(mid[c] - expected) < 0.01 * max(abs(mid[c]), abs(expected)), (c, mid[c], expected)
+
+
+@pytest.mark.parametrize("temperature", [0.1, 0.9])
+def test_current_linear_response(O, temperature):
+    """tests/physics/current_linear_response_test.cu (double), on the oracle."""
+    o = O.Oracle(configs.linear_response_square(temperature))
+    s = o.setup
+    d = np.zeros((1, 2, s.n0, s.n0))
+    d[0, 0] = O.delta_bulk(temperature, "s")
+    o.set_state(d, np.full((2, s.n0, s.n0), LINEAR_RESPONSE_A))
+    o.compute()
+    linear_response_check(o.results()[1], temperature, O.bulk_yoshida_s_wave)
+
+
+def solenoid_annulus_check(free_energies, converged, bulk) -> None:
+    """tests/physics/swave_annulus_solenoid_gauge_test.cu:136-173: each flux's
+    free energy within 1e-3 (doctest scale 0) of the parabola in Phi - q w,
+    every run converged, and the minimum at Phi = q w."""
+    op, fe, yoshida = bulk
+    d = op(0.2)
+    f_bulk, y = fe(0.2, d), yoshida(0.2, d, 16.0)
+    for flux, f in zip(configs.SOLENOID_FLUXES, free_energies):
+        expected = configs.solenoid_annulus_free_energy(flux, d, f_bulk, y)
+        assert abs(f - expected) < 1e-3 * max(abs(f), abs(expected)), (flux, f, expected)
+    assert all(converged)
+    assert free_energies[1] < free_energies[0] and free_energies[1] < free_energies[2]
+
+
+def test_solenoid_annulus_free_energy(O):
+    """tests/physics/swave_annulus_solenoid_gauge_test.cu (double), on the
+    oracle: three fluxes around the winding's own, 100 iterations at most."""
+    fes, conv = [], []
+    for flux in configs.SOLENOID_FLUXES:
+        o = O.Oracle(configs.solenoid_annulus(flux))
+        s = o.setup
+        o.set_state(configs.phase_winding_state(s.n0, O.bulk_s_wave(0.2), 1.0), np.zeros((2, s.n0, s.n0)))
+        ok = False
+        for _ in range(100):
+            o.compute()
+            if o.is_converged():
+                ok = True
+                break
+        fes.append(o.scalars()["free_energy_per_area"])
+        conv.append(ok)
+    solenoid_annulus_check(fes, conv, (O.bulk_s_wave, O.bulk_free_energy_s_wave, O.bulk_yoshida_s_wave))
+
+
 def test_free_energy_component_order(O):
     """tests/free_energy_test.cu:144-169: the free energy does not depend on
     the order of the order-parameter components (s with Tc 0.1 and d_xy with

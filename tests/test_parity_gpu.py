@@ -284,6 +284,123 @@ def test_low_temperature_bulk_values(engine_lib, case, mode):
     e.close()
 
 
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+def test_current_follows_phase_gradient(engine_lib, mode):
+    """tests/physics/current_phase_gradient_test.cu:22-122 on the engine: one
+    iteration from a phase winding of +1 (charge sign -1); the current runs
+    against the phase gradient at every site, and FP64 matches the oracle."""
+    from oracle import oracle as O
+    import superconga_b200 as sb
+    from tests.test_oracle_golden import phase_gradient_signs_ok
+    cfg = configs.phase_gradient_disc()
+    e = sb.Context(cfg, mode=mode)
+    n0 = e.dims.n0
+    d = configs.phase_winding_state(n0, O.delta_bulk(0.9, "s"), 1.0)
+    e.set_state(d, np.zeros((2, n0, n0)))
+    e.compute(1)
+    _, current, _ = e.results()
+    x = e.state()[0]
+    assert np.max(np.abs(current)) > 0.0
+    assert phase_gradient_signs_ok(x, current, -1)
+    if mode == "fp64":
+        o = O.Oracle(cfg)
+        o.set_state(d, np.zeros((2, n0, n0)))
+        o.compute()
+        assert _rel(current, o.results()[1]) < TOL
+        assert _rel(x, o.state()[0]) < TOL
+    e.close()
+
+
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+def test_penetration_depth(engine_lib, mode):
+    """tests/physics/penetration_depth_test.cu:89-179 on the engine: converged
+    within 100 iterations and the London-fitted penetration depth within 0.1
+    of lambda = 1; FP64 takes the oracle's iterations and ends on its vector
+    potential (1e-10)."""
+    from oracle import oracle as O
+    import superconga_b200 as sb
+    cfg = configs.penetration_depth_disc()
+    e = sb.Context(cfg, mode=mode)
+    n0 = e.dims.n0
+    d = np.zeros((1, 2, n0, n0))
+    d[0, 0] = O.delta_bulk(0.1, "s")
+    e.set_state(d, np.zeros((2, n0, n0)))
+    it, conv = e.run(0, 100)
+    a = e.state()[1]
+    lam = configs.penetration_depth_from_state(a, e.domain(), 0.2, 0.5, 20.0, 1.0)
+    assert conv
+    assert abs(lam - 1.0) < 0.1 * max(abs(lam), 1.0), lam
+    if mode == "fp64":
+        o = O.Oracle(cfg)
+        o.set_state(d, np.zeros((2, n0, n0)))
+        n = 0
+        while n < 100:
+            o.compute()
+            n += 1
+            if o.is_converged():
+                break
+        assert n == it
+        assert _rel(a, o.state()[1]) < TOL
+    e.close()
+
+
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+@pytest.mark.parametrize("temperature", [0.1, 0.9])
+def test_current_linear_response(engine_lib, temperature, mode):
+    """tests/physics/current_linear_response_test.cu on the engine: one
+    iteration in a uniform vector potential (0.01, 0.01); the middle current
+    is -Y(T) A within 1 %, and FP64 matches the oracle's current."""
+    from oracle import oracle as O
+    import superconga_b200 as sb
+    from tests.test_oracle_golden import LINEAR_RESPONSE_A, linear_response_check
+    cfg = configs.linear_response_square(temperature)
+    e = sb.Context(cfg, mode=mode)
+    n0 = e.dims.n0
+    d = np.zeros((1, 2, n0, n0))
+    d[0, 0] = O.delta_bulk(temperature, "s")
+    a = np.full((2, n0, n0), LINEAR_RESPONSE_A)
+    e.set_state(d, a)
+    e.compute(1)
+    current = e.results()[1]
+    linear_response_check(current, temperature, sb.bulk_yoshida_s_wave)
+    if mode == "fp64":
+        o = O.Oracle(cfg)
+        o.set_state(d, a)
+        o.compute()
+        assert _rel(current, o.results()[1]) < TOL
+    e.close()
+
+
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+def test_solenoid_annulus_free_energy(engine_lib, mode):
+    """tests/physics/swave_annulus_solenoid_gauge_test.cu on the engine: the
+    free energy per area of the once-winding annulus is the parabola in the
+    flux about Phi = q w (1e-3), and FP64 ends on the oracle's free energy."""
+    from oracle import oracle as O
+    import superconga_b200 as sb
+    from tests.test_oracle_golden import solenoid_annulus_check
+    fes, conv = [], []
+    for flux in configs.SOLENOID_FLUXES:
+        cfg = configs.solenoid_annulus(flux)
+        e = sb.Context(cfg, mode=mode)
+        n0 = e.dims.n0
+        d = configs.phase_winding_state(n0, O.bulk_s_wave(0.2), 1.0)
+        e.set_state(d, np.zeros((2, n0, n0)))
+        it, ok = e.run(0, 100)
+        fes.append(e.scalars()["free_energy_per_area"])
+        conv.append(ok)
+        e.close()
+        if mode == "fp64":
+            o = O.Oracle(cfg)
+            o.set_state(d, np.zeros((2, n0, n0)))
+            for _ in range(it):
+                o.compute()
+            so = o.scalars()["free_energy_per_area"]
+            assert abs(fes[-1] - so) <= TOL * abs(so), (flux, fes[-1], so)
+    solenoid_annulus_check(fes, conv, (sb.bulk_order_parameter_s_wave, sb.bulk_free_energy_s_wave,
+                                       sb.bulk_yoshida_s_wave))
+
+
 def test_mixed_precision(engine_lib):
     """FP32 stepping with FP64 accumulation against the FP64 form after five
     iterations: |Delta - Delta_FP64| / Delta_bulk <= 1e-5."""
