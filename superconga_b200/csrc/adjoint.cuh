@@ -844,8 +844,9 @@ int sc_adjoint(sc_ctx *ctx, double w_omega, const double *beta_j, double *g_delt
     ctx->err = "sc_adjoint: FP64 self-consistency contexts only";
     return SC_ERR_STATE;
   }
-  if (ctx->ept > 4) {
-    ctx->err = "sc_adjoint: more than four energies per thread";
+  if (ctx->ept > 4 || ctx->e_pass < ctx->S.ne) {
+    ctx->err = ctx->e_pass < ctx->S.ne ? "sc_adjoint: at most 64 Ozaki energies"
+                                       : "sc_adjoint: more than four energies per thread";
     return SC_ERR_STATE;
   }
   if (!ctx->boundary_initialized) {

@@ -55,6 +55,10 @@ struct EngineError {
 };
 
 constexpr int REDUCE_THREADS = 256;
+// Ozaki energies one sweep pass takes (the residues sit in shared memory);
+// more are swept in passes of ENERGY_PASS (eight threads of four energies).
+constexpr int SWEEP_MAX_ENERGIES = 64;
+constexpr int ENERGY_PASS = 32;
 constexpr int NQ = 48;  // partial-sum slots of the finalize reduction
 
 // ------------------------------------------------------------------ kernels --
@@ -111,6 +115,8 @@ __device__ __forceinline__ double2 as_d2(float2 v) { return make_double2(v.x, v.
 template <typename R>
 struct SweepArgs {
   int n0, n1, ne, nc, groups, log_groups, ept, n_items;
+  int ne_stride;   // energies per boundary entry (all of them; ne counts this pass's)
+  int accumulate;  // add the pass's Matsubara sums to the frame instead of storing them
   int burn_in, has_vp, has_ext, gauge;
   int slot_base;
   int pair;  // angle offset of the mirrored partner angle (n_angles / 2), 0 = unpaired
@@ -377,12 +383,12 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
         const R din = entry ? (R)A.dist_in_gt[in_base + nin] : R(0);
         const R dout = exit ? (R)A.dist_out_gt[out_base + nout] : R(0);
         site_step<R, EMAX, KEL>(l, 3, 2, dre, dim, es, pdre, pdim, pes, ere, eim, coh, A.ept, ecount, h,
-                                din, A.bin_gt + (size_t)(in_base + nin) * ne + e0, dout,
-                                A.bout_gt + (size_t)(out_base + nout) * ne + e0);
+                                din, A.bin_gt + (size_t)(in_base + nin) * A.ne_stride + e0, dout,
+                                A.bout_gt + (size_t)(out_base + nout) * A.ne_stride + e0);
         if (A.pair && exit) {
           // gamma of the partner angle at its exit is conj(gammaTilde) here.
-          const Cx<R> *src = A.bout_gt + (size_t)(out_base + nout) * ne + e0;
-          Cx<R> *dst = A.bout_g + (size_t)(A.idx_out_g[pax] + nout) * ne + e0;
+          const Cx<R> *src = A.bout_gt + (size_t)(out_base + nout) * A.ne_stride + e0;
+          Cx<R> *dst = A.bout_g + (size_t)(A.idx_out_g[pax] + nout) * A.ne_stride + e0;
 #pragma unroll
           for (int j = 0; j < EMAX; ++j)
             if (j < ecount) dst[j] = Cx<R>{src[j].re, -src[j].im};
@@ -447,12 +453,12 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
         const R din = entry ? (R)A.dist_in_g[in_base + nin] : R(0);
         const R dout = exit ? (R)A.dist_out_g[out_base + nout] : R(0);
         site_step<R, EMAX, KEL>(l, 2, 3, dre, dim, es, pdre, pdim, pes, ere, eim, coh, A.ept, ecount, h,
-                                din, A.bin_g + (size_t)(in_base + nin) * ne + e0, dout,
-                                A.bout_g + (size_t)(out_base + nout) * ne + e0);
+                                din, A.bin_g + (size_t)(in_base + nin) * A.ne_stride + e0, dout,
+                                A.bout_g + (size_t)(out_base + nout) * A.ne_stride + e0);
         if (A.pair && exit) {
           // gammaTilde of the partner angle at its exit is conj(gamma) here.
-          const Cx<R> *src = A.bout_g + (size_t)(out_base + nout) * ne + e0;
-          Cx<R> *dst = A.bout_gt + (size_t)(A.idx_out_gt[pax] + nout) * ne + e0;
+          const Cx<R> *src = A.bout_g + (size_t)(out_base + nout) * A.ne_stride + e0;
+          Cx<R> *dst = A.bout_gt + (size_t)(A.idx_out_gt[pax] + nout) * A.ne_stride + e0;
 #pragma unroll
           for (int j = 0; j < EMAX; ++j)
             if (j < ecount) dst[j] = Cx<R>{src[j].re, -src[j].im};
@@ -495,15 +501,29 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
       const int lg = A.log_groups;
       group_sum4_scatter(v, g, lg, gmask);
       if (lg == 0) {
+        if (A.accumulate) {
+          const double2 of = as_d2(fg[fi]), og = as_d2(gi[fi]);
+          v[0] += of.x;
+          v[1] += of.y;
+          v[2] += og.x;
+          v[3] += og.y;
+        }
         fg[fi] = frame_pair<Fr>(v[0], v[1]);
         gi[fi] = frame_pair<Fr>(v[2], v[3]);
       } else if (lg == 1) {
-        (g ? gi : fg)[fi] = frame_pair<Fr>(v[0], v[1]);
+        Fr *dst = (g ? gi : fg) + fi;
+        if (A.accumulate) {
+          const double2 o = as_d2(*dst);
+          v[0] += o.x;
+          v[1] += o.y;
+        }
+        *dst = frame_pair<Fr>(v[0], v[1]);
       } else {
         const int sh = lg - 2;  // low bits below the two value bits
         if ((g & ((1 << sh) - 1)) == 0) {
           const int k = g >> sh;  // value index 0..3
           auto *dst = &((k < 2 ? fg : gi) + fi)->x;
+          if (A.accumulate) v[0] += (double)dst[k & 1];
           dst[k & 1] = (decltype(Fr::x))v[0];
         }
       }
@@ -513,8 +533,8 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
 
 template <typename R, int EMAX, int MINB, bool KEL, bool STEP_PER_ANGLE = false>
 __global__ void __launch_bounds__(128, MINB) k_sweep(const SweepArgs<R> A) {
-  __shared__ double s_res[64];  // residues (at most 64 energies)
-  for (int e = threadIdx.x; e < A.ne && e < 64; e += blockDim.x) s_res[e] = A.res[e];
+  __shared__ double s_res[SWEEP_MAX_ENERGIES];  // residues of this pass's energies
+  for (int e = threadIdx.x; e < A.ne && e < SWEEP_MAX_ENERGIES; e += blockDim.x) s_res[e] = A.res[e];
   __syncthreads();
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int item = tid >> A.log_groups;
@@ -1505,6 +1525,10 @@ struct sc_ctx {
   DevArray<int> onode_a_g, onode_x_g, onode_y_g, onode_a_gt, onode_x_gt, onode_y_gt;
   std::vector<Chunk> chunks;
   int groups = 1, log_groups = 0, ept = 1;
+  // Ozaki energies per sweep pass: all of them up to SWEEP_MAX_ENERGIES; above
+  // that the sweep runs in passes of ENERGY_PASS energies that add into the
+  // frame sums (low temperatures: T = 0.001 at cutoff 32 takes 281 energies).
+  int e_pass = 1;
   bool emax2 = false;  // two-energies-per-thread sweep variant (tuning)
   int pair = 0;  // > 0: mixed mode sweeps angles [0, n/2) and mirrors them onto [n/2, n)
 
@@ -1599,6 +1623,7 @@ SweepArgs<R> sweep_args(sc_ctx *c, const Chunk *ch, int burn_in) {
   A.n0 = S.n0;
   A.n1 = S.n1;
   A.ne = S.ne;
+  A.ne_stride = S.ne;
   A.nc = S.nc;
   A.groups = c->groups;
   A.log_groups = c->log_groups;
@@ -1652,13 +1677,7 @@ void launch_frame_fields(sc_ctx *c, const Chunk &ch, const SweepArgs<R> &A) {
 }
 
 template <typename R>
-void launch_sweep(sc_ctx *c, const Chunk &ch, int burn_in) {
-  SweepArgs<R> A = sweep_args<R>(c, &ch, burn_in);
-  const size_t threads = (size_t)A.n_items * c->groups;
-  if (!threads) return;
-  const unsigned blocks = grid1(threads, 128);
-  launch_frame_fields<R>(c, ch, A);
-  ProfScope prof(c, 0);
+void launch_sweep_pass(sc_ctx *c, const SweepArgs<R> &A, unsigned blocks) {
   // Resident blocks per SM, fastest measured on B200 (606 x 606 d-wave square,
   // 256 angles, 14 energies): FP64 three (four energies per thread, 158
   // registers, no spills: 35.4 ms against 36.3 with four blocks), mixed four
@@ -1696,6 +1715,36 @@ void launch_sweep(sc_ctx *c, const Chunk &ch, int burn_in) {
     k_sweep<R, 16, 1, false><<<blocks, 128, 0, c->stream>>>(A);
   }
   check_launch(c);
+}
+
+template <typename R>
+void launch_sweep(sc_ctx *c, const Chunk &ch, int burn_in) {
+  SweepArgs<R> A = sweep_args<R>(c, &ch, burn_in);
+  const size_t threads = (size_t)A.n_items * c->groups;
+  if (!threads) return;
+  const unsigned blocks = grid1(threads, 128);
+  launch_frame_fields<R>(c, ch, A);
+  ProfScope prof(c, 0);
+  const int ne = c->S.ne, pass = c->e_pass;
+  if (pass >= ne) {
+    launch_sweep_pass<R>(c, A, blocks);
+    return;
+  }
+  // Energy passes: each pass steps energies [e, e + pass) of every column
+  // from their own boundary values and adds its Matsubara sums to the frame.
+  for (int e = 0; e < ne; e += pass) {
+    SweepArgs<R> P = A;
+    P.ne = std::min(pass, ne - e);
+    P.accumulate = e > 0;
+    P.e_re += e;
+    P.e_im += e;
+    P.res += e;
+    P.bin_g += e;
+    P.bout_g += e;
+    P.bin_gt += e;
+    P.bout_gt += e;
+    launch_sweep_pass<R>(c, P, blocks);
+  }
 }
 
 void extend_reference(sc_ctx *c) {
@@ -2121,7 +2170,7 @@ void plan_chunks(sc_ctx *c, std::vector<int4> &items) {
   if (const char *env = std::getenv("SCB_SCRATCH_MB")) budget_mb = std::atof(env);
   // A batch grain sweeps all its angles in one chunk (the batch pools memory).
   const double budget = c->batch_member ? 1e300 : budget_mb * 1048576.0;
-  const size_t per_row = (size_t)S.ne * c->esize() + 3 * sizeof(double);
+  const size_t per_row = (size_t)c->e_pass * c->esize() + 3 * sizeof(double);
   const size_t frame_slot = S.keldysh ? (size_t)n1 * n1 * S.ne * sizeof(double)
                                       : (size_t)n1 * n1 * 2 * sizeof(double2);
   items.clear();
@@ -2279,6 +2328,7 @@ void upload_static(sc_ctx *c) {
     }
     if (ok) c->pair = na / 2;
   }
+  c->e_pass = (S.keldysh || S.ne <= SWEEP_MAX_ENERGIES) ? S.ne : ENERGY_PASS;
   std::vector<int4> items;
   plan_chunks(c, items);
   c->items.upload(items, s);
@@ -2295,7 +2345,7 @@ void upload_static(sc_ctx *c) {
   int want = 1;
   if (eg) want = std::atoi(eg);
   else {
-    while ((S.ne + want - 1) / want > per_thread && want < 8) want *= 2;
+    while ((c->e_pass + want - 1) / want > per_thread && want < 8) want *= 2;
     // Small grains: too few trajectory columns to fill the GPU twice over,
     // so spread the energies over more threads per column.
     int dev = 0, n_sm = 148;
@@ -2304,13 +2354,13 @@ void upload_static(sc_ctx *c) {
     const double resident = (double)n_sm * (fp32_sweep ? 4 : 3) * 128;
     size_t max_items = 0;
     for (const Chunk &ch : c->chunks) max_items = std::max(max_items, (size_t)(ch.item_end - ch.item_begin));
-    while ((double)max_items * want < 2.0 * resident && want < 8 && (S.ne + want - 1) / want > 1) want *= 2;
+    while ((double)max_items * want < 2.0 * resident && want < 8 && (c->e_pass + want - 1) / want > 1) want *= 2;
   }
   while (c->groups < want && c->groups < 8) {
     c->groups *= 2;
     c->log_groups++;
   }
-  c->ept = (S.ne + c->groups - 1) / c->groups;
+  c->ept = (c->e_pass + c->groups - 1) / c->groups;
   if (c->ept > 16) throw EngineError(SC_ERR_ARG, "too many Ozaki energies per thread");
   c->emax2 = fp32_sweep ? !std::getenv("SCB_SWEEP_EMAX4") : std::getenv("SCB_SWEEP_EMAX2") != nullptr;
 
@@ -2339,7 +2389,7 @@ void upload_static(sc_ctx *c) {
   int max_slots = 1;
   for (const Chunk &ch : c->chunks) {
     const size_t ni = (size_t)(ch.item_end - ch.item_begin);
-    scr = std::max(scr, ni * ch.kmax * S.ne * c->esize());
+    scr = std::max(scr, ni * ch.kmax * c->e_pass * c->esize());
     scr2 = std::max(scr2, ni * ch.kmax * 3);
     max_slots = std::max(max_slots, chunk_slots(c, ch));
   }
@@ -2439,9 +2489,7 @@ int create_context(int mode, sc_ctx **out, F make) {
     const std::string e = make(c->S);
     if (!e.empty()) throw EngineError(SC_ERR_ARG, e);
     if (c->S.nc > MAX_COMP) throw EngineError(SC_ERR_ARG, "at most 4 order-parameter components");
-    if (c->S.ne > 64)
-      throw EngineError(SC_ERR_ARG, c->S.keldysh ? "at most 64 energies per LDOS block"
-                                                 : "at most 64 Ozaki energies (raise the temperature or lower the cutoff)");
+    if (c->S.keldysh && c->S.ne > SWEEP_MAX_ENERGIES) throw EngineError(SC_ERR_ARG, "at most 64 energies per LDOS block");
     if (2 * c->S.nc + 2 > 16) throw EngineError(SC_ERR_ARG, "too many accelerator fields");
     CUDA_TRY(cudaGetDevice(&c->device));
     CUDA_TRY(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
