@@ -424,6 +424,94 @@ def solenoid_annulus_free_energy(flux_quanta: float, bulk_gap: float, bulk_free_
 SOLENOID_FLUXES = (-1.5, -1.0, -0.5)
 
 
+def radial_annulus() -> dict:
+    """tests/physics/swave_annulus_radial_gauge_test.cu:345-425: s-wave annulus
+    with outer radius 20 xi0 and inner radius 10 xi0 at 6.2 points/xi0, 32
+    angles, T = 0.2, cutoff 16, one flux quantum, lambda = 30 with a
+    self-consistent vector potential (error 1e-3), symmetric gauge, charge
+    sign -1, L-infinity residuals, criterion 1e-4, Barzilai-Borwein; the
+    initial order parameter winds -2 times (q w = 2)."""
+    return {
+        "physics": {"temperature": 0.2, "external_flux_quanta": 1.0, "penetration_depth": 30.0,
+                    "charge_sign": -1, "gauge": "symmetric", "crystal_axes_rotation": 0.0,
+                    "order_parameter": {"s": {"critical_temperature": 1.0}}},
+        "geometry": [{"disc": {"add": True, "radius": 20.0, "center_x": 0.0, "center_y": 0.0}},
+                     {"disc": {"add": False, "radius": 10.0, "center_x": 0.0, "center_y": 0.0}}],
+        "numerics": {"points_per_coherence_length": 6.2, "num_fermi_momenta": 32,
+                     "energy_cutoff": 16.0, "convergence_criterion": 1e-4, "norm": "linf",
+                     "vector_potential_error": 1e-3},
+        "accelerator": {"name": "barzilai-borwein"},
+    }
+
+
+def _annulus_factors(outer, inner, lam_t, flux, winding, charge):
+    """The London solution of a thick annulus in the radial gauge
+    (tests/physics/swave_annulus_radial_gauge_test.cu:96-150): the
+    coefficients a, b of B = a I0(r/k) - b K0(r/k) in the grain and the
+    fluxoid coefficient c, with k = lam_t the temperature-dependent
+    penetration depth and the pi of the flux unit A0 = Phi0 / (pi xi0)."""
+    from scipy.special import iv, kv
+    hole = math.pi * inner * inner
+    grain = math.pi * outer * outer - hole
+    big, small = outer / lam_t, inner / lam_t
+    qw = charge * winding
+    inv_m = math.pi / (iv(0, big) * kv(2, small) - iv(2, small) * kv(0, big))
+    a = inv_m * (flux * kv(2, small) / grain - qw * kv(0, big) / hole)
+    b = inv_m * (flux * iv(2, small) / grain - qw * iv(0, big) / hole)
+    c = inv_m * (2.0 * math.pi * lam_t * lam_t * flux / grain
+                 + qw * (iv(0, big) * kv(0, small) - iv(0, small) * kv(0, big)))
+    return a, b, c, grain, hole
+
+
+def annulus_analytic(outer, inner, lam, flux, winding, charge, temperature, cutoff, bulk):
+    """Expected free energy per area, magnetic free energy per area and
+    magnetic moment per area of the annulus
+    (tests/physics/swave_annulus_radial_gauge_test.cu:152-337): bulk energy
+    plus the kinetic and magnetic London terms, integrated over the grain by
+    32-point Gauss-Legendre quadrature, plus the field energy in the hole; the
+    moment in closed form.  ``bulk`` = (gap(T), free energy(T, gap),
+    Yoshida(T, gap, cutoff))."""
+    from scipy.special import iv, kv
+    op_fn, fe_fn, y_fn = bulk
+    d = op_fn(temperature)
+    f_bulk = fe_fn(temperature, d)
+    k = lam / math.sqrt(y_fn(temperature, d, cutoff))
+    a, b, c, grain, hole = _annulus_factors(outer, inner, k, flux, winding, charge)
+    scale = 2.0 * math.pi * lam * lam / (2.0 * grain)
+    b_ext = math.pi * flux / grain
+    x, w = np.polynomial.legendre.leggauss(32)
+    r = 0.5 * (outer - inner) * x + 0.5 * (outer + inner)
+    w = 0.5 * (outer - inner) * w
+    mag = scale * np.sum(w * r * (a * iv(0, r / k) - b * kv(0, r / k) - b_ext) ** 2)
+    mag += scale * 0.5 * ((c / hole - b_ext) * inner) ** 2
+    kin = scale * np.sum(w * r * (a * iv(1, r / k) + b * kv(1, r / k)) ** 2)
+    moment = annulus_moment(outer, inner, lam, flux, winding, charge, temperature, cutoff, (op_fn, y_fn))
+    return f_bulk + kin + mag, mag, moment
+
+
+def annulus_moment(outer, inner, lam, flux, winding, charge, temperature, cutoff, bulk):
+    """The closed-form magnetic moment per area of the annulus
+    (tests/physics/swave_annulus_radial_gauge_test.cu:152-205); ``bulk`` =
+    (gap(T), Yoshida(T, gap, cutoff))."""
+    from scipy.special import iv, kv
+    op_fn, y_fn = bulk
+    d = op_fn(temperature)
+    k = lam / math.sqrt(y_fn(temperature, d, cutoff))
+    a, b, _, grain, _ = _annulus_factors(outer, inner, k, flux, winding, charge)
+    scale = 2.0 * math.pi * lam * lam / (2.0 * grain)
+    return -scale * (outer * outer * (a * iv(2, outer / k) - b * kv(2, outer / k))
+                     - inner * inner * (a * iv(2, inner / k) - b * kv(2, inner / k)))
+
+
+def magnetic_moment(current: np.ndarray, h: float, n_grain: int) -> float:
+    """GridFunctions::moment (GridFunctions_GPU.h:602-616,726-754) per grain
+    area: 0.5 h^3 sum (x j_y - y j_x) over the lattice, x and y in sites from
+    its centre, divided by n_grain h^2."""
+    n = current.shape[-1]
+    c = np.arange(n, dtype=np.float64) - 0.5 * (n - 1)
+    return 0.5 * h ** 3 * float(np.sum(c[None, :] * current[1] - c[:, None] * current[0])) / (n_grain * h * h)
+
+
 def bulk_dos(energy: np.ndarray, broadening: float, delta: float, swave: bool, n_angles: int) -> np.ndarray:
     """The expected DOS of tests/physics/dos_test.cu:168-198: sum over the
     circle's angles of w_k Im[e / sqrt(|eta_k delta|^2 - e^2)], e = E + i delta_b,

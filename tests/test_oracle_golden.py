@@ -294,6 +294,61 @@ def test_solenoid_annulus_free_energy(O):
     solenoid_annulus_check(fes, conv, (O.bulk_s_wave, O.bulk_free_energy_s_wave, O.bulk_yoshida_s_wave))
 
 
+def test_annulus_magnetic_moment_expression():
+    """tests/physics/swave_annulus_radial_gauge_test.cu:470-557: at zero
+    temperature (Yoshida function 1) the moment of the London solution equals
+    its parts per flux quantum and per winding, which match the reference's
+    Mathematica values -0.1953280762339516 and -0.2336266542359196 (100 eps)."""
+    from scipy.special import iv, kv
+    from oracle.oracle import bulk_s_wave, bulk_yoshida_s_wave
+    outer, inner, lam, charge, flux, winding = 20.0, 10.0, 30.0, -1, 1.0, 2.0
+    big, small = outer / lam, inner / lam
+    hole = math.pi * inner * inner
+    grain = math.pi * outer * outer - hole
+    scale = 2.0 * math.pi * lam * lam / (2.0 * grain)
+    m = iv(0, big) * kv(2, small) - iv(2, small) * kv(0, big)
+    per_flux = scale * (hole + grain) * (iv(2, small) * kv(2, big) - iv(2, big) * kv(2, small)) / (m * grain)
+    per_winding = scale * (2.0 * math.pi * lam * lam / (m * hole) - 1.0)
+    total = per_flux * flux - per_winding * winding * charge
+    expected = configs.annulus_moment(outer, inner, lam, flux, winding, charge, 0.0, 100.0,
+                                      (bulk_s_wave, bulk_yoshida_s_wave))
+    eps = 100 * np.finfo(np.float64).eps
+    assert abs(total - expected) < eps * max(abs(total), abs(expected))
+    assert abs(per_flux + 0.1953280762339516) < eps * 0.1953280762339516
+    assert abs(per_winding + 0.2336266542359196) < eps * 0.2336266542359196
+
+
+def radial_annulus_check(fe, fe_mag, moment, converged, bulk) -> None:
+    """tests/physics/swave_annulus_radial_gauge_test.cu:427-466: free energy
+    and magnetic moment per area within 1e-3 of the London solution, the
+    magnetic free energy within 2e-2 (doctest scale 0), converged."""
+    f, fm, mom = configs.annulus_analytic(20.0, 10.0, 30.0, 1.0, -2.0, -1, 0.2, 16.0, bulk)
+    assert converged
+    assert abs(fe - f) < 1e-3 * max(abs(fe), abs(f)), (fe, f)
+    assert abs(fe_mag - fm) < 2e-2 * max(abs(fe_mag), abs(fm)), (fe_mag, fm)
+    assert abs(moment - mom) < 1e-3 * max(abs(moment), abs(mom)), (moment, mom)
+
+
+def test_radial_annulus(O):
+    """tests/physics/swave_annulus_radial_gauge_test.cu:345-466 (double) on the
+    oracle: the annulus with a self-consistent vector potential (N0 = 254)
+    converges within 100 iterations onto the London solution."""
+    cfg = configs.radial_annulus()
+    o = O.Oracle(cfg)
+    s = o.setup
+    o.set_state(configs.phase_winding_state(s.n0, O.bulk_s_wave(0.2), -2.0), np.zeros((2, s.n0, s.n0)))
+    converged = False
+    for _ in range(100):
+        o.compute()
+        if o.is_converged():
+            converged = True
+            break
+    sc = o.scalars()
+    moment = configs.magnetic_moment(o.results()[1], 1.0 / 6.2, int(sc["n_grain"]))
+    radial_annulus_check(sc["free_energy_per_area"], sc["magnetic_free_energy_per_area"], moment, converged,
+                         (O.bulk_s_wave, O.bulk_free_energy_s_wave, O.bulk_yoshida_s_wave))
+
+
 def test_free_energy_component_order(O):
     """tests/free_energy_test.cu:144-169: the free energy does not depend on
     the order of the order-parameter components (s with Tc 0.1 and d_xy with

@@ -411,6 +411,37 @@ def test_solenoid_annulus_free_energy(engine_lib, mode):
                                        sb.bulk_yoshida_s_wave))
 
 
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+def test_radial_annulus(engine_lib, mode):
+    """tests/physics/swave_annulus_radial_gauge_test.cu on the engine: free
+    energy, magnetic free energy and magnetic moment of the converged annulus
+    against the London solution (1e-3, 2e-2, 1e-3); FP64 follows the oracle's
+    first three iterations (1e-10)."""
+    from oracle import oracle as O
+    import superconga_b200 as sb
+    from tests.test_oracle_golden import radial_annulus_check
+    cfg = configs.radial_annulus()
+    e = sb.Context(cfg, mode=mode)
+    n0 = e.dims.n0
+    d = configs.phase_winding_state(n0, O.bulk_s_wave(0.2), -2.0)
+    e.set_state(d, np.zeros((2, n0, n0)))
+    if mode == "fp64":
+        o = O.Oracle(cfg)
+        o.set_state(d, np.zeros((2, n0, n0)))
+        for it in range(3):
+            o.compute()
+            e.compute(1)
+            assert _rel(e.state()[0], o.state()[0]) < TOL, it
+            assert _rel(e.state()[1], o.state()[1]) < TOL, it
+            assert _rel(e.results()[1], o.results()[1]) < TOL, it
+    _, conv = e.run(0, 100)
+    sc = e.scalars()
+    moment = configs.magnetic_moment(e.results()[1], 1.0 / 6.2, int(sc["n_grain"]))
+    radial_annulus_check(sc["free_energy_per_area"], sc["magnetic_free_energy_per_area"], moment, conv,
+                         (sb.bulk_order_parameter_s_wave, sb.bulk_free_energy_s_wave, sb.bulk_yoshida_s_wave))
+    e.close()
+
+
 def _many_energies_disc():
     """The small disc in a field with a self-consistent vector potential at
     T = 0.005 and cutoff 16: 89 Ozaki energies, more than one sweep pass
