@@ -349,6 +349,29 @@ def test_radial_annulus(O):
                          (O.bulk_s_wave, O.bulk_free_energy_s_wave, O.bulk_yoshida_s_wave))
 
 
+@pytest.mark.parametrize("disc", [True, False], ids=["disc", "square"])
+def test_grain_area(O, disc):
+    """tests/geometry_test.cu:131-183,210-231: a disc or a square of width 1
+    xi0 at 1000 points/xi0 covers pi/4 or 1 within 2/1000 (doctest scale 1),
+    the grain area being its lattice sites times h^2; the engine's host
+    set-up marks the same sites as the oracle."""
+    from superconga_b200.engine import Setup
+    geom = ({"disc": {"add": True, "radius": 0.5, "center_x": 0.0, "center_y": 0.0}} if disc else
+            {"regular_polygon": {"add": True, "num_edges": 4, "side_length": 1.0, "rotation": 0.0,
+                                 "center_x": 0.0, "center_y": 0.0}})
+    cfg = {"physics": {"temperature": 0.5, "external_flux_quanta": 0.0, "penetration_depth": -1.0,
+                       "charge_sign": -1, "gauge": "symmetric", "crystal_axes_rotation": 0.0,
+                       "order_parameter": {"s": {"critical_temperature": 1.0}}},
+           "geometry": [geom],
+           "numerics": {"points_per_coherence_length": 1000.0, "num_fermi_momenta": 4, "energy_cutoff": 4.0,
+                        "convergence_criterion": 1e-4, "norm": "linf"}}
+    grain = O.Oracle(cfg).domain() > 0
+    area = grain.sum() * 1e-6
+    expected = 0.25 * math.pi if disc else 1.0
+    assert abs(expected - area) < 2e-3 * (1.0 + max(area, expected)), (area, expected)
+    assert np.array_equal(Setup(cfg).domain() > 0, grain)
+
+
 def test_free_energy_component_order(O):
     """tests/free_energy_test.cu:144-169: the free energy does not depend on
     the order of the order-parameter components (s with Tc 0.1 and d_xy with
