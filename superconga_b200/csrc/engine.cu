@@ -3016,11 +3016,17 @@ struct sc_batch {
   std::vector<int> iterations;
   DevArray<double> pool;
   size_t pool_bytes = 0;
-  struct Wave {
-    std::vector<int> grains;
+  // One launch of the persistent sweep: the work units and SweepArgs<R> of
+  // the grains that take part (an energy pass of each grain with energies left).
+  struct Pass {
     DevArray<int2> units;
     int n_units = 0;
-    DevArray<unsigned char> args;  // SweepArgs<R> of the wave's grains
+    int ept = 0;  // largest energies per thread among the pass's grains
+    DevArray<unsigned char> args;
+  };
+  struct Wave {
+    std::vector<int> grains;
+    std::vector<std::unique_ptr<Pass>> passes;  // energy passes, swept one after another
   };
   std::vector<std::unique_ptr<Wave>> waves;
   DevArray<int> counters;
@@ -3101,34 +3107,60 @@ void batch_plan(sc_batch *b) {
   for (auto &m : members) {
     auto wv = std::make_unique<sc_batch::Wave>();
     wv->grains = m;
-    std::vector<SweepArgs<R>> args;
-    std::vector<std::pair<int, int2>> keyed;  // (column length, unit)
+    int n_passes = 1;
     for (int k = 0; k < (int)m.size(); ++k) {
       sc_ctx *c = b->grains[m[k]];
+      const int ne = c->e_pass;  // energies per pass: all of them up to 64, else 32
       c->log_groups = 0;
-      while (((c->S.ne + (1 << c->log_groups) - 1) >> c->log_groups) > b->ept_max && c->log_groups < 3)
+      while (((ne + (1 << c->log_groups) - 1) >> c->log_groups) > b->ept_max && c->log_groups < 3)
         c->log_groups++;
       c->groups = 1 << c->log_groups;
-      c->ept = (c->S.ne + c->groups - 1) / c->groups;
-      const int per_warp = 32 >> c->log_groups;
-      const Chunk &ch = c->chunks[0];
-      args.push_back(sweep_args<R>(c, &ch, 0));
-      const int n = ch.item_end - ch.item_begin;
-      const int4 *items = c->h_items.data() + ch.item_begin;
-      for (int i = 0; i < n; i += per_warp) {
-        int len = 0;
-        for (int j = i; j < std::min(n, i + per_warp); ++j) len = std::max(len, items[j].w - items[j].z + 1);
-        keyed.push_back({len, make_int2(k, i)});
-      }
+      c->ept = (ne + c->groups - 1) / c->groups;
+      n_passes = std::max(n_passes, (c->S.ne + ne - 1) / ne);
     }
-    std::stable_sort(keyed.begin(), keyed.end(), [](const auto &x, const auto &y) { return x.first > y.first; });
-    std::vector<int2> units;
-    for (auto &kv : keyed) units.push_back(kv.second);
-    wv->n_units = (int)units.size();
-    wv->units.upload(units, b->stream);
-    std::vector<unsigned char> raw(args.size() * sizeof(SweepArgs<R>));
-    std::memcpy(raw.data(), args.data(), raw.size());
-    wv->args.upload(raw, b->stream);
+    for (int p = 0; p < n_passes; ++p) {
+      wv->passes.push_back(std::make_unique<sc_batch::Pass>());
+      sc_batch::Pass &ps = *wv->passes.back();
+      std::vector<SweepArgs<R>> args;
+      std::vector<std::pair<int, int2>> keyed;  // (column length, unit)
+      for (int k = 0; k < (int)m.size(); ++k) {
+        sc_ctx *c = b->grains[m[k]];
+        const int e = p * c->e_pass;
+        if (e >= c->S.ne) continue;
+        const int per_warp = 32 >> c->log_groups;
+        const Chunk &ch = c->chunks[0];
+        SweepArgs<R> A = sweep_args<R>(c, &ch, 0);
+        if (c->e_pass < c->S.ne) {
+          A.ne = std::min(c->e_pass, c->S.ne - e);
+          A.accumulate = e > 0;
+          A.e_re += e;
+          A.e_im += e;
+          A.res += e;
+          A.bin_g += e;
+          A.bout_g += e;
+          A.bin_gt += e;
+          A.bout_gt += e;
+        }
+        const int slot = (int)args.size();
+        args.push_back(A);
+        ps.ept = std::max(ps.ept, c->ept);
+        const int n = ch.item_end - ch.item_begin;
+        const int4 *items = c->h_items.data() + ch.item_begin;
+        for (int i = 0; i < n; i += per_warp) {
+          int len = 0;
+          for (int j = i; j < std::min(n, i + per_warp); ++j) len = std::max(len, items[j].w - items[j].z + 1);
+          keyed.push_back({len, make_int2(slot, i)});
+        }
+      }
+      std::stable_sort(keyed.begin(), keyed.end(), [](const auto &x, const auto &y) { return x.first > y.first; });
+      std::vector<int2> units;
+      for (auto &kv : keyed) units.push_back(kv.second);
+      ps.n_units = (int)units.size();
+      ps.units.upload(units, b->stream);
+      std::vector<unsigned char> raw(args.size() * sizeof(SweepArgs<R>));
+      std::memcpy(raw.data(), args.data(), raw.size());
+      ps.args.upload(raw, b->stream);
+    }
     b->waves.push_back(std::move(wv));
   }
   b->counters.alloc(std::max<size_t>(1, b->waves.size()));
@@ -3138,33 +3170,35 @@ void batch_plan(sc_batch *b) {
 
 template <typename R>
 void launch_batch_sweep(sc_batch *b, sc_batch::Wave &w, int wi) {
-  const SweepArgs<R> *args = (const SweepArgs<R> *)w.args.p;
   int *counter = b->counters.p + wi;
-  CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(int), b->stream));
-  int ept = 0;
-  for (int g : w.grains) ept = std::max(ept, b->grains[g]->ept);
-  auto run = [&](auto kernel) {
-    int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 128, 0);
-    const int blocks = std::max(1, per_sm) * b->n_sm;
-    kernel<<<blocks, 128, 0, b->stream>>>(args, w.units.p, w.n_units, counter);
-  };
-  if (ept <= 2 && b->minb == 6) {
-    run(k_sweep_batch<R, 2, 6>);
-  } else if (ept <= 2 && b->minb == 4) {
-    run(k_sweep_batch<R, 2, 4>);
-  } else if (ept <= 4) {
-    if (b->minb == 4) run(k_sweep_batch<R, 4, 4>);
-    else if (b->minb == 3) run(k_sweep_batch<R, 4, 3>);
-    else run(k_sweep_batch<R, 4, 1>);
-  } else if (ept <= 8) {
-    run(k_sweep_batch<R, 8, 1>);
-  } else {
-    run(k_sweep_batch<R, 16, 1>);
+  for (auto &pp : w.passes) {
+    sc_batch::Pass &ps = *pp;
+    const SweepArgs<R> *args = (const SweepArgs<R> *)ps.args.p;
+    CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(int), b->stream));
+    const int ept = ps.ept;
+    auto run = [&](auto kernel) {
+      int per_sm = 1;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 128, 0);
+      const int blocks = std::max(1, per_sm) * b->n_sm;
+      kernel<<<blocks, 128, 0, b->stream>>>(args, ps.units.p, ps.n_units, counter);
+    };
+    if (ept <= 2 && b->minb == 6) {
+      run(k_sweep_batch<R, 2, 6>);
+    } else if (ept <= 2 && b->minb == 4) {
+      run(k_sweep_batch<R, 2, 4>);
+    } else if (ept <= 4) {
+      if (b->minb == 4) run(k_sweep_batch<R, 4, 4>);
+      else if (b->minb == 3) run(k_sweep_batch<R, 4, 3>);
+      else run(k_sweep_batch<R, 4, 1>);
+    } else if (ept <= 8) {
+      run(k_sweep_batch<R, 8, 1>);
+    } else {
+      run(k_sweep_batch<R, 16, 1>);
+    }
+    b->launches++;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) throw EngineError(SC_ERR_CUDA, std::string("batch sweep launch: ") + cudaGetErrorString(e));
   }
-  b->launches++;
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) throw EngineError(SC_ERR_CUDA, std::string("batch sweep launch: ") + cudaGetErrorString(e));
 }
 
 void batch_fork(sc_batch *b) {
@@ -3336,7 +3370,6 @@ int sc_batch_create(const char *const *configs, int n, int mode, sc_batch **out)
       const std::string &e = errs[i];
       if (!e.empty()) throw EngineError(SC_ERR_ARG, "grain " + std::to_string(i) + ": " + e);
       if (c->S.nc > MAX_COMP) throw EngineError(SC_ERR_ARG, "at most 4 order-parameter components");
-      if (c->S.ne > 32) throw EngineError(SC_ERR_ARG, "grain " + std::to_string(i) + ": at most 32 Ozaki energies in a batch");
       c->device = dev;
       c->stream = b->stream;
       upload_static(c);

@@ -151,3 +151,39 @@ def test_batch_vs_oracle(engine_lib):
             assert _rel(j_b, j_o) < 1e-10, it
             assert abs(g.scalars()["free_energy"] - o.scalars()["free_energy"]) <= 1e-10 * abs(o.scalars()["free_energy"])
     b.close()
+
+
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+def test_batch_low_temperature_grains(engine_lib, mode):
+    """A temperature sweep in one batch: the small disc at T = 0.5 (7 Ozaki
+    energies), T = 0.01 at cutoff 8 (45: one pass, eight energies per thread
+    for some threads) and T = 0.005 at cutoff 16 (89: three energy passes of
+    32, 32 and 25) give the results of the same grains run on their own."""
+    import superconga_b200 as sb
+    from oracle import oracle as O
+    cfgs = []
+    for t, cut in ((0.5, 8.0), (0.01, 8.0), (0.005, 16.0)):
+        c = configs.small_disc()
+        c["physics"]["temperature"] = t
+        c["numerics"]["energy_cutoff"] = cut
+        cfgs.append(c)
+    states = []
+    for i, c in enumerate(cfgs):
+        s = O.make_setup(c)
+        db = O.delta_bulk(s.temperature, s.symmetries[0])
+        states.append(configs.seeded_state(s.n_comp, s.n0, db, 20 + i, 0.05, True, 0.02))
+    b = sb.Batch(cfgs, mode=mode)
+    assert [g.dims.n_energies for g in b.grains] == [7, 45, 89]
+    for g, (d, a) in zip(b.grains, states):
+        g.set_state(d, a)
+    b.compute(3)  # iteration 1 eager, 2-3 graph replays
+    tol = 1e-11 if mode == "fp64" else 1e-4
+    for g, c, (d, a) in zip(b.grains, cfgs, states):
+        e = sb.Context(c, mode=mode)
+        e.set_state(d, a)
+        e.compute(3)
+        assert _rel(g.results()[0], e.results()[0]) < tol
+        assert _rel(g.results()[1], e.results()[1]) < 100 * tol
+        assert abs(g.scalars()["free_energy"] - e.scalars()["free_energy"]) <= tol * abs(e.scalars()["free_energy"])
+        e.close()
+    b.close()
