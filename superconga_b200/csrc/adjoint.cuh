@@ -155,7 +155,7 @@ __device__ void adjoint_column(const AdjArgs &J, const double *s_res, int item, 
 #pragma unroll
         for (int j = 0; j < EMAX; ++j)
           if (j < ecount)
-            coh[j] = riccati_step<double>(dre, dim, es, eim[j], ((const C *)A.bin_gt)[(size_t)(in_gt + nin) * ne + e0 + j], st);
+            coh[j] = riccati_step<double>(dre, dim, es, eim[j], ((const C *)A.bin_gt)[(size_t)(in_gt + nin) * A.ne_stride + e0 + j], st);
         ++nin;
       } else {
         const double mre = (dre + p0) * 0.5, mim = (dim + p1) * 0.5, mes = (es + p2) * 0.5;
@@ -191,7 +191,7 @@ __device__ void adjoint_column(const AdjArgs &J, const double *s_res, int item, 
 #pragma unroll
         for (int j = 0; j < EMAX; ++j)
           if (j < ecount)
-            coh[j] = riccati_step<double>(dre, dim, es, eim[j], ((const C *)A.bin_g)[(size_t)(in_g + nin) * ne + e0 + j], st);
+            coh[j] = riccati_step<double>(dre, dim, es, eim[j], ((const C *)A.bin_g)[(size_t)(in_g + nin) * A.ne_stride + e0 + j], st);
         ++nin;
       } else {
         const double mre = (dre + p0) * 0.5, mim = (dim + p1) * 0.5, mes = (es + p2) * 0.5;
@@ -228,7 +228,7 @@ __device__ void adjoint_column(const AdjArgs &J, const double *s_res, int item, 
 #pragma unroll
           for (int j = 0; j < EMAX; ++j)
             if (j < ecount)
-              cc[j] = riccati_step<double>(dre, dim, es, eim[j], ((const C *)A.bin_g)[(size_t)(in_g + nin) * ne + e0 + j], st);
+              cc[j] = riccati_step<double>(dre, dim, es, eim[j], ((const C *)A.bin_g)[(size_t)(in_g + nin) * A.ne_stride + e0 + j], st);
           ++nin;
         } else {
           const double mre = (dre + p0) * 0.5, mim = (dim + p1) * 0.5, mes = (es + p2) * 0.5;
@@ -266,7 +266,7 @@ __device__ void adjoint_column(const AdjArgs &J, const double *s_res, int item, 
 #pragma unroll
           for (int j = 0; j < EMAX; ++j)
             if (j < ecount)
-              cc[j] = riccati_step<double>(dre, dim, es, eim[j], ((const C *)A.bin_gt)[(size_t)(in_gt + nin) * ne + e0 + j], st);
+              cc[j] = riccati_step<double>(dre, dim, es, eim[j], ((const C *)A.bin_gt)[(size_t)(in_gt + nin) * A.ne_stride + e0 + j], st);
           ++nin;
         } else {
           const double mre = (dre + p0) * 0.5, mim = (dim + p1) * 0.5, mes = (es + p2) * 0.5;
@@ -340,7 +340,7 @@ __device__ void adjoint_column(const AdjArgs &J, const double *s_res, int item, 
               if (j < ecount) {
                 C gg0, gD;
                 double ge;
-                riccati_step_adj(dre, dim, es, eim[j], ((const C *)A.bin_g)[(size_t)(in_g + nin) * ne + e0 + j], st,
+                riccati_step_adj(dre, dim, es, eim[j], ((const C *)A.bin_g)[(size_t)(in_g + nin) * A.ne_stride + e0 + j], st,
                                  lam[j], gg0, gD, ge);
                 ownD = cadd(ownD, gD);
                 ownE += ge;
@@ -384,8 +384,14 @@ __device__ void adjoint_column(const AdjArgs &J, const double *s_res, int item, 
           group_sum(ownE, A.groups, gmask);
         }
         if (g == 0) {
-          J.grad_d[slot + site] = make_double2(ownD.re, ownD.im);
-          J.grad_e[slot + site] = ownE;
+          if (A.accumulate) {  // a later energy pass adds to the earlier ones
+            const double2 o = J.grad_d[slot + site];
+            J.grad_d[slot + site] = make_double2(o.x + ownD.re, o.y + ownD.im);
+            J.grad_e[slot + site] += ownE;
+          } else {
+            J.grad_d[slot + site] = make_double2(ownD.re, ownD.im);
+            J.grad_e[slot + site] = ownE;
+          }
         }
       }
     }
@@ -434,7 +440,7 @@ __device__ void adjoint_column(const AdjArgs &J, const double *s_res, int item, 
               if (j < ecount) {
                 C gg0, gD;
                 double ge;
-                riccati_step_adj(dre, dim, es, eim[j], ((const C *)A.bin_gt)[(size_t)(in_gt + nin) * ne + e0 + j], st,
+                riccati_step_adj(dre, dim, es, eim[j], ((const C *)A.bin_gt)[(size_t)(in_gt + nin) * A.ne_stride + e0 + j], st,
                                  lam[j], gg0, gD, ge);
                 ownT = cadd(ownT, gD);
                 ownE += ge;
@@ -772,8 +778,29 @@ void adjoint_run(sc_ctx *c, AdjBuffers &B, double w_omega, const double *beta_ho
     J.grad_d = grad_d;
     J.grad_e = B.grad_e.p;
     const size_t threads = ni * c->groups;
-    k_adjoint<4><<<grid1(threads, 128), 128, 0, c->stream>>>(J);
-    check_launch(c);
+    if (c->ept <= 4 && c->e_pass >= S.ne) {
+      k_adjoint<4><<<grid1(threads, 128), 128, 0, c->stream>>>(J);
+      check_launch(c);
+    } else {
+      // Energy passes of four energies per thread, each from its own slice
+      // of the boundary values, adding into the gradients of the earlier ones.
+      const int pass = 4 * c->groups;
+      for (int e = 0; e < S.ne; e += pass) {
+        AdjArgs P = J;
+        P.S.ne = std::min(pass, S.ne - e);
+        P.S.ept = 4;
+        P.S.accumulate = e > 0;
+        P.S.e_re += e;
+        P.S.e_im += e;
+        P.S.res += e;
+        P.S.bin_g += e;
+        P.S.bin_gt += e;
+        P.S.bout_g += e;
+        P.S.bout_gt += e;
+        k_adjoint<4><<<grid1(threads, 128), 128, 0, c->stream>>>(P);
+        check_launch(c);
+      }
+    }
     dim3 gridf(grid1(nn1, 256), nslots);
     k_adj_fields_t<<<gridf, 256, 0, c->stream>>>(A, ch.a_begin, ch.a_end, grad_d, B.grad_e.p, B.g_dext.p,
                                                   B.g_avec.p, B.g_b.p);
@@ -842,11 +869,6 @@ int sc_adjoint(sc_ctx *ctx, double w_omega, const double *beta_j, double *g_delt
   if (!ctx) return SC_ERR_ARG;
   if (ctx->mode != SC_MODE_FP64 || ctx->S.keldysh || ctx->batch_member) {
     ctx->err = "sc_adjoint: FP64 self-consistency contexts only";
-    return SC_ERR_STATE;
-  }
-  if (ctx->ept > 4 || ctx->e_pass < ctx->S.ne) {
-    ctx->err = ctx->e_pass < ctx->S.ne ? "sc_adjoint: at most 64 Ozaki energies"
-                                       : "sc_adjoint: more than four energies per thread";
     return SC_ERR_STATE;
   }
   if (!ctx->boundary_initialized) {

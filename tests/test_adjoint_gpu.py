@@ -133,4 +133,26 @@ def test_autograd_function(engine_lib):
     with torch.no_grad():
         step = 1e-4 / max(float(delta.grad.abs().max()), 1e-30)
         loss2 = FreeEnergy.apply(delta - step * delta.grad, av, b, e, 1.0, None)
-    assert float(loss2) < float(loss)
+    assert float(loss2.detach()) < float(loss.detach())
+
+
+@pytest.mark.parametrize("temperature,cutoff,n_energies", [(0.01, 8.0, 45), (0.005, 16.0, 89)])
+def test_adjoint_energy_passes_vs_fd(engine_lib, temperature, cutoff, n_energies):
+    """The adjoint over energy passes of four energies per thread (45
+    energies: two passes; 89: three, beside the forward sweep's own passes)
+    against central differences of the engine."""
+    cfg = configs.small_disc()
+    cfg["physics"]["temperature"] = temperature
+    cfg["numerics"]["energy_cutoff"] = cutoff
+    e, o, d, a, db, dom = _setup(cfg)
+    assert e.dims.n_energies == n_energies
+    b0 = e.external_field()
+    e.evaluate()
+    gd, ga, gb = e.adjoint(1.0)
+    rng = np.random.default_rng(17)
+    for vd, va, vb in _directions(rng, d, a, dom, db, 3):
+        fp = _engine_f(e, d + EPS * vd, a + EPS * va, b0 + EPS * vb)
+        fm = _engine_f(e, d - EPS * vd, a - EPS * va, b0 - EPS * vb)
+        fd = (fp - fm) / (2 * EPS)
+        ad = float(np.sum(gd * vd) + np.sum(ga * va) + gb * vb)
+        assert abs(fd - ad) <= TOL * max(abs(ad), abs(fd)), (fd, ad)
