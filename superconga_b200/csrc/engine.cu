@@ -472,7 +472,7 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
       if (A.burn_in) continue;
       if constexpr (KEL) {
         if (l != 0) {
-          double *o = A.ldf + ((size_t)(a - A.slot_base) * nn1 + (size_t)y * n1 + x) * ne + e0;
+          double *o = A.ldf + ((size_t)(a - A.slot_base) * nn1 + (size_t)y * n1 + x) * A.ne_stride + e0;
 #pragma unroll
           for (int j = 0; j < EMAX; ++j)
             if (j < ecount) o[j] = (double)greens_g_im<R>(coh[j], gt[j]);
@@ -1743,6 +1743,7 @@ void launch_sweep(sc_ctx *c, const Chunk &ch, int burn_in) {
     P.bout_g += e;
     P.bin_gt += e;
     P.bout_gt += e;
+    P.ldf += e;  // LDOS frames: energy-innermost, this pass's slice
     launch_sweep_pass<R>(c, P, blocks);
   }
 }
@@ -2328,7 +2329,7 @@ void upload_static(sc_ctx *c) {
     }
     if (ok) c->pair = na / 2;
   }
-  c->e_pass = (S.keldysh || S.ne <= SWEEP_MAX_ENERGIES) ? S.ne : ENERGY_PASS;
+  c->e_pass = S.ne <= SWEEP_MAX_ENERGIES ? S.ne : ENERGY_PASS;
   std::vector<int4> items;
   plan_chunks(c, items);
   c->items.upload(items, s);
@@ -2489,7 +2490,6 @@ int create_context(int mode, sc_ctx **out, F make) {
     const std::string e = make(c->S);
     if (!e.empty()) throw EngineError(SC_ERR_ARG, e);
     if (c->S.nc > MAX_COMP) throw EngineError(SC_ERR_ARG, "at most 4 order-parameter components");
-    if (c->S.keldysh && c->S.ne > SWEEP_MAX_ENERGIES) throw EngineError(SC_ERR_ARG, "at most 64 energies per LDOS block");
     if (2 * c->S.nc + 2 > 16) throw EngineError(SC_ERR_ARG, "too many accelerator fields");
     CUDA_TRY(cudaGetDevice(&c->device));
     CUDA_TRY(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));

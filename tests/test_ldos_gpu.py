@@ -54,6 +54,29 @@ def test_ldos_blocks(engine_lib):
     assert _rel(e.ldos(), L.ldos) < TOL
 
 
+def test_ldos_block_passes(engine_lib):
+    """A block of 80 real energies, more than one sweep pass takes (64), is
+    swept in passes of 32, 32 and 16 into one LDOS frame; the block and the
+    short one after it (20 energies) match the oracle (1e-10)."""
+    sim = configs.small_disc()
+    from oracle import oracle as O
+    db = O.delta_bulk(0.5, "s")
+    pp = configs.ldos_postprocess(db, n_energies=100, per_block=80, n_angles=32)
+    L, e, _ = _pair(sim, pp)
+    for b in range(2):
+        L.begin_block(b)
+        e.begin_block(b)
+        L.burn_in()
+        e.burn_in(1)
+        for it in range(2):
+            r_o, _, _ = L.iterate()
+            r_e, _ = e.iterate(1)
+            assert abs(r_e - r_o) <= 1e-8 * r_o, (b, it, r_e, r_o)
+        for which in range(4):
+            assert _rel(e.boundary(which), L.oracle.boundary(which)) < TOL
+    assert _rel(e.ldos(), L.ldos) < TOL
+
+
 def test_ldos_d_wave_square(engine_lib):
     """d-wave square with pair-breaking edges, vector potential, one block."""
     sim = configs.small_square_d()
