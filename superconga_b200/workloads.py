@@ -21,10 +21,36 @@ D_WAVE_BULK = math.exp(-EULER_MASCHERONI - 0.5) / math.sqrt(2.0)
 
 
 def bulk_s_wave(t: float) -> float:
-    """Bulk s-wave gap at temperature t (units of 2 pi k_B T_c), from the
-    library's computeOrderParameterBulkSWave (OrderParameterBulk.h:88-221)."""
-    from .engine import bulk_order_parameter_s_wave
-    return bulk_order_parameter_s_wave(t)
+    """Bulk s-wave gap at temperature t (units of 2 pi k_B T_c), the secant
+    iteration of computeOrderParameterBulkSWave (OrderParameterBulk.h:88-221).
+    Kept in numpy rather than calling the library's sc_bulk_order_parameter_s_wave:
+    the workload inputs are also built for the CPU reference arm, which loads
+    no part of the engine."""
+    eps = np.finfo(np.float64).eps
+    if t >= 1.0:
+        return 0.0
+    if t < eps:
+        return S_WAVE_BULK
+    ne = int(100.0 / t - 0.5) + 1
+    n = np.arange(ne - 1, -1, -1, dtype=np.float64)
+    en = t * (n + 0.5)
+    coupling = 1.0 / (math.log(t) / t + float(np.sum(1.0 / en)))
+
+    def resid(op):
+        return op * (float(np.sum(1.0 / np.hypot(op, en))) * coupling - 1.0)
+
+    op = S_WAVE_BULK * math.sqrt(1.0 - t ** 3)
+    ops = [op, math.sqrt(op)]
+    res = [resid(ops[0]), resid(ops[1])]
+    for _ in range(10):
+        w = 1.0 / (1.0 - (ops[0] / ops[1]) / (res[0] / res[1]))
+        op = (1.0 - w) * ops[0] + w * ops[1]
+        r = resid(op)
+        if abs(r / op) < 10 * eps:
+            break
+        k = 0 if abs(res[0]) > abs(res[1]) else 1
+        ops[k], res[k] = op, r
+    return op
 
 
 def delta_bulk(t: float, symmetry: str) -> float:
