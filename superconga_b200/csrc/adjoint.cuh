@@ -841,6 +841,7 @@ extern "C" {
 
 int sc_set_external_field(sc_ctx *ctx, double b) {
   if (!ctx || ctx->batch_member) return SC_ERR_ARG;
+  ctx->drop_graph();
   ctx->S.flux_quanta = b * ctx->S.area / M_PI;
   return SC_OK;
 }
@@ -853,6 +854,7 @@ int sc_get_external_field(const sc_ctx *ctx, double *b) {
 
 int sc_evaluate(sc_ctx *ctx, double *free_energy) {
   if (!ctx) return SC_ERR_ARG;
+  ctx->drop_graph();
   if (ctx->mode != SC_MODE_FP64 || ctx->S.keldysh || ctx->batch_member) {
     ctx->err = "sc_evaluate: FP64 self-consistency contexts only";
     return SC_ERR_STATE;
@@ -867,6 +869,7 @@ int sc_evaluate(sc_ctx *ctx, double *free_energy) {
 int sc_adjoint(sc_ctx *ctx, double w_omega, const double *beta_j, double *g_delta, double *g_a,
                double *g_b) {
   if (!ctx) return SC_ERR_ARG;
+  ctx->drop_graph();
   if (ctx->mode != SC_MODE_FP64 || ctx->S.keldysh || ctx->batch_member) {
     ctx->err = "sc_adjoint: FP64 self-consistency contexts only";
     return SC_ERR_STATE;

@@ -1577,6 +1577,19 @@ struct sc_ctx {
   bool profiling = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof[4];
 
+  // One steady-state iteration (accelerator step to scalars) captured as a
+  // CUDA graph and replayed by sc_compute.  Every call that could change what
+  // an iteration enqueues (state flags, field, stream, frame buffers) drops
+  // it; sc_set_state only writes new values into the buffers the graph reads.
+  cudaGraphExec_t iter_graph = nullptr;
+  long long iter_graph_launches = 0;
+  bool iter_graph_failed = false;
+  void drop_graph() {
+    if (iter_graph) cudaGraphExecDestroy(iter_graph);
+    iter_graph = nullptr;
+  }
+  ~sc_ctx() { drop_graph(); }
+
   size_t nn0() const { return (size_t)S.n0 * S.n0; }
   size_t esize() const { return mode == SC_MODE_FP64 ? sizeof(Cx<double>) : sizeof(Cx<float>); }
   // Bytes of one frame-buffer element (FrameOf<R>: float2 for the FP32 sweep).
@@ -2052,6 +2065,48 @@ void compute_once(sc_ctx *c) {
   compute_pre<R>(c);
   run_chunks<R>(c, 0);
   compute_post<R>(c);
+}
+
+// One Context::compute iteration; once the iteration is steady (after the
+// first one, boundary values set, frames cleared) it is captured as a CUDA
+// graph and replayed, so a small grain pays one graph launch instead of ~25
+// kernel launches per iteration.
+template <typename R>
+void compute_iteration(sc_ctx *c) {
+  static const bool no_graph = std::getenv("SCB_NO_GRAPH") != nullptr;
+  const bool steady = !c->first_compute && c->boundary_initialized && (c->frames_zeroed || c->chunks.size() > 1) &&
+                      !c->profiling && !c->batch_member && !c->iter_graph_failed && !no_graph;
+  if (!steady) {
+    c->drop_graph();
+    compute_once<R>(c);
+    return;
+  }
+  if (!c->iter_graph) {
+    const long long l0 = c->launches;
+    cudaGraph_t g = nullptr;
+    CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    try {
+      compute_once<R>(c);
+    } catch (...) {
+      cudaStreamEndCapture(c->stream, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    CUDA_TRY(cudaStreamEndCapture(c->stream, &g));
+    const cudaError_t e = cudaGraphInstantiate(&c->iter_graph, g, 0);
+    cudaGraphDestroy(g);
+    c->iter_graph_launches = c->launches - l0;
+    c->launches = l0;
+    if (e != cudaSuccess) {  // run eagerly from now on (nothing of the capture ran)
+      (void)cudaGetLastError();
+      c->iter_graph = nullptr;
+      c->iter_graph_failed = true;
+      compute_once<R>(c);
+      return;
+    }
+  }
+  CUDA_TRY(cudaGraphLaunch(c->iter_graph, c->stream));
+  c->launches += c->iter_graph_launches;
 }
 
 template <typename R>
@@ -2564,6 +2619,7 @@ int sc_site_updates(const sc_ctx *ctx, long long *per_iteration) {
 
 int sc_set_stream(sc_ctx *ctx, void *stream) {
   if (!ctx) return SC_ERR_ARG;
+  ctx->drop_graph();
   API_BEGIN
   CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
@@ -2628,8 +2684,8 @@ int sc_compute(sc_ctx *ctx, int n, double *residual, int *converged) {
   }
   API_BEGIN
   for (int i = 0; i < n; ++i) {
-    if (ctx->mode == SC_MODE_FP64) compute_once<double>(ctx);
-    else compute_once<float>(ctx);
+    if (ctx->mode == SC_MODE_FP64) compute_iteration<double>(ctx);
+    else compute_iteration<float>(ctx);
   }
   read_scalars(ctx);
   const Scalars &s = ctx->host_scalars;
@@ -2641,6 +2697,7 @@ int sc_compute(sc_ctx *ctx, int n, double *residual, int *converged) {
 
 int sc_burn_in(sc_ctx *ctx, int n, double *residual, int *converged) {
   if (!ctx || n < 0) return SC_ERR_ARG;
+  ctx->drop_graph();
   API_BEGIN
   for (int i = 0; i < n; ++i) {
     if (ctx->mode == SC_MODE_FP64) burn_in_once<double>(ctx);
@@ -2681,6 +2738,7 @@ int sc_ldos_energies(const sc_ctx *ctx, double *energies, double *broadening) {
 
 int sc_ldos_begin_block(sc_ctx *ctx, int block) {
   if (!ctx || !ctx->S.keldysh) return SC_ERR_ARG;
+  ctx->drop_graph();
   API_BEGIN
   ldos_begin_block(ctx, block);
   API_END
@@ -2688,6 +2746,7 @@ int sc_ldos_begin_block(sc_ctx *ctx, int block) {
 
 int sc_ldos_iterate(sc_ctx *ctx, int n, double *residual, int *converged) {
   if (!ctx || !ctx->S.keldysh || n < 0) return SC_ERR_ARG;
+  ctx->drop_graph();
   API_BEGIN
   for (int i = 0; i < n; ++i) {
     if (ctx->mode == SC_MODE_FP64) ldos_once<double>(ctx);
@@ -2702,6 +2761,7 @@ int sc_ldos_iterate(sc_ctx *ctx, int n, double *residual, int *converged) {
 
 int sc_ldos_run(sc_ctx *ctx, int burnin, int it_min, int it_max, int *converged, int *iterations) {
   if (!ctx || !ctx->S.keldysh) return SC_ERR_ARG;
+  ctx->drop_graph();
   API_BEGIN
   // runPostprocess (run_simulation.h:44-104) with runIterations
   // (run_iteration.h:75-130); "until converged" loops stop after 100000.
@@ -2818,6 +2878,7 @@ int sc_get_boundary(sc_ctx *ctx, int which, double *values) {
 
 int sc_set_boundary(sc_ctx *ctx, int which, const double *values) {
   if (!ctx || which < 0 || which > 3 || !values) return SC_ERR_ARG;
+  ctx->drop_graph();
   API_BEGIN
   const size_t n = (size_t)ctx->n_bnd(which) * ctx->S.ne;
   if (n) {
@@ -2839,6 +2900,7 @@ int sc_set_boundary(sc_ctx *ctx, int which, const double *values) {
 
 int sc_boundary_initial(sc_ctx *ctx) {
   if (!ctx) return SC_ERR_ARG;
+  ctx->drop_graph();
   API_BEGIN
   if (ctx->mode == SC_MODE_FP64) boundary_initial<double>(ctx);
   else boundary_initial<float>(ctx);
@@ -2849,6 +2911,7 @@ int sc_boundary_initial(sc_ctx *ctx) {
 
 int sc_angle_greens(sc_ctx *ctx, int angle, double *f, double *g_re, double *i_re) {
   if (!ctx || angle < 0 || angle >= ctx->S.n_angles) return SC_ERR_ARG;
+  ctx->drop_graph();
   if (ctx->S.keldysh) {
     ctx->err = "sc_angle_greens: not available on an LDOS context";
     return SC_ERR_STATE;
@@ -2909,6 +2972,7 @@ int sc_angle_greens(sc_ctx *ctx, int angle, double *f, double *g_re, double *i_r
 
 int sc_poisson(sc_ctx *ctx, const double *j, double *a_out) {
   if (!ctx || !j || !a_out) return SC_ERR_ARG;
+  ctx->drop_graph();
   if (!ctx->has_vp() || ctx->S.keldysh) {
     ctx->err = "sc_poisson: the configuration has no finite penetration depth (or is an LDOS context)";
     return SC_ERR_STATE;
@@ -2965,6 +3029,7 @@ int sc_measure_fma_peak(int precision, double *flops_per_second) {
 
 int sc_profile(sc_ctx *ctx, int enable) {
   if (!ctx) return SC_ERR_ARG;
+  ctx->drop_graph();
   ctx->profiling = enable != 0;
   return SC_OK;
 }
