@@ -2076,7 +2076,9 @@ void compute_iteration(sc_ctx *c) {
   static const bool no_graph = std::getenv("SCB_NO_GRAPH") != nullptr;
   const bool steady = !c->first_compute && c->boundary_initialized && (c->frames_zeroed || c->chunks.size() > 1) &&
                       !c->profiling && !c->batch_member && !c->iter_graph_failed && !no_graph;
-  if (!steady) {
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  CUDA_TRY(cudaStreamIsCapturing(c->stream, &cap));
+  if (!steady || cap != cudaStreamCaptureStatusNone) {  // a caller's capture records the eager launches
     c->drop_graph();
     compute_once<R>(c);
     return;
