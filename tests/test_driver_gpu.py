@@ -60,6 +60,35 @@ def test_driver_golden_disc(engine_lib, tmp_path):
     assert abs(res2["free_energy_per_unit_area"] - fe) <= 1e-4 * abs(fe)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_driver_low_temperature(engine_lib, tmp_path, precision):
+    """The d_{x2-y2} square of tests/physics/low_temp_free_energy_test.cu (T =
+    0.001, cutoff 32: 281 Ozaki energies, swept in energy passes) run by the
+    drop-in executable from the reference's JSON: converged within 50
+    iterations, free energy per area within 1e-4 of the bulk value
+    -D_WAVE_BULK^2 / 2 and mean gap within 1e-5 of D_WAVE_BULK."""
+    from oracle.oracle import D_WAVE_BULK
+    cfg = configs.low_temperature_bulk(swave=False, disc=False)
+    cfg["physics"]["order_parameter"]["dx2-y2"].update({"initial_noise_stddev": 0.0,
+                                                        "initial_phase_shift": 0.0, "vortices": []})
+    cfg["numerics"].update({"num_iterations_burnin": 0, "num_iterations_min": 1,
+                            "num_iterations_max": 50})
+    out = tmp_path / "out"
+    cfg["misc"] = {"save_path": str(out), "save_frequency": -1, "load_path": "",
+                   "verbose": False, "data_format": "csv"}
+    if precision == "mixed":
+        cfg["b200"] = {"precision": "mixed"}
+    r = _run(cfg, tmp_path)
+    assert r.returncode == 0, r.stderr
+    conv = list(csv.reader(open(out / "simulation_convergence.csv")))
+    last = [float(v) for v in conv[-1][1:6]]
+    assert len(conv) - 1 <= 50 and max(last) < 1e-3, conv[-1]
+    res = json.loads((out / "simulation_results.json").read_text())
+    expected = -0.5 * D_WAVE_BULK * D_WAVE_BULK
+    assert abs(res["free_energy_per_unit_area"] - expected) <= 1e-4 * abs(expected), res
+    assert abs(res["order_parameter_average_magnitude"] - D_WAVE_BULK) <= 1e-5 * D_WAVE_BULK, res
+
+
 def test_driver_load_other_lattice(engine_lib, tmp_path):
     """A run saved at 3 points/xi0 continued at 4 points/xi0: the order
     parameter is extended past the grain and resampled onto the finer lattice
