@@ -76,6 +76,35 @@ def build(force: bool = False) -> str:
     return LIB_PATH
 
 
+REF_INCLUDE = os.environ.get("SCB_REFERENCE_INCLUDE", "/root/reference/include")
+REF_DIR = os.path.join(HERE, "_ref")
+REF_LIB = os.path.join(REF_DIR, "libscb_ref.so")
+
+
+def build_ref(force: bool = False):
+    """Compile ref_harness.cpp against the reference's own header files, read
+    where they lie (REF_INCLUDE), into oracle/_ref/libscb_ref.so: g++ on the
+    reference's CPU backend (Thrust on OpenMP; the flags of the reference's
+    CMakeLists.txt:192-214), Thrust from the CUDA toolkit's headers.  Returns
+    the library path, or None when the reference tree is not present (then a
+    library built earlier is used if there is one)."""
+    src = os.path.join(HERE, "ref_harness.cpp")
+    if not os.path.isdir(os.path.join(REF_INCLUDE, "conga")):
+        return REF_LIB if os.path.exists(REF_LIB) else None
+    if not force and os.path.exists(REF_LIB) and os.path.getmtime(REF_LIB) >= os.path.getmtime(src):
+        return REF_LIB
+    os.makedirs(REF_DIR, exist_ok=True)
+    cuda_inc = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "include")
+    tmp = REF_LIB + ".tmp"
+    subprocess.check_call([
+        "g++", "-std=c++17", "-O2", "-DNDEBUG", "-fopenmp", "-fPIC", "-shared", "-x", "c++",
+        "-DCONGA_BACKEND_CPU=1", "-DTHRUST_DEVICE_SYSTEM=THRUST_DEVICE_SYSTEM_OMP",
+        "-DTHRUST_HOST_SYSTEM=THRUST_HOST_SYSTEM_CPP", "-D_LIBCUDACXX_STRING_H_HAS_CONST_OVERLOADS=1",
+        "-I", REF_INCLUDE, "-I", cuda_inc, src, "-o", tmp])
+    os.replace(tmp, REF_LIB)
+    return REF_LIB
+
+
 class OrcParams(ctypes.Structure):
     _fields_ = [
         ("n0", ctypes.c_int), ("n1", ctypes.c_int), ("n_angles", ctypes.c_int),
