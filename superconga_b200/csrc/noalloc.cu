@@ -15,6 +15,7 @@
 // overwrites everything it later reads, so nothing relies on them.  Calls whose
 // work overlaps on the GPU (different streams, or different host threads on
 // the same device) race on the array and must be ordered by the caller.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -31,10 +32,18 @@ constexpr int NA_PT = 32;
 
 __device__ __align__(256) double g_noalloc_scratch[NOALLOC_SCRATCH_DOUBLES];
 
-// Device address of g_noalloc_scratch per device ordinal, found once per device.
+// Device address of g_noalloc_scratch, looked up once per device and CUDA
+// context.  The context is part of the key because the array moves when the
+// device's context is destroyed and created again (cudaDeviceReset, or the
+// primary context released and retained): the module is then reloaded and the
+// old address is no longer valid.
 std::mutex g_mutex;
 constexpr int MAX_DEVICES = 64;
-double *g_scratch_addr[MAX_DEVICES] = {nullptr};
+struct ScratchSlot {
+  CUcontext ctx = nullptr;
+  double *addr = nullptr;
+};
+ScratchSlot g_scratch[MAX_DEVICES];
 
 // Per-block sums of both current components (first half of `partial`: x,
 // second half: y).
@@ -130,22 +139,59 @@ __global__ void k_na_scale(size_t n2, double factor, double *a) {
   if (i < n2) a[i] *= factor;
 }
 
-// Finds this device's address of g_noalloc_scratch the first time the device
-// is used; later calls reuse it.
+// The CUDA context current on this thread, through the driver's
+// cuCtxGetCurrent (reached via the runtime, so the library needs no link to
+// libcuda).  nullptr when no context is current yet.
+CUcontext current_context() {
+  using GetCurrent = CUresult (*)(CUcontext *);
+  static GetCurrent fn = [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<GetCurrent>(f);
+  }();
+  CUcontext c = nullptr;
+  if (!fn || fn(&c) != CUDA_SUCCESS) return nullptr;
+  return c;
+}
+
+// Set-up of the current device: its address of g_noalloc_scratch.  The first
+// call on a device (and the first after its context was re-created) makes the
+// lookup with cudaGetSymbolAddress, which also loads this library's device code
+// on that device; later calls in the same context reuse the address.
 cudaError_t scratch_address(double **out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= MAX_DEVICES) return cudaErrorInvalidDevice;
   std::lock_guard<std::mutex> lock(g_mutex);
-  if (!g_scratch_addr[dev]) {
+  ScratchSlot &slot = g_scratch[dev];
+  const CUcontext ctx = current_context();
+  if (!slot.addr || !ctx || slot.ctx != ctx) {
     double *ptr = nullptr;
     e = cudaGetSymbolAddress((void **)&ptr, g_noalloc_scratch);
     if (e != cudaSuccess) return e;
-    g_scratch_addr[dev] = ptr;
+    slot.addr = ptr;
+    slot.ctx = current_context();  // current now, if it was not before the lookup
   }
-  *out = g_scratch_addr[dev];
+  *out = slot.addr;
   return cudaSuccess;
+}
+
+// Launches kernel on the stream and returns that launch's own status, so a
+// failure is reported whatever error an earlier call of the caller left behind.
+template <typename... KArgs, typename... Args>
+cudaError_t launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cfg.attrs = nullptr;
+  cfg.numAttrs = 0;
+  return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
 }
 
 unsigned blocks_for(size_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
@@ -168,16 +214,21 @@ extern "C" int sc_poisson_noalloc(int n0, int n_filters, const double *d_filters
   double *t0 = s + 2 * nn;
   double *t1 = t0 + 2 * nn;
   const size_t n2 = 2 * nn;
-  k_na_partial_sums<<<NA_REDUCE_BLOCKS, NA_THREADS, 0, st>>>(nn, d_j, partial);
-  k_na_subtract_mean<<<blocks_for(n2, NA_THREADS), NA_THREADS, 0, st>>>(
-      nn, NA_REDUCE_BLOCKS, (double)n_grain, partial, d_j, s);
+  const dim3 thr(NA_THREADS), elem(blocks_for(n2, NA_THREADS));
+  cudaError_t e = launch(k_na_partial_sums, dim3(NA_REDUCE_BLOCKS), thr, st, nn, d_j, partial);
+  if (e == cudaSuccess)
+    e = launch(k_na_subtract_mean, elem, thr, st, nn, NA_REDUCE_BLOCKS, (double)n_grain, partial, d_j, s);
   const dim3 blk(NA_PT, 8), grid((n0 + NA_PT - 1) / NA_PT, (n0 + NA_PT - 1) / NA_PT, 2);
-  for (int k = 0; k < n_filters; ++k) {
+  for (int k = 0; k < n_filters && e == cudaSuccess; ++k) {
     const double *f = d_filters + (size_t)k * (2 * n0 - 1);
-    k_na_toeplitz<<<grid, blk, 0, st>>>(n0, f, s, t0);
-    k_na_toeplitz<<<grid, blk, 0, st>>>(n0, f, t0, t1);
-    k_na_accumulate<<<blocks_for(n2, NA_THREADS), NA_THREADS, 0, st>>>(n2, k == 0, positive[k] != 0, t1, d_a);
+    e = launch(k_na_toeplitz, grid, blk, st, n0, f, s, t0);
+    if (e == cudaSuccess) e = launch(k_na_toeplitz, grid, blk, st, n0, f, t0, t1);
+    if (e == cudaSuccess) e = launch(k_na_accumulate, elem, thr, st, n2, k == 0 ? 1 : 0, positive[k] != 0 ? 1 : 0, t1, d_a);
   }
-  k_na_scale<<<blocks_for(n2, NA_THREADS), NA_THREADS, 0, st>>>(n2, factor, d_a);
-  return cudaGetLastError() == cudaSuccess ? SC_OK : SC_ERR_CUDA;
+  if (e == cudaSuccess) e = launch(k_na_scale, elem, thr, st, n2, factor, d_a);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();  // the error is this call's own: report it and clear it
+    return SC_ERR_CUDA;
+  }
+  return SC_OK;
 }
