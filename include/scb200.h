@@ -69,7 +69,16 @@ int sc_get_state(sc_ctx *ctx, double *delta, double *a_internal);
  * accelerator step (from the second iteration on), Riccati sweep and Green
  * accumulation for all angles, boundary condition, vector potential.  On
  * return *residual holds Context::getResidual and *converged
- * Context::isPartiallyConverged of the last iteration.  Either may be NULL. */
+ * Context::isPartiallyConverged of the last iteration.  Either may be NULL.
+ * Under a stream capture by the caller (ctx's stream, sc_set_stream, is being
+ * captured into a CUDA graph) the n iterations are only recorded into the
+ * caller's graph; nothing is read back or synchronised, so *residual and
+ * *converged are left unchanged (read them with sc_get_scalars after the graph
+ * has run).  Only a steady iteration can be recorded: at least one iteration
+ * must have run outside the capture, with profiling off and not on a batch
+ * grain; otherwise SC_ERR_STATE is returned and nothing is recorded.  Every
+ * other call that returns host data synchronises and is not available under
+ * capture (sc_burn_in returns SC_ERR_STATE). */
 int sc_compute(sc_ctx *ctx, int n, double *residual, int *converged);
 
 /* Runs n burn-in iterations (Context::burnIn, Context.h:377-389): boundary
@@ -95,6 +104,36 @@ int sc_set_stream(sc_ctx *ctx, void *stream);
 int sc_set_state_device(sc_ctx *ctx, const double *d_delta, const double *d_a_internal);
 int sc_get_state_device(sc_ctx *ctx, double *d_delta, double *d_a_internal);
 
+/* ---- frozen-boundary evaluation and its adjoint --------------------------- */
+
+/* No counterpart in the reference (its drivers have no derivative); these
+ * replace a finite-difference loop around Context::compute (Context.h:391-447).
+ * The functional is one pass of the self-consistency map with the incoming
+ * boundary values held fixed (IntegrationIteratorOzaki.h:302-404 without the
+ * boundary update):
+ *   L(Delta, A, B_ext) = w_omega * Omega + sum_r beta(r) . j(r)
+ * with Omega the free energy of ComputeFreeEnergy.h:281-414 and j the current
+ * of ComputeCurrent.h:175-222.  FP64 self-consistency contexts only (others
+ * return SC_ERR_STATE); the boundary values must be set (an iteration, a
+ * burn-in or sc_boundary_initial). */
+
+/* Sets the external field B_ext in units of B0 (the reference's
+ * external_flux_quanta Phi = B_ext * area / pi, RiccatiSolver.h:137-139). */
+int sc_set_external_field(sc_ctx *ctx, double b_ext);
+int sc_get_external_field(const sc_ctx *ctx, double *b_ext);
+
+/* One frozen-boundary pass at the current state: *free_energy = Omega;
+ * sc_get_results then returns that pass's Delta, j and A. */
+int sc_evaluate(sc_ctx *ctx, double *free_energy);
+
+/* Reverse-mode derivative of L at the current state (checkpointed adjoint
+ * Riccati sweeps, gamma kept every 16 sites).  beta_j [2][N0][N0] host (NULL:
+ * no current term); outputs, host, any may be NULL: g_delta [Nc][2][N0][N0]
+ * = dL/dRe Delta, dL/dIm Delta; g_a [2][N0][N0] = dL/dA (internal units);
+ * *g_b = dL/dB_ext. */
+int sc_adjoint(sc_ctx *ctx, double w_omega, const double *beta_j, double *g_delta, double *g_a,
+               double *g_b);
+
 /* ---- probes used by the parity tests ------------------------------------ */
 
 /* Frame geometry of one angle: labels [N1*N1] (0 out, 1 in, 2 entry, 3 exit)
@@ -108,6 +147,13 @@ int sc_get_domain(const sc_ctx *ctx, signed char *domain);
 /* Sizes of the sparse boundary storage: in/out for gamma, in/out for
  * gammaTilde (BoundaryStorage.h:440-490). */
 int sc_boundary_sizes(const sc_ctx *ctx, int *sizes);
+
+/* How the angles are swept: the number of angle chunks (the sweep scratch and
+ * frame buffers of all angles are held within a device-memory budget, 35% of
+ * the free memory at creation or SCB_SCRATCH_MB; one chunk unless a grain is
+ * too large) and whether mixed mode pairs each angle with its mirror angle
+ * theta + pi (one sweep serves both).  Either pointer may be NULL. */
+int sc_sweep_plan(const sc_ctx *ctx, int *n_chunks, int *paired);
 
 /* Boundary coherence values, interleaved (re, im), count*Ne complex values.
  * which: 0 in-gamma, 1 out-gamma, 2 in-gammaTilde, 3 out-gammaTilde. */
@@ -147,10 +193,12 @@ int sc_poisson(sc_ctx *ctx, const double *j, double *a_out);
  *   stream     cudaStream_t the work is issued on (asynchronous)
  * Limit: n0 <= 724 (6 n0^2 + 128 doubles of scratch); larger n0 returns SC_ERR_SIZE
  * before any work.  It allocates nothing (no cudaMalloc, no allocating
- * library call).  The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress) and should come before any stream capture.
- * All calls share the array: calls whose work overlaps on the GPU race on it
- * and must be ordered by the caller. */
+ * library call).  The first call on a device (and the first after that
+ * device's context was re-created, e.g. by cudaDeviceReset) looks up the
+ * array's device address (cudaGetSymbolAddress) and should come before any
+ * stream capture.  Each kernel launch is checked as it is issued; a launch
+ * error returns SC_ERR_CUDA.  All calls share the array: calls whose work
+ * overlaps on the GPU race on it and must be ordered by the caller. */
 int sc_poisson_noalloc(int n0, int n_filters, const double *d_filters, const int *positive,
                        double factor, int n_grain, const double *d_j, double *d_a, void *stream);
 
@@ -214,6 +262,19 @@ int sc_batch_grain(sc_batch *b, int i, sc_ctx **ctx);
 int sc_batch_compute(sc_batch *b, int n, int *n_active);
 /* Per grain: still active, iterations done, last residual (arrays of size n). */
 int sc_batch_status(const sc_batch *b, int *active, int *iterations, double *residual);
+/* Per grain (array of size n) how it stands: still running, finished
+ * converged, finished at its num_iterations_max without converging (the
+ * reference's "FAILURE! Simulation did not converge", run_simulation.h:174-181),
+ * or diverged.  No counterpart in the reference: a grain whose iteration gives
+ * a non-finite residual or free energy (a NaN or infinity anywhere in its
+ * order parameter, current or vector potential reaches both) is frozen with
+ * its last state, leaves the batch and is reported here; the other grains
+ * continue unchanged. */
+#define SC_GRAIN_RUNNING 0
+#define SC_GRAIN_CONVERGED 1
+#define SC_GRAIN_AT_CAP 2
+#define SC_GRAIN_DIVERGED 3
+int sc_batch_grain_state(const sc_batch *b, int *state);
 /* CUDA-graph replay of the iteration on (default) or off. */
 int sc_batch_set_graph(sc_batch *b, int enable);
 /* Mapping of the persistent sweep: each grain takes the fewest threads per

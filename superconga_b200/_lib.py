@@ -33,6 +33,7 @@ SIGNATURES = {
     "sc_get_frame_labels": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, _c_int_p]),
     "sc_get_domain": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "sc_boundary_sizes": (ctypes.c_int, [ctypes.c_void_p, _c_int_p]),
+    "sc_sweep_plan": (ctypes.c_int, [ctypes.c_void_p, _c_int_p, _c_int_p]),
     "sc_get_boundary": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _c_double_p]),
     "sc_set_boundary": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _c_double_p]),
     "sc_boundary_initial": (ctypes.c_int, [ctypes.c_void_p]),
@@ -63,6 +64,7 @@ SIGNATURES = {
     "sc_batch_compute": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _c_int_p]),
     "sc_batch_status": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "sc_batch_set_graph": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "sc_batch_grain_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "sc_batch_config": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "sc_batch_get_config": (ctypes.c_int, [ctypes.c_void_p, _c_int_p, _c_int_p, _c_int_p]),
     "sc_batch_autotune": (ctypes.c_int, [ctypes.c_void_p, _c_int_p, _c_int_p, ctypes.POINTER(ctypes.c_double)]),

@@ -737,14 +737,21 @@ __global__ void __launch_bounds__(256) k_ldos_finalize(int n0, int n_fields, con
 struct Res6 {
   double s[6];
 };
+// Maximum that keeps a NaN (fmax drops it): a non-finite value anywhere in a
+// residual reaches the residual, so a diverged state never reads as converged.
+// Equal to fmax for numbers.
+__device__ __forceinline__ double max_nan(double a, double b) {
+  return (a != a) ? a : ((b != b) ? b : fmax(a, b));
+}
+
 __device__ __forceinline__ void res_add(double *q, double o, double n) {
   const double d = o - n;
   q[0] += d * d;
   q[1] += o * o;
   q[2] += fabs(d);
   q[3] += fabs(o);
-  q[4] = fmax(q[4], fabs(d));
-  q[5] = fmax(q[5], fabs(o));
+  q[4] = max_nan(q[4], fabs(d));
+  q[5] = max_nan(q[5], fabs(o));
 }
 
 // Block reduction of NQ slots: slots listed in max_mask are max-reduced.
@@ -756,7 +763,7 @@ __device__ void block_reduce(double *q, int nq, unsigned long long max_mask, dou
     for (int s = blockDim.x / 2; s > 0; s >>= 1) {
       if ((int)threadIdx.x < s) {
         const double o = sh[threadIdx.x + s];
-        sh[threadIdx.x] = ((max_mask >> k) & 1ull) ? fmax(sh[threadIdx.x], o) : sh[threadIdx.x] + o;
+        sh[threadIdx.x] = ((max_mask >> k) & 1ull) ? max_nan(sh[threadIdx.x], o) : sh[threadIdx.x] + o;
       }
       __syncthreads();
     }
@@ -1096,8 +1103,8 @@ __device__ double residual_from(const double *t, size_t n_elem, int norm) {
     denom = sqrt(t[1]);
     eps *= (double)n_elem;
   } else {
-    numer = fmax(t[4], 2.2250738585072014e-308);
-    denom = fmax(t[5], 2.2250738585072014e-308);
+    numer = max_nan(t[4], 2.2250738585072014e-308);
+    denom = max_nan(t[5], 2.2250738585072014e-308);
   }
   return numer / fmax(denom, eps);
 }
@@ -1113,11 +1120,11 @@ __device__ void reduce_slots(const double *partial, int nblocks, int nq, unsigne
     double v = 0.0;
     for (int b = lane; b < nblocks; b += 32) {
       const double p = partial[(size_t)b * nq + k];
-      v = mx ? fmax(v, p) : v + p;
+      v = mx ? max_nan(v, p) : v + p;
     }
     for (int o = 16; o > 0; o >>= 1) {
       const double u = __shfl_xor_sync(0xffffffffu, v, o);
-      v = mx ? fmax(v, u) : v + u;
+      v = mx ? max_nan(v, u) : v + u;
     }
     if (lane == 0) t[k] = v;
   }
@@ -1139,7 +1146,7 @@ __global__ void k_scalars_a(FinalizeConsts C, const double *partial, int nblocks
   reduce_slots(partial, nblocks, NQ, FIN_MAX_MASK, t);
   if (threadIdx.x != 0) return;
   double rop = 0.0;
-  for (int c = 0; c < C.nc; ++c) rop = fmax(rop, residual_from(&t[6 * c], C.n_elem_field, C.norm));
+  for (int c = 0; c < C.nc; ++c) rop = max_nan(rop, residual_from(&t[6 * c], C.n_elem_field, C.norm));
   S->res_op = rop;
   S->conv_op = rop < C.conv;
   const double rj = residual_from(&t[24], C.n_elem_field, C.norm);
@@ -1177,14 +1184,14 @@ __global__ void k_scalars_b(int norm, size_t n_elem_g, size_t n_elem_gt, size_t 
   }
   if (do_vp) reduce_slots(p_vp, nb_vp, 6, 0x30ull, &t[12]);
   if (threadIdx.x != 0) return;
-  if (do_bc) S->res_bc = fmax(residual_from(&t[0], n_elem_g, norm), residual_from(&t[6], n_elem_gt, norm));
+  if (do_bc) S->res_bc = max_nan(residual_from(&t[0], n_elem_g, norm), residual_from(&t[6], n_elem_gt, norm));
   if (do_vp) S->res_vp = residual_from(&t[12], n_elem_vp, norm);
   double r = S->res_vp;
-  r = fmax(S->res_bc, r);
+  r = max_nan(S->res_bc, r);
   if (compute_mode) {
-    r = fmax(r, S->res_op);
-    r = fmax(r, S->res_j);
-    r = fmax(r, S->res_fe);
+    r = max_nan(r, S->res_op);
+    r = max_nan(r, S->res_j);
+    r = max_nan(r, S->res_fe);
   }
   S->residual = r;
 }
@@ -2078,7 +2085,11 @@ void compute_iteration(sc_ctx *c) {
                       !c->profiling && !c->batch_member && !c->iter_graph_failed && !no_graph;
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   CUDA_TRY(cudaStreamIsCapturing(c->stream, &cap));
-  if (!steady || cap != cudaStreamCaptureStatusNone) {  // a caller's capture records the eager launches
+  if (cap != cudaStreamCaptureStatusNone) {  // a caller's capture records the launches (sc_compute checked
+    compute_once<R>(c);                      // that the iteration is steady); the own graph stays valid
+    return;
+  }
+  if (!steady) {
     c->drop_graph();
     compute_once<R>(c);
     return;
@@ -2201,6 +2212,13 @@ void ldos_once(sc_ctx *c) {
   k_ldos_finalize<<<c->nb_vp, 256, 0, c->stream>>>(S.n0, nf, c->dom.p, c->ldos_acc.p, blk, c->partial_vp.p);
   check_launch(c);
   launch_scalars_b(c, 1, 1, 0, (size_t)nf * c->nn0());
+}
+
+// Whether the caller is capturing the context's stream into a CUDA graph.
+bool stream_captured(sc_ctx *c) {
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  CUDA_TRY(cudaStreamIsCapturing(c->stream, &cap));
+  return cap != cudaStreamCaptureStatusNone;
 }
 
 void read_scalars(sc_ctx *c) {
@@ -2685,6 +2703,22 @@ int sc_compute(sc_ctx *ctx, int n, double *residual, int *converged) {
     return SC_ERR_STATE;
   }
   API_BEGIN
+  if (stream_captured(ctx)) {
+    // The caller records the iterations into its own CUDA graph.  Only a
+    // steady iteration (the form that replays unchanged) may be recorded, and
+    // nothing is read back: a capture allows no synchronisation.
+    const bool steady = !ctx->first_compute && ctx->boundary_initialized &&
+                        (ctx->frames_zeroed || ctx->chunks.size() > 1) && !ctx->profiling && !ctx->batch_member;
+    if (!steady)
+      throw EngineError(SC_ERR_STATE,
+                        "sc_compute under stream capture: run one iteration outside the capture first "
+                        "(profiling off, not a batch grain)");
+    for (int i = 0; i < n; ++i) {
+      if (ctx->mode == SC_MODE_FP64) compute_iteration<double>(ctx);
+      else compute_iteration<float>(ctx);
+    }
+    return SC_OK;
+  }
   for (int i = 0; i < n; ++i) {
     if (ctx->mode == SC_MODE_FP64) compute_iteration<double>(ctx);
     else compute_iteration<float>(ctx);
@@ -2699,8 +2733,10 @@ int sc_compute(sc_ctx *ctx, int n, double *residual, int *converged) {
 
 int sc_burn_in(sc_ctx *ctx, int n, double *residual, int *converged) {
   if (!ctx || n < 0) return SC_ERR_ARG;
-  ctx->drop_graph();
   API_BEGIN
+  if (stream_captured(ctx))
+    throw EngineError(SC_ERR_STATE, "sc_burn_in: not available under stream capture (it reads the residual back)");
+  ctx->drop_graph();
   for (int i = 0; i < n; ++i) {
     if (ctx->mode == SC_MODE_FP64) burn_in_once<double>(ctx);
     else burn_in_once<float>(ctx);
@@ -2855,6 +2891,13 @@ int sc_get_domain(const sc_ctx *ctx, signed char *domain) {
 int sc_boundary_sizes(const sc_ctx *ctx, int *sizes) {
   if (!ctx || !sizes) return SC_ERR_ARG;
   for (int w = 0; w < 4; ++w) sizes[w] = ctx->n_bnd(w);
+  return SC_OK;
+}
+
+int sc_sweep_plan(const sc_ctx *ctx, int *n_chunks, int *paired) {
+  if (!ctx) return SC_ERR_ARG;
+  if (n_chunks) *n_chunks = (int)ctx->chunks.size();
+  if (paired) *paired = ctx->pair > 0 ? 1 : 0;
   return SC_OK;
 }
 
@@ -3081,6 +3124,7 @@ struct sc_batch {
   int n_sm = 148;
   std::vector<char> active;
   std::vector<int> iterations;
+  std::vector<int> grain_state;  // SC_GRAIN_*: running, converged, at its iteration cap, diverged
   DevArray<double> pool;
   size_t pool_bytes = 0;
   // One launch of the persistent sweep: the work units and SweepArgs<R> of
@@ -3382,11 +3426,21 @@ void batch_step(sc_batch *b) {
     c->host_scalars = b->host_scalars[g];
     b->iterations[g]++;
     const Scalars &s = c->host_scalars;
+    // A grain whose iteration produced a non-finite residual or free energy
+    // has diverged: it is frozen (leaves the batch with its last state, for
+    // inspection) and reported, and the other grains go on unchanged.
+    if (!std::isfinite(s.residual) || !std::isfinite(s.fe)) {
+      b->active[g] = 0;
+      b->grain_state[g] = SC_GRAIN_DIVERGED;
+      changed = true;
+      continue;
+    }
     const bool conv = s.residual < c->S.conv_crit && s.conv_op && s.conv_j && s.conv_fe;
     const bool done = (conv && b->iterations[g] >= c->S.it_min) ||
                       (c->S.it_max >= 0 && b->iterations[g] >= c->S.it_max);
     if (done) {
       b->active[g] = 0;
+      b->grain_state[g] = conv ? SC_GRAIN_CONVERGED : SC_GRAIN_AT_CAP;
       changed = true;
     }
   }
@@ -3457,6 +3511,7 @@ int sc_batch_create(const char *const *configs, int n, int mode, sc_batch **out)
     b->pool.alloc(b->pool_bytes / sizeof(double) + 1);
     b->active.assign(n, 1);
     b->iterations.assign(n, 0);
+    b->grain_state.assign(n, SC_GRAIN_RUNNING);
     std::vector<const Scalars *> src(n);
     for (int i = 0; i < n; ++i) src[i] = b->grains[i]->scalars.p;
     b->scalar_src.upload(src, b->stream);
@@ -3530,6 +3585,12 @@ int sc_batch_status(const sc_batch *b, int *active, int *iterations, double *res
     if (iterations) iterations[g] = b->iterations[g];
     if (residual) residual[g] = b->grains[g]->host_scalars.residual;
   }
+  return SC_OK;
+}
+
+int sc_batch_grain_state(const sc_batch *b, int *state) {
+  if (!b || !state) return SC_ERR_ARG;
+  for (size_t g = 0; g < b->grains.size(); ++g) state[g] = b->grain_state[g];
   return SC_OK;
 }
 

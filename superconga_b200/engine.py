@@ -217,6 +217,12 @@ class Context:
         self._check(_lib.load().sc_boundary_sizes(self._h, s))
         return list(s)
 
+    def sweep_plan(self):
+        """(number of angle chunks, mirror pairing on) of the sweep."""
+        n, p = ctypes.c_int(), ctypes.c_int()
+        self._check(_lib.load().sc_sweep_plan(self._h, ctypes.byref(n), ctypes.byref(p)))
+        return n.value, bool(p.value)
+
     def boundary(self, which: int) -> np.ndarray:
         n = self.boundary_sizes()[which] * self.dims.n_energies
         v = np.zeros(2 * n)
@@ -488,6 +494,16 @@ class Batch:
         res = np.zeros(self.n)
         self._check(_lib.load().sc_batch_status(self._h, _p(act), _p(it), _p(res)))
         return act.astype(bool), it, res
+
+    GRAIN_STATES = ("running", "converged", "at_cap", "diverged")
+
+    def grain_states(self) -> list:
+        """Per grain: 'running', 'converged', 'at_cap' (stopped at its
+        num_iterations_max) or 'diverged' (frozen after a non-finite residual
+        or free energy)."""
+        st = np.zeros(self.n, np.int32)
+        self._check(_lib.load().sc_batch_grain_state(self._h, _p(st)))
+        return [self.GRAIN_STATES[int(v)] for v in st]
 
     def set_graph(self, enable: bool):
         self._check(_lib.load().sc_batch_set_graph(self._h, int(bool(enable))))

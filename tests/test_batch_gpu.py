@@ -187,3 +187,55 @@ def test_batch_low_temperature_grains(engine_lib, mode):
         assert abs(g.scalars()["free_energy"] - e.scalars()["free_energy"]) <= tol * abs(e.scalars()["free_energy"])
         e.close()
     b.close()
+
+
+def test_diverged_grain_is_frozen_and_reported(engine_lib):
+    """A grain whose order parameter holds a NaN (written on the host through
+    its context's set_state; no fault of any kind on the GPU) is reported as
+    diverged after its first iteration and frozen there, while the other
+    grains continue and give the results of a batch without it."""
+    import superconga_b200 as sb
+    cfgs, states = _grains()
+    bad = 1
+    d_bad = states[bad][0].copy()
+    n0 = d_bad.shape[-1]
+    d_bad[0, 0, n0 // 2, n0 // 2] = np.nan  # a site inside the grain
+    b = sb.Batch(cfgs, mode="fp64")
+    for i, (g, (d, a)) in enumerate(zip(b.grains, states)):
+        g.set_state(d_bad if i == bad else d, a)
+    b.compute(3)
+    st = b.grain_states()
+    act, it, res = b.status()
+    assert st[bad] == "diverged"
+    assert it[bad] == 1 and not act[bad] and not np.isfinite(res[bad])
+    assert all(s == "running" for i, s in enumerate(st) if i != bad)
+    assert all(it[i] == 3 for i in range(len(cfgs)) if i != bad)
+    keep = [i for i in range(len(cfgs)) if i != bad]
+    b2 = sb.Batch([cfgs[i] for i in keep], mode="fp64")
+    for g, i in zip(b2.grains, keep):
+        g.set_state(*states[i])
+    b2.compute(3)
+    for g2, i in zip(b2.grains, keep):
+        for x, y in zip(b.grains[i].results(), g2.results()):
+            assert _rel(x, y) < 1e-12
+    b.close()
+    b2.close()
+
+
+def test_nan_state_never_reads_as_converged(engine_lib):
+    """One context with a NaN in its order parameter: the residual of the
+    iteration is not finite and the iteration does not report convergence
+    (the residual maxima keep NaNs; an fmax would drop them)."""
+    import superconga_b200 as sb
+    cfgs, states = _grains()
+    for norm in ("l2", "linf"):
+        cfg = dict(cfgs[0])
+        cfg["numerics"] = dict(cfg["numerics"], norm=norm)
+        d, a = (x.copy() for x in states[0])
+        n0 = d.shape[-1]
+        d[0, 1, n0 // 2, n0 // 2] = np.nan
+        e = sb.Context(cfg, mode="fp64")
+        e.set_state(d, a)
+        res, conv = e.compute(2)
+        assert not np.isfinite(res) and not conv, norm
+        e.close()

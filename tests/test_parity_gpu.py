@@ -478,6 +478,58 @@ def test_iteration_graph_equals_eager(engine_lib, mode):
     assert lg == le
 
 
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+def test_compute_under_caller_capture(engine_lib, mode):
+    """sc_compute on a stream that the caller is capturing into a CUDA graph.
+    On a fresh context (no steady iteration yet) it returns SC_ERR_STATE and
+    records nothing.  After one iteration it records steady iterations into
+    the caller's graph and reads nothing back (residual and convergence flag
+    untouched); three replays of a graph holding one iteration give the state,
+    results and scalars of four eager iterations bit for bit."""
+    import ctypes
+    import torch
+    import superconga_b200 as sb
+    from oracle import oracle as O
+    torch.cuda.set_device(0)
+    cfg = configs.small_disc()
+    s = O.make_setup(cfg)
+    db = O.delta_bulk(s.temperature, s.symmetries[0])
+    d, a = configs.seeded_state(s.n_comp, s.n0, db, 8, 0.05, True, 0.05)
+    ref = sb.Context(cfg, mode=mode)
+    ref.set_state(d, a)
+    ref.compute(4)
+    want = ref.state() + ref.results()
+    want_scalars = ref.scalars()
+    ref.close()
+
+    e = sb.Context(cfg, mode=mode)
+    stream = torch.cuda.Stream()
+    e.set_stream(stream.cuda_stream)
+    e.set_state(d, a)
+    marker = torch.zeros(1, device="cuda")
+    g0 = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g0, stream=stream):
+        marker += 1.0
+        st0 = engine_lib.sc_compute(e._h, 1, None, None)
+    assert st0 == -3  # SC_ERR_STATE: nothing steady to record yet
+    e.compute(1)
+    g = torch.cuda.CUDAGraph()
+    r, c = ctypes.c_double(-7.0), ctypes.c_int(-7)
+    with torch.cuda.graph(g, stream=stream):
+        st = engine_lib.sc_compute(e._h, 1, ctypes.byref(r), ctypes.byref(c))
+    assert st == 0
+    assert r.value == -7.0 and c.value == -7  # nothing read back under capture
+    for _ in range(3):
+        g.replay()
+    torch.cuda.synchronize()
+    got = e.state() + e.results()
+    for x, y in zip(got, want):
+        assert np.array_equal(x, y)
+    assert e.scalars() == want_scalars
+    del g, g0
+    e.close()
+
+
 def _many_energies_disc():
     """The small disc in a field with a self-consistent vector potential at
     T = 0.005 and cutoff 16: 89 Ozaki energies, more than one sweep pass
