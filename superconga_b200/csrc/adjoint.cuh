@@ -93,10 +93,12 @@ __device__ __forceinline__ void riccati_step_adj(double dre, double dim, double 
 
 __device__ __forceinline__ void fields_at(const SweepArgs<double> &A, size_t ni, int item, int r,
                                           double &f0, double &f1, double &f2) {
-  const double *s2 = A.scratch2 + (size_t)r * 3 * ni + item;
+  (void)ni;
+  const size_t T = tile_items(A);
+  const double *s2 = A.scratch2 + fields_index(A, item, r);
   f0 = s2[0];
-  f1 = s2[ni];
-  f2 = s2[2 * ni];
+  f1 = s2[T];
+  f2 = s2[2 * T];
 }
 
 // The adjoint of one trajectory column for the EMAX energies of thread g.

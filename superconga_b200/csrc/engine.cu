@@ -120,6 +120,7 @@ struct SweepArgs {
   int burn_in, has_vp, has_ext, gauge;
   int slot_base;
   int pair;  // angle offset of the mirrored partner angle (n_angles / 2), 0 = unpaired
+  int kmax;  // longest column of the chunk: rows of one scratch tile
   double h, lam_scale, flux_b, q, area;
   const int4 *items;  // (angle, x, first row, last row)
   const AngleParams *ang;
@@ -130,11 +131,30 @@ struct SweepArgs {
   Cx<R> *bout_g, *bout_gt;
   const double2 *rf;   // [n0*n0][nc + 1]: extended order parameter per component, then A (k_pack_reference)
   const double *e_re, *e_im, *res;
-  Cx<R> *scratch;   // [row][energy][item]
-  R *scratch2;      // [row][3][item]: Re D, Im D, energy shift (in R: the sweep steps in R)
+  Cx<R> *scratch;   // [tile][row][energy][item of tile]
+  R *scratch2;      // [tile][row][3][item of tile]: Re D, Im D, energy shift (in R: the sweep steps in R)
   typename FrameOf<R>::type *fg, *gi;  // frame buffers [slot][n1*n1]: (Re F, Im F), (Re G, Re I)
   double *ldf;      // LDOS frame buffer [slot][n1*n1][energy]: Im g per real energy
 };
+
+// Scratch tiles: the items of one warp (32 / G trajectory columns) keep their
+// sweep scratch together, row after row, so the rows a warp steps through are
+// contiguous in memory instead of spread over planes the size of the chunk.
+template <typename R>
+__device__ __forceinline__ size_t tile_items(const SweepArgs<R> &A) { return (size_t)(32 >> A.log_groups); }
+// First element of an item's tile rows: scratch [tile][row][energy][k], fields [tile][row][3][k].
+template <typename R>
+__device__ __forceinline__ size_t scratch_index(const SweepArgs<R> &A, int item, int r, int e) {
+  const int sh = 5 - A.log_groups;
+  const size_t tile = (size_t)(item >> sh), k = (size_t)(item & ((1 << sh) - 1));
+  return (((tile * A.kmax + r) * A.ne + e) << sh) + k;
+}
+template <typename R>
+__device__ __forceinline__ size_t fields_index(const SweepArgs<R> &A, int item, int r) {
+  const int sh = 5 - A.log_groups;
+  const size_t tile = (size_t)(item >> sh), k = (size_t)(item & ((1 << sh) - 1));
+  return (((tile * A.kmax + r) * 3) << sh) + k;
+}
 
 // Gauges, include/conga/riccati/energy_shift/Gauges.h:25-62.
 __device__ __forceinline__ void gauge_potential(int gauge, double b, double area, double x,
@@ -247,16 +267,16 @@ __global__ void __launch_bounds__(FF_COLS * FF_ROWS) k_frame_fields(const SweepA
   const int4 it = A.items[item];
   const int a = it.x, x = it.y, lo = it.z, hi = it.w;
   const AngleParams &P = A.ang[a];  // read in place (a local copy went to the stack)
-  const size_t ni = (size_t)A.n_items;
   const int r0 = blockIdx.y * rows_per_block;
   const int r1 = min(r0 + rows_per_block, hi - lo + 1);
   for (int r = r0 + threadIdx.y; r < r1; r += FF_ROWS) {
     double dre, dim, es;
     frame_fields(A, P, x, lo + r, dre, dim, es);
-    R *s2 = A.scratch2 + (size_t)r * 3 * ni + item;
+    const size_t T = tile_items(A);
+    R *s2 = A.scratch2 + fields_index(A, item, r);
     s2[0] = (R)dre;
-    s2[ni] = (R)dim;
-    s2[2 * ni] = (R)es;
+    s2[T] = (R)dim;
+    s2[2 * T] = (R)es;
   }
 }
 
@@ -334,7 +354,7 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
   const int n1 = A.n1, ne = A.ne;
   const size_t nn1 = (size_t)n1 * n1;
   const uint8_t *lab = A.labels + (size_t)a * nn1;
-  const size_t ni = (size_t)A.n_items;
+  const size_t T = tile_items(A);
   const R h = STEP_PER_ANGLE ? (R)A.ang[a].hs : (R)A.h;  // h / |v_F| of this angle
   const int e0 = g * A.ept;
   int ecount = ne - e0;
@@ -349,6 +369,7 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
   }
 
   Cx<R> coh[EMAX];
+  const size_t sb0 = scratch_index(A, item, 0, e0), s_row = (size_t)ne * T;
   const size_t ax = (size_t)a * n1 + x;
   // Mirrored partner column (angle + pi, x -> n1 - 1 - x) when paired.
   const size_t pax = (size_t)(a + A.pair) * n1 + (n1 - 1 - x);
@@ -361,20 +382,28 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
     R pdre = 0, pdim = 0, pes = 0;
 #pragma unroll
     for (int j = 0; j < EMAX; ++j) coh[j] = Cx<R>{R(0), R(0)};
-    uint8_t l_nx = lab[(size_t)hi * n1 + x];
-    const R *s2 = A.scratch2 + (size_t)(hi - lo) * 3 * ni + item;
-    R f0 = s2[0], f1 = s2[ni], f2 = s2[2 * ni];
+    const uint8_t *lcol = lab + x;
+    const R *fb = A.scratch2 + fields_index(A, item, 0);
+    const size_t f_row = 3 * T;
+    uint8_t l_nx = lcol[(size_t)hi * n1];
+    R f0, f1, f2;
+    {
+      const R *s2 = fb + (size_t)(hi - lo) * f_row;
+      f0 = s2[0];
+      f1 = s2[T];
+      f2 = s2[2 * T];
+    }
     for (int y = hi; y >= lo; --y) {
       const int r = y - lo;
       const uint8_t l = l_nx;
       // gammaTilde uses -conj(Delta) (RiccatiSolverConfined.h:74-79).
       const R dre = (R)(-f0), dim = (R)f1, es = (R)f2;
       if (y > lo) {
-        l_nx = lab[(size_t)(y - 1) * n1 + x];
-        const R *s2n = A.scratch2 + (size_t)(r - 1) * 3 * ni + item;
+        l_nx = lcol[(size_t)(y - 1) * n1];
+        const R *s2n = fb + (size_t)(r - 1) * f_row;
         f0 = s2n[0];
-        f1 = s2n[ni];
-        f2 = s2n[2 * ni];
+        f1 = s2n[T];
+        f2 = s2n[2 * T];
       }
       if (l == 1) {
         interior_step<R, EMAX, KEL>(dre, dim, es, pdre, pdim, pes, ere, eim, coh, A.ept, h);
@@ -397,10 +426,10 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
         nout += exit;
       }
       if (!A.burn_in) {
-        Cx<R> *sc = A.scratch + (size_t)r * ne * ni + (size_t)e0 * ni + item;
+        Cx<R> *sc = A.scratch + sb0 + (size_t)r * s_row;
 #pragma unroll
         for (int j = 0; j < EMAX; ++j)
-          if (j < ecount) sc[(size_t)j * ni] = coh[j];
+          if (j < ecount) sc[(size_t)j * T] = coh[j];
       }
       pdre = dre;
       pdim = dim;
@@ -417,14 +446,17 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
     using Fr = typename FrameOf<R>::type;
     Fr *fg = A.fg + (size_t)(a - A.slot_base) * nn1;
     Fr *gi = A.gi + (size_t)(a - A.slot_base) * nn1;
-    uint8_t l_nx = lab[(size_t)lo * n1 + x];
-    R f0 = A.scratch2[item], f1 = A.scratch2[ni + item], f2 = A.scratch2[2 * ni + item];
+    const uint8_t *lcol = lab + x;
+    const R *fb = A.scratch2 + fields_index(A, item, 0);
+    const size_t f_row = 3 * T;
+    uint8_t l_nx = lcol[(size_t)lo * n1];
+    R f0 = fb[0], f1 = fb[T], f2 = fb[2 * T];
     Cx<R> gt_nx[EMAX];
     if (!A.burn_in) {
-      const Cx<R> *sc = A.scratch + (size_t)e0 * ni + item;
+      const Cx<R> *sc = A.scratch + sb0;
 #pragma unroll
       for (int j = 0; j < EMAX; ++j)
-        if (j < ecount) gt_nx[j] = sc[(size_t)j * ni];
+        if (j < ecount) gt_nx[j] = sc[(size_t)j * T];
     }
     for (int y = lo; y <= hi; ++y) {
       const int r = y - lo;
@@ -434,16 +466,16 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
 #pragma unroll
       for (int j = 0; j < EMAX; ++j) gt[j] = gt_nx[j];
       if (y < hi) {
-        l_nx = lab[(size_t)(y + 1) * n1 + x];
-        const R *s2n = A.scratch2 + (size_t)(r + 1) * 3 * ni + item;
+        l_nx = lcol[(size_t)(y + 1) * n1];
+        const R *s2n = fb + (size_t)(r + 1) * f_row;
         f0 = s2n[0];
-        f1 = s2n[ni];
-        f2 = s2n[2 * ni];
+        f1 = s2n[T];
+        f2 = s2n[2 * T];
         if (!A.burn_in) {
-          const Cx<R> *sc = A.scratch + (size_t)(r + 1) * ne * ni + (size_t)e0 * ni + item;
+          const Cx<R> *sc = A.scratch + sb0 + (size_t)(r + 1) * s_row;
 #pragma unroll
           for (int j = 0; j < EMAX; ++j)
-            if (j < ecount) gt_nx[j] = sc[(size_t)j * ni];
+            if (j < ecount) gt_nx[j] = sc[(size_t)j * T];
         }
       }
       if (l == 1) {
@@ -1655,6 +1687,7 @@ SweepArgs<R> sweep_args(sc_ctx *c, const Chunk *ch, int burn_in) {
   A.has_ext = std::fabs(A.flux_b) > 0.0;
   A.gauge = S.gauge;
   A.slot_base = ch ? ch->a_begin : 0;
+  A.kmax = ch ? ch->kmax : 0;
   A.pair = (ch && ch->a_begin == 0 && ch->a_end == S.n_angles) ? c->pair : 0;
   A.h = S.h;
   A.lam_scale = c->has_vp() ? 1.0 / (S.lambda * S.lambda) : 0.0;
@@ -1698,12 +1731,13 @@ void launch_frame_fields(sc_ctx *c, const Chunk &ch, const SweepArgs<R> &A) {
 
 template <typename R>
 void launch_sweep_pass(sc_ctx *c, const SweepArgs<R> &A, unsigned blocks) {
-  // Resident blocks per SM, fastest measured on B200 (606 x 606 d-wave square,
-  // 256 angles, 14 energies): FP64 three (four energies per thread, 158
-  // registers, no spills: 35.4 ms against 36.3 with four blocks), mixed four
-  // (two energies per thread: 10.5 ms against 11.2 with five or six blocks).
+  // Resident blocks per SM, fastest measured on B200 with the tiled scratch
+  // (606 x 606 d-wave square, 256 angles, 14 energies): FP64 three (four
+  // energies per thread, 158 registers: 24.6 ms against 28.6 with four blocks
+  // and 29.9 with two), mixed five (two energies per thread: 8.70 ms against
+  // 8.79 with six and 8.93 with four).
   static const char *minb_env = std::getenv("SCB_SWEEP_MINB");
-  const int variant = minb_env ? std::atoi(minb_env) : (sizeof(R) == 8 ? 3 : (c->emax2 ? 4 : 1));
+  const int variant = minb_env ? std::atoi(minb_env) : (sizeof(R) == 8 ? 3 : (c->emax2 ? 5 : 1));
   if (c->S.fs_tight_binding) {
     // Non-circular Fermi surface: per-angle step, generic mappings.
     if (c->S.keldysh) {
@@ -2465,8 +2499,9 @@ void upload_static(sc_ctx *c) {
   int max_slots = 1;
   for (const Chunk &ch : c->chunks) {
     const size_t ni = (size_t)(ch.item_end - ch.item_begin);
-    scr = std::max(scr, ni * ch.kmax * c->e_pass * c->esize());
-    scr2 = std::max(scr2, ni * ch.kmax * 3);
+    const size_t ni32 = (ni + 31) / 32 * 32;  // whole scratch tiles
+    scr = std::max(scr, ni32 * ch.kmax * c->e_pass * c->esize());
+    scr2 = std::max(scr2, ni32 * ch.kmax * 3);
     max_slots = std::max(max_slots, chunk_slots(c, ch));
   }
   c->need_scratch = scr + 8;
