@@ -280,10 +280,12 @@ def _curl(a, h):
     return (day - dax) / h
 
 
-def converge_c1(max_it: int, max_s: float):
+def converge_c1(max_it: int, max_s: float, extra_it: int = 400):
     """Time to converge (residual 1e-6) of the C1 disc in both precisions from
     the same seeded start, and the distance of the mixed solution from the FP64
-    one in Delta, j, B and Omega."""
+    one in Delta, j, B and Omega: where both runs stop at the criterion, and
+    after both continue for extra_it more iterations towards their fixed
+    points (with the FP64 run's own distance between the two for scale)."""
     import numpy as np
     import superconga_b200 as sb
     from superconga_b200 import workloads
@@ -308,8 +310,18 @@ def converge_c1(max_it: int, max_s: float):
         d, j, _ = ctx.results()
         _, a = ctx.state()
         sol[mode] = (d, j, a, ctx.scalars()["free_energy"])
+        # Then on towards the fixed point itself: the difference of the two
+        # runs at the criterion is mostly where each stopped.
+        res2, _ = ctx.compute(extra_it)
+        d, j, _ = ctx.results()
+        _, a = ctx.state()
+        sol[mode + "_fp"] = (d, j, a, ctx.scalars()["free_energy"])
+        out[mode]["residual_after_more"] = res2
         ctx.close()
     out["mixed_vs_fp64"] = _field_errors(cfg, "s", sol["fp64"], sol["mixed"])
+    out["continued_iterations"] = extra_it
+    out["mixed_vs_fp64_continued"] = _field_errors(cfg, "s", sol["fp64_fp"], sol["mixed_fp"])
+    out["fp64_at_criterion_vs_continued"] = _field_errors(cfg, "s", sol["fp64_fp"], sol["fp64"])
     out["speedup_mixed_over_fp64"] = out["fp64"]["seconds"] / out["mixed"]["seconds"]
     out["workload"] = "c1: s-wave disc R=10 xi0 @10/xi0, 64 angles, T=0.5, b=0.02 B0, kappa=2"
     return out

@@ -103,8 +103,8 @@ __device__ __forceinline__ Cx<R> riccati_step(R dre, R dim, R ere, R eim, Cx<R> 
   const Cx<R> tg = cmul(t, g);
   const Cx<R> c{tg.re - h * dim, tg.im + h * dre};
   const R bm = ser - R(1);
-  const R hd2 = h * h * (dre * dre + dim * dim);
-  const Cx<R> disc = csqrt_dev<R>(bm * bm - sei * sei + hd2 - R(8) * ag.re, R(2) * bm * sei - R(8) * ag.im);
+  const R s0 = h * h * (dre * dre + dim * dim) - sei * sei;  // the site's part: shared by all energies
+  const Cx<R> disc = csqrt_dev<R>((bm * bm + s0) - R(8) * ag.re, (R(2) * bm) * sei - R(8) * ag.im);
   const R den_re = disc.re - b.re, den_im = disc.im - b.im;
   const R inv = rcp_(den_re * den_re + den_im * den_im);
   const R c2r = R(2) * c.re, c2i = R(2) * c.im;
@@ -127,24 +127,24 @@ __device__ __forceinline__ void riccati_homogeneous(R dre, R dim, R ere, R eim, 
 
 // Local Green functions of one energy (LocalGreens.h:32-70) and the free-energy
 // kernel (ComputeFreeEnergy.h:95-103): returns f + f~* in F, Re g and Im I.
+// With p = g gt and w = 2 / |1 + p|^2, the common factor i 2 / (1 + p) of f
+// and f~ is fac = w (Im p, 1 + Re p), and
+//   Re g = Re[-i (1 - p) / (1 + p)] = -2 Im p / |1 + p|^2 = -Re fac,
+//   f + f~* = -fac g + conj(fac gt) = (Re[fac (gt - g)], -Im[fac (g + gt)]),
+//   Im I = Im[conj(D) g - D gt] = Re D Im(g - gt) - Im D Re(g + gt),
+// the same quantities as the reference's in fewer operations.
 template <typename R>
 __device__ __forceinline__ void local_greens(Cx<R> g, Cx<R> gt, R dre, R dim, Cx<R> &F,
                                              R &g_re, R &i_im) {
   const Cx<R> p = cmul(g, gt);
   const R den_re = R(1) + p.re, den_im = p.im;
-  const R inv = rcp_(den_re * den_re + den_im * den_im);
-  // (1 - p) / (1 + p)
-  const R nr = R(1) - p.re, ni = -p.im;
-  const R q_im = (ni * den_re - nr * den_im) * inv;
-  g_re = q_im;  // g = -i (1 - p) / (1 + p)
-  // 2 / (1 + p) and factor = i * 2 / (1 + p)
-  const R t2r = R(2) * den_re * inv, t2i = -R(2) * den_im * inv;
-  const Cx<R> fac{-t2i, t2r};
-  const Cx<R> fg = cmul(fac, g);
-  const Cx<R> fgt = cmul(fac, gt);
-  F = Cx<R>{-fg.re + fgt.re, -fg.im - fgt.im};
-  // I = conj(D) g - D g~
-  i_im = (dre * g.im - dim * g.re) - (dre * gt.im + dim * gt.re);
+  const R w = R(2) * rcp_(den_re * den_re + den_im * den_im);
+  const R fre = den_im * w, fim = den_re * w;
+  g_re = -fre;
+  const R ure = gt.re - g.re, uim = gt.im - g.im;  // gt - g
+  const R vre = g.re + gt.re, vim = g.im + gt.im;  // g + gt
+  F = Cx<R>{fre * ure - fim * uim, -(fre * vim + fim * vre)};
+  i_im = -(dre * uim + dim * vre);
 }
 
 // Im g of one real energy, g = -i (1 - g gt) / (1 + g gt) (LocalGreens.h:32-43).
