@@ -2041,11 +2041,15 @@ void frame_to_reference(sc_ctx *c, const Chunk &ch) {
 template <typename R>
 void run_chunks_ldos(sc_ctx *c, int burn_in) {
   const HostSetup &S = c->S;
-  const size_t nn1 = (size_t)S.n1 * S.n1;
+  // The LDOS frame buffer is not cleared between chunks or iterations: the
+  // sweep rewrites every grain site of the chunk's angles and the extension
+  // every site next to the grain, and those are the only frame sites that the
+  // bilinear rotation back reads for a site inside the grain; sites outside
+  // the grain may read values left by other angles, and k_ldos_finalize
+  // discards them.  (The buffer is zeroed once at creation, so every value in
+  // it is finite.)  Clearing 32 energies x N1^2 sites for every angle cost
+  // about as much as the sweep itself on large grains.
   for (const Chunk &ch : c->chunks) {
-    const int nslots = ch.a_end - ch.a_begin;
-    if (!burn_in)
-      CUDA_TRY(cudaMemsetAsync(c->ldf.p, 0, (size_t)nslots * S.ne * nn1 * sizeof(double), c->stream));
     launch_sweep<R>(c, ch, burn_in);
     if (burn_in) continue;
     const int h0 = S.halo_angle_off[ch.a_begin], h1 = S.halo_angle_off[ch.a_end];
@@ -2515,6 +2519,7 @@ void upload_static(sc_ctx *c) {
     c->w_scratch = c->scratch.p;
     c->w_scratch2 = c->scratch2.p;
     c->ldf.alloc((size_t)max_slots * S.ne * n1 * n1);
+    c->ldf.zero(s);  // once: afterwards every slot holds finite values (see run_chunks_ldos)
     c->ldos_acc.alloc((size_t)S.ne * nn);
     c->ldos_all.alloc((size_t)S.ldos_n_blocks * S.ldos_block * nn);
     c->ldos_all.zero(s);

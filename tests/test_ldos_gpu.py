@@ -77,20 +77,31 @@ def test_ldos_block_passes(engine_lib):
     assert _rel(e.ldos(), L.ldos) < TOL
 
 
-def test_ldos_d_wave_square(engine_lib):
-    """d-wave square with pair-breaking edges, vector potential, one block."""
+@pytest.mark.parametrize("scratch_mb", [None, 1], ids=["one_chunk", "chunked"])
+def test_ldos_d_wave_square(engine_lib, monkeypatch, scratch_mb):
+    """d-wave square with pair-breaking edges, vector potential, two blocks;
+    once with all angles in one chunk and once in many (a 1 MB budget): the
+    LDOS frame buffer is reused across chunks and iterations without being
+    cleared, and the LDOS inside the grain must not depend on it."""
     sim = configs.small_square_d()
     from oracle import oracle as O
+    if scratch_mb is None:
+        monkeypatch.delenv("SCB_SCRATCH_MB", raising=False)
+    else:
+        monkeypatch.setenv("SCB_SCRATCH_MB", str(scratch_mb))
     db = O.delta_bulk(0.1, "dx2-y2")
-    pp = configs.ldos_postprocess(db, n_energies=8, per_block=8, n_angles=24, broadening=0.03)
+    pp = configs.ldos_postprocess(db, n_energies=16, per_block=8, n_angles=24, broadening=0.03)
     L, e, _ = _pair(sim, pp, seed=3)
-    L.begin_block(0)
-    e.begin_block(0)
-    L.burn_in()
-    e.burn_in(1)
-    for _ in range(2):
-        L.iterate()
-        e.iterate(1)
+    n_chunks, _ = e.sweep_plan()
+    assert (n_chunks == 1) if scratch_mb is None else (n_chunks >= 4), n_chunks
+    for b in range(2):
+        L.begin_block(b)
+        e.begin_block(b)
+        L.burn_in()
+        e.burn_in(1)
+        for _ in range(2):
+            L.iterate()
+            e.iterate(1)
     assert _rel(e.ldos(), L.ldos) < TOL
 
 
