@@ -94,11 +94,10 @@ __device__ __forceinline__ void riccati_step_adj(double dre, double dim, double 
 __device__ __forceinline__ void fields_at(const SweepArgs<double> &A, size_t ni, int item, int r,
                                           double &f0, double &f1, double &f2) {
   (void)ni;
-  const size_t T = tile_items(A);
-  const double *s2 = A.scratch2 + fields_index(A, item, r);
-  f0 = s2[0];
-  f1 = s2[T];
-  f2 = s2[2 * T];
+  const double4 v = ((const double4 *)A.scratch2)[rec_index(A, A.log_groups, item, r)];
+  f0 = v.x;
+  f1 = v.y;
+  f2 = v.z;
 }
 
 // The adjoint of one trajectory column for the EMAX energies of thread g.

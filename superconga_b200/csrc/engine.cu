@@ -132,28 +132,32 @@ struct SweepArgs {
   const double2 *rf;   // [n0*n0][nc + 1]: extended order parameter per component, then A (k_pack_reference)
   const double *e_re, *e_im, *res;
   Cx<R> *scratch;   // [tile][row][energy][item of tile]
-  R *scratch2;      // [tile][row][3][item of tile]: Re D, Im D, energy shift (in R: the sweep steps in R)
+  R *scratch2;      // frame-field records [tile][row][item of tile] of (Re D, Im D, energy shift, label), in R
   typename FrameOf<R>::type *fg, *gi;  // frame buffers [slot][n1*n1]: (Re F, Im F), (Re G, Re I)
   double *ldf;      // LDOS frame buffer [slot][n1*n1][energy]: Im g per real energy
 };
 
-// Scratch tiles: the items of one warp (32 / G trajectory columns) keep their
-// sweep scratch together, row after row, so the rows a warp steps through are
-// contiguous in memory instead of spread over planes the size of the chunk.
+// Scratch tiles: the items of one warp (32 / G trajectory columns, G = 2^lg
+// threads per column) keep their sweep scratch together, row after row, so the
+// rows a warp steps through are contiguous in memory instead of spread over
+// planes the size of the chunk: gammaTilde [tile][row][energy][column of tile].
 template <typename R>
-__device__ __forceinline__ size_t tile_items(const SweepArgs<R> &A) { return (size_t)(32 >> A.log_groups); }
-// First element of an item's tile rows: scratch [tile][row][energy][k], fields [tile][row][3][k].
-template <typename R>
-__device__ __forceinline__ size_t scratch_index(const SweepArgs<R> &A, int item, int r, int e) {
-  const int sh = 5 - A.log_groups;
+__device__ __forceinline__ size_t scratch_index(const SweepArgs<R> &A, int lg, int item, int r, int e) {
+  const int sh = 5 - lg;
   const size_t tile = (size_t)(item >> sh), k = (size_t)(item & ((1 << sh) - 1));
   return (((tile * A.kmax + r) * A.ne + e) << sh) + k;
 }
+// Frame-field records, one per column site in the same tiles: (Re D, Im D,
+// energy shift, frame label), [tile][row][column of tile], read by the sweep
+// with one vector load per site.
+template <typename R> struct Rec4;
+template <> struct Rec4<double> { using type = double4; };
+template <> struct Rec4<float> { using type = float4; };
 template <typename R>
-__device__ __forceinline__ size_t fields_index(const SweepArgs<R> &A, int item, int r) {
-  const int sh = 5 - A.log_groups;
+__device__ __forceinline__ size_t rec_index(const SweepArgs<R> &A, int lg, int item, int r) {
+  const int sh = 5 - lg;
   const size_t tile = (size_t)(item >> sh), k = (size_t)(item & ((1 << sh) - 1));
-  return (((tile * A.kmax + r) * 3) << sh) + k;
+  return ((tile * A.kmax + r) << sh) + k;
 }
 
 // Gauges, include/conga/riccati/energy_shift/Gauges.h:25-62.
@@ -255,7 +259,8 @@ __device__ __forceinline__ void group_sum4_scatter(double v[4], int g, int log_g
 }
 
 // Rotated order parameter and Doppler shift of every site of every trajectory
-// column of a chunk, written to scratch2[row][3][item] for the sweep.
+// column of a chunk, written with the site's frame label as one record per
+// site (rec_index) for the sweep.
 // Block (FF_COLS, FF_ROWS): a warp covers 8 neighbouring columns x 4 rows, a
 // compact patch of the frame whose rotated corners fall on few cache lines of
 // the reference grid (a warp along one row touched ~20 sectors per gather).
@@ -272,11 +277,9 @@ __global__ void __launch_bounds__(FF_COLS * FF_ROWS) k_frame_fields(const SweepA
   for (int r = r0 + threadIdx.y; r < r1; r += FF_ROWS) {
     double dre, dim, es;
     frame_fields(A, P, x, lo + r, dre, dim, es);
-    const size_t T = tile_items(A);
-    R *s2 = A.scratch2 + fields_index(A, item, r);
-    s2[0] = (R)dre;
-    s2[T] = (R)dim;
-    s2[2 * T] = (R)es;
+    const uint8_t lab = A.labels[(size_t)a * A.n1 * A.n1 + (size_t)(lo + r) * A.n1 + x];
+    typedef typename Rec4<R>::type V4;
+    ((V4 *)A.scratch2)[rec_index(A, A.log_groups, item, r)] = V4{(R)dre, (R)dim, (R)es, (R)lab};
   }
 }
 
@@ -346,15 +349,15 @@ __device__ __forceinline__ void interior_step(R dre, R dim, R es, R pdre, R pdim
 // STEP_PER_ANGLE: the Riccati step h/|v_F| is read per angle (a non-circular
 // Fermi surface, and the batch); otherwise it is the uniform lattice spacing h
 // of the circle, which stays a kernel parameter.
-template <typename R, int EMAX, bool KEL, bool STEP_PER_ANGLE>
+template <typename R, int EMAX, bool KEL, bool STEP_PER_ANGLE, int LG = -1>
 __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double *s_res, int item,
                                              int g, unsigned gmask) {
+  const int lgc = LG >= 0 ? LG : A.log_groups;  // a compile-time group size when the launch knows it
   const int4 it = A.items[item];
   const int a = it.x, x = it.y, lo = it.z, hi = it.w;
   const int n1 = A.n1, ne = A.ne;
   const size_t nn1 = (size_t)n1 * n1;
-  const uint8_t *lab = A.labels + (size_t)a * nn1;
-  const size_t T = tile_items(A);
+  const size_t T = (size_t)(32 >> lgc);
   const R h = STEP_PER_ANGLE ? (R)A.ang[a].hs : (R)A.h;  // h / |v_F| of this angle
   const int e0 = g * A.ept;
   int ecount = ne - e0;
@@ -369,7 +372,7 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
   }
 
   Cx<R> coh[EMAX];
-  const size_t sb0 = scratch_index(A, item, 0, e0), s_row = (size_t)ne * T;
+  const size_t sb0 = scratch_index(A, lgc, item, 0, e0), s_row = (size_t)ne * T;
   const size_t ax = (size_t)a * n1 + x;
   // Mirrored partner column (angle + pi, x -> n1 - 1 - x) when paired.
   const size_t pax = (size_t)(a + A.pair) * n1 + (n1 - 1 - x);
@@ -382,29 +385,15 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
     R pdre = 0, pdim = 0, pes = 0;
 #pragma unroll
     for (int j = 0; j < EMAX; ++j) coh[j] = Cx<R>{R(0), R(0)};
-    const uint8_t *lcol = lab + x;
-    const R *fb = A.scratch2 + fields_index(A, item, 0);
-    const size_t f_row = 3 * T;
-    uint8_t l_nx = lcol[(size_t)hi * n1];
-    R f0, f1, f2;
-    {
-      const R *s2 = fb + (size_t)(hi - lo) * f_row;
-      f0 = s2[0];
-      f1 = s2[T];
-      f2 = s2[2 * T];
-    }
+    typedef typename Rec4<R>::type V4;
+    const V4 *fb = (const V4 *)A.scratch2 + rec_index(A, lgc, item, 0);
+    V4 fr = fb[(size_t)(hi - lo) * T];
     for (int y = hi; y >= lo; --y) {
       const int r = y - lo;
-      const uint8_t l = l_nx;
+      const uint8_t l = (uint8_t)fr.w;
       // gammaTilde uses -conj(Delta) (RiccatiSolverConfined.h:74-79).
-      const R dre = (R)(-f0), dim = (R)f1, es = (R)f2;
-      if (y > lo) {
-        l_nx = lcol[(size_t)(y - 1) * n1];
-        const R *s2n = fb + (size_t)(r - 1) * f_row;
-        f0 = s2n[0];
-        f1 = s2n[T];
-        f2 = s2n[2 * T];
-      }
+      const R dre = (R)(-fr.x), dim = (R)fr.y, es = (R)fr.z;
+      if (y > lo) fr = fb[(size_t)(r - 1) * T];
       if (l == 1) {
         interior_step<R, EMAX, KEL>(dre, dim, es, pdre, pdim, pes, ere, eim, coh, A.ept, h);
       } else {
@@ -446,11 +435,9 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
     using Fr = typename FrameOf<R>::type;
     Fr *fg = A.fg + (size_t)(a - A.slot_base) * nn1;
     Fr *gi = A.gi + (size_t)(a - A.slot_base) * nn1;
-    const uint8_t *lcol = lab + x;
-    const R *fb = A.scratch2 + fields_index(A, item, 0);
-    const size_t f_row = 3 * T;
-    uint8_t l_nx = lcol[(size_t)lo * n1];
-    R f0 = fb[0], f1 = fb[T], f2 = fb[2 * T];
+    typedef typename Rec4<R>::type V4;
+    const V4 *fb = (const V4 *)A.scratch2 + rec_index(A, lgc, item, 0);
+    V4 fr = fb[0];
     Cx<R> gt_nx[EMAX];
     if (!A.burn_in) {
       const Cx<R> *sc = A.scratch + sb0;
@@ -460,17 +447,13 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
     }
     for (int y = lo; y <= hi; ++y) {
       const int r = y - lo;
-      const uint8_t l = l_nx;
-      const R dre = (R)f0, dim = (R)f1, es = (R)f2;
+      const uint8_t l = (uint8_t)fr.w;
+      const R dre = (R)fr.x, dim = (R)fr.y, es = (R)fr.z;
       Cx<R> gt[EMAX];
 #pragma unroll
       for (int j = 0; j < EMAX; ++j) gt[j] = gt_nx[j];
       if (y < hi) {
-        l_nx = lcol[(size_t)(y + 1) * n1];
-        const R *s2n = fb + (size_t)(r + 1) * f_row;
-        f0 = s2n[0];
-        f1 = s2n[T];
-        f2 = s2n[2 * T];
+        fr = fb[(size_t)(r + 1) * T];
         if (!A.burn_in) {
           const Cx<R> *sc = A.scratch + sb0 + (size_t)(r + 1) * s_row;
 #pragma unroll
@@ -530,7 +513,7 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
       // from this frame at the mirrored site.
       const size_t fi = (size_t)y * n1 + x;
       double v[4] = {sfr, sfi, sg, -si};
-      const int lg = A.log_groups;
+      const int lg = lgc;
       group_sum4_scatter(v, g, lg, gmask);
       if (lg == 0) {
         if (A.accumulate) {
@@ -563,19 +546,19 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
   }
 }
 
-template <typename R, int EMAX, int MINB, bool KEL, bool STEP_PER_ANGLE = false>
+template <typename R, int EMAX, int MINB, bool KEL, bool STEP_PER_ANGLE = false, int LG = -1>
 __global__ void __launch_bounds__(128, MINB) k_sweep(const SweepArgs<R> A) {
   __shared__ double s_res[SWEEP_MAX_ENERGIES];  // residues of this pass's energies
   for (int e = threadIdx.x; e < A.ne && e < SWEEP_MAX_ENERGIES; e += blockDim.x) s_res[e] = A.res[e];
   __syncthreads();
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-  const int item = tid >> A.log_groups;
-  const int g = tid & (A.groups - 1);
+  const int lgk = LG >= 0 ? LG : A.log_groups, groups = 1 << lgk;
+  const int item = tid >> lgk;
+  const int g = tid & (groups - 1);
   const int lane = threadIdx.x & 31;
-  const unsigned gmask = ((A.groups == 32) ? 0xffffffffu : ((1u << A.groups) - 1u))
-                         << (lane & ~(A.groups - 1));
+  const unsigned gmask = ((groups == 32) ? 0xffffffffu : ((1u << groups) - 1u)) << (lane & ~(groups - 1));
   if (item >= A.n_items) return;  // whole groups leave together (groups divide the warp)
-  sweep_column<R, EMAX, KEL, STEP_PER_ANGLE>(A, s_res, item, g, gmask);
+  sweep_column<R, EMAX, KEL, STEP_PER_ANGLE, LG>(A, s_res, item, g, gmask);
 }
 
 // The sweep of many grains in one persistent launch.  A work unit is one
@@ -1736,6 +1719,11 @@ void launch_sweep_pass(sc_ctx *c, const SweepArgs<R> &A, unsigned blocks) {
   // energies per thread, 158 registers: 24.6 ms against 28.6 with four blocks
   // and 29.9 with two), mixed five (two energies per thread: 8.70 ms against
   // 8.79 with six and 8.93 with four).
+  // The common mappings (FP64: four energies per thread, four threads per
+  // column; mixed and LDOS: eight threads per column) are compiled with the
+  // group size fixed, which turns the per-site group reduction, frame store
+  // and tile addressing into straight-line code (C2: FP64 sweep -5%, mixed
+  // -12%); other mappings take it at run time.
   static const char *minb_env = std::getenv("SCB_SWEEP_MINB");
   const int variant = minb_env ? std::atoi(minb_env) : (sizeof(R) == 8 ? 3 : (c->emax2 ? 5 : 1));
   if (c->S.fs_tight_binding) {
@@ -1750,17 +1738,20 @@ void launch_sweep_pass(sc_ctx *c, const SweepArgs<R> &A, unsigned blocks) {
       else k_sweep<R, 16, 1, false, true><<<blocks, 128, 0, c->stream>>>(A);
     }
   } else if (c->S.keldysh) {
-    if (c->ept <= 4) k_sweep<R, 4, 1, true><<<blocks, 128, 0, c->stream>>>(A);
+    if (c->ept <= 4 && c->log_groups == 3) k_sweep<R, 4, 1, true, false, 3><<<blocks, 128, 0, c->stream>>>(A);
+    else if (c->ept <= 4) k_sweep<R, 4, 1, true><<<blocks, 128, 0, c->stream>>>(A);
     else if (c->ept <= 8) k_sweep<R, 8, 1, true><<<blocks, 128, 0, c->stream>>>(A);
     else k_sweep<R, 16, 1, true><<<blocks, 128, 0, c->stream>>>(A);
   } else if (c->ept <= 2 && c->emax2) {
     if (variant >= 6) k_sweep<R, 2, 6, false><<<blocks, 128, 0, c->stream>>>(A);
+    else if (variant == 5 && c->log_groups == 3) k_sweep<R, 2, 5, false, false, 3><<<blocks, 128, 0, c->stream>>>(A);
     else if (variant == 5) k_sweep<R, 2, 5, false><<<blocks, 128, 0, c->stream>>>(A);
     else if (variant == 3) k_sweep<R, 2, 3, false><<<blocks, 128, 0, c->stream>>>(A);
     else k_sweep<R, 2, 4, false><<<blocks, 128, 0, c->stream>>>(A);
   } else if (c->ept <= 4) {
     if (variant == 4) k_sweep<R, 4, 4, false><<<blocks, 128, 0, c->stream>>>(A);
     else if (variant == 5) k_sweep<R, 4, 5, false><<<blocks, 128, 0, c->stream>>>(A);
+    else if (variant == 3 && c->log_groups == 2) k_sweep<R, 4, 3, false, false, 2><<<blocks, 128, 0, c->stream>>>(A);
     else if (variant == 3) k_sweep<R, 4, 3, false><<<blocks, 128, 0, c->stream>>>(A);
     else k_sweep<R, 4, 1, false><<<blocks, 128, 0, c->stream>>>(A);
   } else if (c->ept <= 8) {
@@ -2505,7 +2496,7 @@ void upload_static(sc_ctx *c) {
     const size_t ni = (size_t)(ch.item_end - ch.item_begin);
     const size_t ni32 = (ni + 31) / 32 * 32;  // whole scratch tiles
     scr = std::max(scr, ni32 * ch.kmax * c->e_pass * c->esize());
-    scr2 = std::max(scr2, ni32 * ch.kmax * 3);
+    scr2 = std::max(scr2, ni32 * ch.kmax * 4);
     max_slots = std::max(max_slots, chunk_slots(c, ch));
   }
   c->need_scratch = scr + 8;
