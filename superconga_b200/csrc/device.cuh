@@ -57,8 +57,11 @@ __device__ __forceinline__ double rsqrt_(double x) {
   return fma(r, e * fma(0.375, e, 0.5), r);
 }
 __device__ __forceinline__ float rsqrt_(float x) { return rsqrtf(x); }
+// FP64 square root of a non-negative argument as x / sqrt(x); the estimate is
+// taken of max(x, smallest normal), which gives 0 for x = 0 with no branch and
+// leaves every normal argument unchanged.
 __device__ __forceinline__ double sqrt_(double x) {
-  return x >= 2.2250738585072014e-308 ? x * rsqrt_(x) : 0.0;  // 0 below the smallest normal
+  return x * rsqrt_(fmax(x, 2.2250738585072014e-308));
 }
 // FP32 square root of a non-negative argument: the hardware approximation
 // (sqrt.approx; 0 for 0), one instruction.
@@ -72,12 +75,13 @@ __device__ __forceinline__ float sqrt_(float x) {
 // square root and one reciprocal square root:
 //   u = (|z| + |x|)/2, t = sqrt(u), v = |y| / (2 t);
 //   sqrt(z) = (t, sign(y) v) for x >= 0 and (v, sign(y) t) otherwise.
+// u = 0 only for z = 0, where the estimate of max(u, smallest normal) is
+// finite and t = v = 0: the root 0 with no branch.
 template <typename R>
 __device__ __forceinline__ Cx<R> csqrt_dev(R x, R y) {
   const R m = sqrt_(x * x + y * y);
   const R u = R(0.5) * (m + fabs(x));
-  if (!(u > R(0))) return Cx<R>{R(0), y};
-  const R r = rsqrt_(u);
+  const R r = rsqrt_(fmax(u, R(sizeof(R) == 8 ? 2.2250738585072014e-308 : 1.17549435e-38)));
   const R t = u * r;
   const R v = R(0.5) * fabs(y) * r;
   const bool pos = x >= R(0);

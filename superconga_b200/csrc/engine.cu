@@ -359,9 +359,14 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
   const size_t nn1 = (size_t)n1 * n1;
   const size_t T = (size_t)(32 >> lgc);
   const R h = STEP_PER_ANGLE ? (R)A.ang[a].hs : (R)A.h;  // h / |v_F| of this angle
-  const int e0 = g * A.ept;
+  // A compile-time group size comes with a full load (EMAX energies per
+  // thread), a sweep that stores its frame sums, and no energy passes.
+  const int ept = LG >= 0 ? EMAX : A.ept;
+  const bool burn_in = LG >= 0 ? false : A.burn_in != 0;
+  const bool accumulate = LG >= 0 ? false : A.accumulate != 0;
+  const int e0 = g * ept;
   int ecount = ne - e0;
-  if (ecount > A.ept) ecount = A.ept;
+  if (ecount > ept) ecount = ept;
   if (ecount < 0) ecount = 0;
 
   R eim[EMAX], ere[EMAX];
@@ -395,12 +400,12 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
       const R dre = (R)(-fr.x), dim = (R)fr.y, es = (R)fr.z;
       if (y > lo) fr = fb[(size_t)(r - 1) * T];
       if (l == 1) {
-        interior_step<R, EMAX, KEL>(dre, dim, es, pdre, pdim, pes, ere, eim, coh, A.ept, h);
+        interior_step<R, EMAX, KEL>(dre, dim, es, pdre, pdim, pes, ere, eim, coh, ept, h);
       } else {
         const bool entry = l == 3, exit = l == 2;
         const R din = entry ? (R)A.dist_in_gt[in_base + nin] : R(0);
         const R dout = exit ? (R)A.dist_out_gt[out_base + nout] : R(0);
-        site_step<R, EMAX, KEL>(l, 3, 2, dre, dim, es, pdre, pdim, pes, ere, eim, coh, A.ept, ecount, h,
+        site_step<R, EMAX, KEL>(l, 3, 2, dre, dim, es, pdre, pdim, pes, ere, eim, coh, ept, ecount, h,
                                 din, A.bin_gt + (size_t)(in_base + nin) * A.ne_stride + e0, dout,
                                 A.bout_gt + (size_t)(out_base + nout) * A.ne_stride + e0);
         if (A.pair && exit) {
@@ -414,7 +419,7 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
         nin += entry;
         nout += exit;
       }
-      if (!A.burn_in) {
+      if (!burn_in) {
         Cx<R> *sc = A.scratch + sb0 + (size_t)r * s_row;
 #pragma unroll
         for (int j = 0; j < EMAX; ++j)
@@ -439,7 +444,7 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
     const V4 *fb = (const V4 *)A.scratch2 + rec_index(A, lgc, item, 0);
     V4 fr = fb[0];
     Cx<R> gt_nx[EMAX];
-    if (!A.burn_in) {
+    if (!burn_in) {
       const Cx<R> *sc = A.scratch + sb0;
 #pragma unroll
       for (int j = 0; j < EMAX; ++j)
@@ -454,7 +459,7 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
       for (int j = 0; j < EMAX; ++j) gt[j] = gt_nx[j];
       if (y < hi) {
         fr = fb[(size_t)(r + 1) * T];
-        if (!A.burn_in) {
+        if (!burn_in) {
           const Cx<R> *sc = A.scratch + sb0 + (size_t)(r + 1) * s_row;
 #pragma unroll
           for (int j = 0; j < EMAX; ++j)
@@ -462,12 +467,12 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
         }
       }
       if (l == 1) {
-        interior_step<R, EMAX, KEL>(dre, dim, es, pdre, pdim, pes, ere, eim, coh, A.ept, h);
+        interior_step<R, EMAX, KEL>(dre, dim, es, pdre, pdim, pes, ere, eim, coh, ept, h);
       } else {
         const bool entry = l == 2, exit = l == 3;
         const R din = entry ? (R)A.dist_in_g[in_base + nin] : R(0);
         const R dout = exit ? (R)A.dist_out_g[out_base + nout] : R(0);
-        site_step<R, EMAX, KEL>(l, 2, 3, dre, dim, es, pdre, pdim, pes, ere, eim, coh, A.ept, ecount, h,
+        site_step<R, EMAX, KEL>(l, 2, 3, dre, dim, es, pdre, pdim, pes, ere, eim, coh, ept, ecount, h,
                                 din, A.bin_g + (size_t)(in_base + nin) * A.ne_stride + e0, dout,
                                 A.bout_g + (size_t)(out_base + nout) * A.ne_stride + e0);
         if (A.pair && exit) {
@@ -484,7 +489,7 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
       pdre = dre;
       pdim = dim;
       pes = es;
-      if (A.burn_in) continue;
+      if (burn_in) continue;
       if constexpr (KEL) {
         if (l != 0) {
           double *o = A.ldf + ((size_t)(a - A.slot_base) * nn1 + (size_t)y * n1 + x) * A.ne_stride + e0;
@@ -516,7 +521,7 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
       const int lg = lgc;
       group_sum4_scatter(v, g, lg, gmask);
       if (lg == 0) {
-        if (A.accumulate) {
+        if (accumulate) {
           const double2 of = as_d2(fg[fi]), og = as_d2(gi[fi]);
           v[0] += of.x;
           v[1] += of.y;
@@ -527,7 +532,7 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
         gi[fi] = frame_pair<Fr>(v[2], v[3]);
       } else if (lg == 1) {
         Fr *dst = (g ? gi : fg) + fi;
-        if (A.accumulate) {
+        if (accumulate) {
           const double2 o = as_d2(*dst);
           v[0] += o.x;
           v[1] += o.y;
@@ -538,7 +543,7 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
         if ((g & ((1 << sh) - 1)) == 0) {
           const int k = g >> sh;  // value index 0..3
           auto *dst = &((k < 2 ? fg : gi) + fi)->x;
-          if (A.accumulate) v[0] += (double)dst[k & 1];
+          if (accumulate) v[0] += (double)dst[k & 1];
           dst[k & 1] = (decltype(Fr::x))v[0];
         }
       }
@@ -1714,18 +1719,19 @@ void launch_frame_fields(sc_ctx *c, const Chunk &ch, const SweepArgs<R> &A) {
 
 template <typename R>
 void launch_sweep_pass(sc_ctx *c, const SweepArgs<R> &A, unsigned blocks) {
-  // Resident blocks per SM, fastest measured on B200 with the tiled scratch
-  // (606 x 606 d-wave square, 256 angles, 14 energies): FP64 three (four
-  // energies per thread, 158 registers: 24.6 ms against 28.6 with four blocks
-  // and 29.9 with two), mixed five (two energies per thread: 8.70 ms against
-  // 8.79 with six and 8.93 with four).
+  // Resident blocks per SM, fastest measured on B200 (606 x 606 d-wave square,
+  // 256 angles, 14 energies, fixed-group kernels): FP64 three (four energies
+  // per thread, 168 registers: 21.8 ms against 22.1 with four blocks and 24.4
+  // with two), mixed six (two energies per thread: 6.72 ms against 6.74 with
+  // four and 6.82 with five).
   // The common mappings (FP64: four energies per thread, four threads per
   // column; mixed and LDOS: eight threads per column) are compiled with the
   // group size fixed, which turns the per-site group reduction, frame store
   // and tile addressing into straight-line code (C2: FP64 sweep -5%, mixed
   // -12%); other mappings take it at run time.
   static const char *minb_env = std::getenv("SCB_SWEEP_MINB");
-  const int variant = minb_env ? std::atoi(minb_env) : (sizeof(R) == 8 ? 3 : (c->emax2 ? 5 : 1));
+  const int variant = minb_env ? std::atoi(minb_env) : (sizeof(R) == 8 ? 3 : (c->emax2 ? 6 : 1));
+  const bool plain = !A.burn_in && !A.accumulate;  // what the fixed-group kernels assume
   if (c->S.fs_tight_binding) {
     // Non-circular Fermi surface: per-angle step, generic mappings.
     if (c->S.keldysh) {
@@ -1738,20 +1744,25 @@ void launch_sweep_pass(sc_ctx *c, const SweepArgs<R> &A, unsigned blocks) {
       else k_sweep<R, 16, 1, false, true><<<blocks, 128, 0, c->stream>>>(A);
     }
   } else if (c->S.keldysh) {
-    if (c->ept <= 4 && c->log_groups == 3) k_sweep<R, 4, 1, true, false, 3><<<blocks, 128, 0, c->stream>>>(A);
+    if (plain && c->ept == 4 && c->log_groups == 3) k_sweep<R, 4, 1, true, false, 3><<<blocks, 128, 0, c->stream>>>(A);
     else if (c->ept <= 4) k_sweep<R, 4, 1, true><<<blocks, 128, 0, c->stream>>>(A);
     else if (c->ept <= 8) k_sweep<R, 8, 1, true><<<blocks, 128, 0, c->stream>>>(A);
     else k_sweep<R, 16, 1, true><<<blocks, 128, 0, c->stream>>>(A);
   } else if (c->ept <= 2 && c->emax2) {
-    if (variant >= 6) k_sweep<R, 2, 6, false><<<blocks, 128, 0, c->stream>>>(A);
-    else if (variant == 5 && c->log_groups == 3) k_sweep<R, 2, 5, false, false, 3><<<blocks, 128, 0, c->stream>>>(A);
+    const bool g8 = plain && c->log_groups == 3 && c->ept == 2;
+    if (variant >= 6 && g8) k_sweep<R, 2, 6, false, false, 3><<<blocks, 128, 0, c->stream>>>(A);
+    else if (variant >= 6) k_sweep<R, 2, 6, false><<<blocks, 128, 0, c->stream>>>(A);
+    else if (variant == 4 && g8) k_sweep<R, 2, 4, false, false, 3><<<blocks, 128, 0, c->stream>>>(A);
+    else if (variant == 5 && g8) k_sweep<R, 2, 5, false, false, 3><<<blocks, 128, 0, c->stream>>>(A);
     else if (variant == 5) k_sweep<R, 2, 5, false><<<blocks, 128, 0, c->stream>>>(A);
     else if (variant == 3) k_sweep<R, 2, 3, false><<<blocks, 128, 0, c->stream>>>(A);
     else k_sweep<R, 2, 4, false><<<blocks, 128, 0, c->stream>>>(A);
   } else if (c->ept <= 4) {
-    if (variant == 4) k_sweep<R, 4, 4, false><<<blocks, 128, 0, c->stream>>>(A);
+    if (variant == 4 && plain && c->log_groups == 2 && c->ept == 4) k_sweep<R, 4, 4, false, false, 2><<<blocks, 128, 0, c->stream>>>(A);
+    else if (variant == 4) k_sweep<R, 4, 4, false><<<blocks, 128, 0, c->stream>>>(A);
     else if (variant == 5) k_sweep<R, 4, 5, false><<<blocks, 128, 0, c->stream>>>(A);
-    else if (variant == 3 && c->log_groups == 2) k_sweep<R, 4, 3, false, false, 2><<<blocks, 128, 0, c->stream>>>(A);
+    else if (variant == 3 && plain && c->log_groups == 2 && c->ept == 4) k_sweep<R, 4, 3, false, false, 2><<<blocks, 128, 0, c->stream>>>(A);
+    else if (variant == 2 && plain && c->log_groups == 2 && c->ept == 4) k_sweep<R, 4, 2, false, false, 2><<<blocks, 128, 0, c->stream>>>(A);
     else if (variant == 3) k_sweep<R, 4, 3, false><<<blocks, 128, 0, c->stream>>>(A);
     else k_sweep<R, 4, 1, false><<<blocks, 128, 0, c->stream>>>(A);
   } else if (c->ept <= 8) {
