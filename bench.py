@@ -602,33 +602,43 @@ def batched_c3(n_grains: int, iters: int, subset: int, cap: int, max_s: float, f
     return res
 
 
-def ldos_c5(iters: int):
+def ldos_c5(iters: int, ppxi: float = 16.0, modes=("mixed", "fp64")):
     """LDOS postprocess throughput on the C5 grain: one block of 32 real
     energies in [-2 Delta0, 2 Delta0], broadening 0.02 Delta0, on the seeded
-    nine-vortex state (device-timed LDOS iterations after one burn-in)."""
+    nine-vortex state (LDOS iterations after one burn-in and one iteration),
+    with the device time of the sweep and of the rotation back per iteration.
+    ppxi < 16 runs the same grain at a coarser lattice (a small case for
+    profiling)."""
     import torch
     import superconga_b200 as sb
     from superconga_b200 import workloads
     cfg = workloads.c5()
+    cfg["numerics"]["points_per_coherence_length"] = ppxi
     d0 = workloads.S_WAVE_BULK
     pp = {"spectroscopy": {"energy_min": -2 * d0, "energy_max": 2 * d0, "num_energies": 512,
                            "energy_broadening": 0.02 * d0},
           "numerics": {"convergence_criterion": 1e-6, "norm": "l2", "num_energies_per_block": 32,
                        "num_fermi_momenta": 128}}
-    out = {"workload": "c5 LDOS: s square 100 xi0 @16/xi0 (N0=1606), 128 angles, 32 energies per block"}
-    for mode in ("mixed", "fp64"):
+    out = {"workload": f"c5 LDOS: s square 100 xi0 @{ppxi:g}/xi0, 128 angles, 32 energies per block"}
+    for mode in modes:
         e = sb.LdosContext(cfg, pp, mode=mode)
         d, a = workloads.initial_state("c5", cfg, e.dims.n0)
         e.set_state(d, a)
         e.begin_block(0)
         e.burn_in(1)
+        e.iterate(1)
         su = e.site_updates()
         torch.cuda.synchronize()
+        e.profile(True)
         t0 = time.perf_counter()
         e.iterate(iters)
         torch.cuda.synchronize()
         sec = (time.perf_counter() - t0) / iters
-        out[mode] = {"site_updates_per_s": su / sec, "s_per_iteration": sec, "site_updates_per_iteration": su}
+        split = {k: e.profile_read(i)[0] / iters for i, k in enumerate(("sweep", "rotate_back"))}
+        e.profile(False)
+        out[mode] = {"n0": e.dims.n0, "n1": e.dims.n1, "angle_chunks": e.sweep_plan()[0],
+                     "site_updates_per_s": su / sec, "s_per_iteration": sec,
+                     "site_updates_per_iteration": su, "kernel_ms_per_iteration": split}
         e.close()
     return out
 
@@ -712,6 +722,10 @@ def run_engine(args):
     from superconga_b200 import workloads
     from superconga_b200.engine import fma_peak
 
+    if args.ldos_only:
+        if rank == 0:
+            print(json.dumps({"ldos": ldos_c5(2, args.ldos_ppxi, args.modes.split(","))}), flush=True)
+        return
     cfg = workloads.WORKLOADS[args.workload]()
     hbm, hbm_kind = _peaks()
     results = {}
@@ -785,7 +799,7 @@ def run_engine(args):
         extra["batched"] = batched_c3(args.batch_grains, args.batch_iters, args.batch_subset, args.batch_cap,
                                       args.batch_max_s, args.c3_full)
     if rank == 0 and world == 1 and args.ldos:
-        extra["ldos"] = ldos_c5(2)
+        extra["ldos"] = ldos_c5(2, args.ldos_ppxi)
     if rank == 0 and world == 1 and not args.no_c5:
         extra["c5"] = c5_solve_and_ldos(args.c5_max_it, args.c5_max_s, args.c5_blocks, args.c5_ldos_max_it)
     if rank == 0 and world == 1 and not args.no_adjoint:
@@ -857,6 +871,9 @@ def main():
     ap.add_argument("--batch-grains", type=int, default=128)
     ap.add_argument("--batch-iters", type=int, default=5)
     ap.add_argument("--ldos", action="store_true", help="also time the C5 LDOS postprocess")
+    ap.add_argument("--ldos-only", action="store_true",
+                    help="only the C5 LDOS iteration timing (modes from --modes), one JSON line")
+    ap.add_argument("--ldos-ppxi", type=float, default=16.0, help="lattice points per xi0 of that run")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--batch-max-s", type=float, default=300.0)
     ap.add_argument("--batch-subset", type=int, default=16)

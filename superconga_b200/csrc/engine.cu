@@ -712,37 +712,60 @@ __global__ void k_halo_ldos(int n_entries, int entry0, int n1, int ne,
 // LDOS frames rotated back onto the reference grid and accumulated in angle
 // order, Im part weighted by the integrand factor (ComputeLDOS.h:140-144,
 // insertRotatedGridAdditive with Type::imag, GridFunctions_GPU.h:991-1054).
-// A thread takes one reference site and LDOS_E consecutive energies: one
-// lookup per angle serves all of them, and the corners' energies are
-// contiguous in the [slot][site][energy] frame.
-constexpr int LDOS_E = 8;
+// The frame is energy-innermost ([slot][site][energy]): EL consecutive lanes
+// take EL consecutive energies of one reference site, so that a warp's corner
+// load reads whole runs of 32 / EL frame sites (two 128-byte lines for 32
+// energies) instead of 32 scattered sites.  A block takes a TX x (256 / EL /
+// TX) tile of reference sites; the bilinear lookups of its sites are computed
+// once per angle into shared memory, RB_ANGLES angles at a time, and read
+// back as broadcasts.  A site whose lookup falls outside the frame adds exact
+// zeros (weight 0, corners read at the frame origin, which holds zeros): the
+// same sums as skipping it, with a loop free of branches so that the loads of
+// consecutive angles overlap.
+constexpr int RB_ANGLES = 32;
+template <int EL, int TX>
 __global__ void __launch_bounds__(256) k_rotate_back_ldos(int n0, int n1, int ne, int a_begin, int a_end,
                                                           const AngleParams *__restrict__ ang,
                                                           const double *__restrict__ ldf, double *acc) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int e0 = blockIdx.z * LDOS_E;
-  if (x >= n0 || y >= n0) return;
+  constexpr int SPB = 256 / EL, TY = SPB / TX;
+  static_assert(SPB % TX == 0, "the site tile must fill the block");
+  __shared__ int s_i00[RB_ANGLES][SPB];
+  __shared__ double2 s_fxy[RB_ANGLES][SPB];
+  __shared__ double s_w[RB_ANGLES][SPB];
+  const int t = threadIdx.x;
+  const int s = t / EL;
+  const int x = blockIdx.x * TX + s % TX, y = blockIdx.y * TY + s / TX;
+  const int e = blockIdx.z * EL + t % EL;
+  const bool valid = x < n0 && y < n0 && e < ne;
   const size_t nn0 = (size_t)n0 * n0, nn1 = (size_t)n1 * n1;
   const size_t i = (size_t)y * n0 + x;
-  const int ecount = min(LDOS_E, ne - e0);
-  double v[LDOS_E];
-#pragma unroll
-  for (int j = 0; j < LDOS_E; ++j) v[j] = (j < ecount) ? acc[(size_t)(e0 + j) * nn0 + i] : 0.0;
-  for (int a = a_begin; a < a_end; ++a) {
-    const AngleParams &P = ang[a];
-    Bilinear b;
-    if (!rotated_lookup(x, y, n0, n1, P.cB, P.sB, b)) continue;
-    const double *f = ldf + ((size_t)(a - a_begin) * nn1 + b.i00) * ne + e0;
-    const size_t dx = (size_t)ne, dy = (size_t)n1 * ne;
-#pragma unroll
-    for (int j = 0; j < LDOS_E; ++j)
-      if (j < ecount)
-        v[j] += bilerp(f[j] * P.w, f[dx + j] * P.w, f[dy + j] * P.w, f[dy + dx + j] * P.w, b.xf, b.yf);
+  const size_t dx = (size_t)ne, dy = (size_t)n1 * ne;
+  double v = valid ? acc[(size_t)e * nn0 + i] : 0.0;
+  for (int ab = a_begin; ab < a_end; ab += RB_ANGLES) {
+    const int na = min(RB_ANGLES, a_end - ab);
+    __syncthreads();  // every thread has read the previous angles' lookups
+    for (int k = t; k < na * SPB; k += 256) {
+      const int ka = k / SPB, ks = k % SPB;
+      const int kx = blockIdx.x * TX + ks % TX, ky = blockIdx.y * TY + ks / TX;
+      const AngleParams &P = ang[ab + ka];
+      Bilinear b;
+      const bool in = kx < n0 && ky < n0 && rotated_lookup(kx, ky, n0, n1, P.cB, P.sB, b);
+      s_i00[ka][ks] = in ? b.i00 : 0;
+      s_fxy[ka][ks] = in ? make_double2(b.xf, b.yf) : make_double2(0.0, 0.0);
+      s_w[ka][ks] = in ? P.w : 0.0;
+    }
+    __syncthreads();
+    if (!valid) continue;
+    const double *f = ldf + (size_t)(ab - a_begin) * nn1 * ne + e;
+#pragma unroll 4
+    for (int ka = 0; ka < na; ++ka) {
+      const double2 fxy = s_fxy[ka][s];
+      const double w = s_w[ka][s];
+      const double *c = f + (size_t)ka * nn1 * ne + (size_t)s_i00[ka][s] * ne;
+      v += bilerp(c[0] * w, c[dx] * w, c[dy] * w, c[dy + dx] * w, fxy.x, fxy.y);
+    }
   }
-#pragma unroll
-  for (int j = 0; j < LDOS_E; ++j)
-    if (j < ecount) acc[(size_t)(e0 + j) * nn0 + i] = v[j];
+  if (valid) acc[(size_t)e * nn0 + i] = v;
 }
 
 // ComputeLDOS::computePropertyFromGreens (ComputeLDOS.h:146-193): LDOS = -sum,
@@ -2040,6 +2063,25 @@ void frame_to_reference(sc_ctx *c, const Chunk &ch) {
   check_launch(c);
 }
 
+// Lanes per reference site: the smallest of 8, 16, 32 that holds the block's
+// energies (more energies take several blocks along z).
+static void launch_rotate_back_ldos(sc_ctx *c, const Chunk &ch) {
+  const HostSetup &S = c->S;
+  auto go = [&](auto kern, int el, int tx) {
+    const int ty = 256 / el / tx;
+    dim3 grid((S.n0 + tx - 1) / tx, (S.n0 + ty - 1) / ty, (S.ne + el - 1) / el);
+    kern<<<grid, 256, 0, c->stream>>>(S.n0, S.n1, S.ne, ch.a_begin, ch.a_end, c->ang.p, c->ldf.p,
+                                      c->ldos_acc.p);
+  };
+  if (S.ne <= 8)
+    go(k_rotate_back_ldos<8, 8>, 8, 8);
+  else if (S.ne <= 16)
+    go(k_rotate_back_ldos<16, 4>, 16, 4);
+  else
+    go(k_rotate_back_ldos<32, 4>, 32, 4);
+  check_launch(c);
+}
+
 template <typename R>
 void run_chunks_ldos(sc_ctx *c, int burn_in) {
   const HostSetup &S = c->S;
@@ -2061,11 +2103,8 @@ void run_chunks_ldos(sc_ctx *c, int burn_in) {
           c->ldf.p);
       check_launch(c);
     }
-    dim3 blk(32, 8), grid((S.n0 + 31) / 32, (S.n0 + 7) / 8, (S.ne + LDOS_E - 1) / LDOS_E);
     ProfScope prof(c, 1);
-    k_rotate_back_ldos<<<grid, blk, 0, c->stream>>>(S.n0, S.n1, S.ne, ch.a_begin, ch.a_end, c->ang.p,
-                                                    c->ldf.p, c->ldos_acc.p);
-    check_launch(c);
+    launch_rotate_back_ldos(c, ch);
   }
 }
 
