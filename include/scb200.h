@@ -297,7 +297,8 @@ int sc_measure_fma_peak(int precision, double *flops_per_second);
 
 /* Per-kernel CUDA-event timing on the context's stream.  kernel: 0 Riccati
  * sweep, 1 rotation back to the reference grid, 2 Poisson filters, 3 boundary
- * condition.  sc_profile_read returns the summed device time and number of
+ * condition, 4 frame fields (the rotated order parameter, Doppler shift and
+ * labels of each chunk's trajectory sites).  sc_profile_read returns the summed device time and number of
  * timed launches since the last read, and resets them. */
 int sc_profile(sc_ctx *ctx, int enable);
 int sc_profile_read(sc_ctx *ctx, int kernel, double *total_ms, long long *launches);

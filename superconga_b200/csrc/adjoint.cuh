@@ -751,7 +751,8 @@ void adjoint_run(sc_ctx *c, AdjBuffers &B, double w_omega, const double *beta_ho
     SweepArgs<double> A = sweep_args<double>(c, &ch, 0);
     if (!A.n_items) continue;
     launch_frame_fields<double>(c, ch, A);
-    double2 *seed = (double2 *)c->w_fg, *grad_d = (double2 *)c->w_gi;
+    // The frame-record buffer (two double2 per site and slot) holds both.
+    double2 *seed = (double2 *)c->w_fr, *grad_d = seed + (size_t)nslots * nn1;
     c->frames_zeroed = false;  // the frame buffers serve as seed and gradient buffers
     CUDA_TRY(cudaMemsetAsync(seed, 0, (size_t)nslots * nn1 * sizeof(double2), c->stream));
     CUDA_TRY(cudaMemsetAsync(grad_d, 0, (size_t)nslots * nn1 * sizeof(double2), c->stream));

@@ -112,6 +112,30 @@ __device__ __forceinline__ F2 frame_pair(double a, double b) {
 __device__ __forceinline__ double2 as_d2(double2 v) { return v; }
 __device__ __forceinline__ double2 as_d2(float2 v) { return make_double2(v.x, v.y); }
 
+// Two consecutive double2 in one 256-bit load through the read-only path
+// (ld.global.nc.v4.f64, sm_100); p must be 32-byte aligned.
+__device__ __forceinline__ void ldg_d2x2(const double2 *p, double2 &a, double2 &b) {
+  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+      : "=d"(a.x), "=d"(a.y), "=d"(b.x), "=d"(b.y)
+      : "l"(p));
+}
+
+// A frame site's record is two frame elements, (Re F, Im F) then (Re g, Re I):
+// 16 bytes in FP32, 32 in FP64, read with one load (the buffers are 256-byte
+// aligned and the records packed).
+struct FrameRec {
+  double2 f, q;
+};
+__device__ __forceinline__ FrameRec load_rec(const float2 *fr, size_t i) {
+  const float4 v = __ldg((const float4 *)fr + i);
+  return FrameRec{make_double2(v.x, v.y), make_double2(v.z, v.w)};
+}
+__device__ __forceinline__ FrameRec load_rec(const double2 *fr, size_t i) {
+  FrameRec r;
+  ldg_d2x2(fr + 2 * i, r.f, r.q);
+  return r;
+}
+
 template <typename R>
 struct SweepArgs {
   int n0, n1, ne, nc, groups, log_groups, ept, n_items;
@@ -133,7 +157,7 @@ struct SweepArgs {
   const double *e_re, *e_im, *res;
   Cx<R> *scratch;   // [tile][row][energy][item of tile]
   R *scratch2;      // frame-field records [tile][row][item of tile] of (Re D, Im D, energy shift, label), in R
-  typename FrameOf<R>::type *fg, *gi;  // frame buffers [slot][n1*n1]: (Re F, Im F), (Re G, Re I)
+  typename FrameOf<R>::type *fr;  // frame records [slot][n1*n1][2]: (Re F, Im F), (Re g, Re I)
   double *ldf;      // LDOS frame buffer [slot][n1*n1][energy]: Im g per real energy
 };
 
@@ -188,15 +212,32 @@ __device__ __forceinline__ void frame_fields(const SweepArgs<R> &A, const AngleP
   dre = 0.0;
   dim = 0.0;
   const int st = A.nc + 1;
-  if (rotated_lookup(x, y, A.n1, n0, P.cD, P.sD, b)) {
+  // One component: a site's record (Delta, A) is 32 bytes, read with one
+  // 256-bit load per corner, which also brings the corner's A when the
+  // vector-potential lookup lands on the same corners (it differs only by the
+  // rounding of its own rotation coefficients).
+  const bool one = A.nc == 1;
+  double2 ca[4];
+  const bool inD = rotated_lookup(x, y, A.n1, n0, P.cD, P.sD, b);
+  if (inD) {
     double c_re[4] = {0, 0, 0, 0}, c_im[4] = {0, 0, 0, 0};
     const int off[4] = {b.i00, b.i00 + 1, b.i00 + n0, b.i00 + n0 + 1};
-    for (int c = 0; c < A.nc; ++c) {
-      const double et = P.eta[c];
+    if (one) {
+      const double et = P.eta[0];
       for (int k = 0; k < 4; ++k) {
-        const double2 v = __ldg(A.rf + (size_t)off[k] * st + c);
+        double2 v;
+        ldg_d2x2(A.rf + (size_t)off[k] * 2, v, ca[k]);
         c_re[k] += v.x * et;
         c_im[k] += v.y * et;
+      }
+    } else {
+      for (int c = 0; c < A.nc; ++c) {
+        const double et = P.eta[c];
+        for (int k = 0; k < 4; ++k) {
+          const double2 v = __ldg(A.rf + (size_t)off[k] * st + c);
+          c_re[k] += v.x * et;
+          c_im[k] += v.y * et;
+        }
       }
     }
     dre = bilerp(c_re[0], c_re[1], c_re[2], c_re[3], b.xf, b.yf);
@@ -213,9 +254,19 @@ __device__ __forceinline__ void frame_fields(const SweepArgs<R> &A, const AngleP
       double rx = 0.0, ry = 0.0;
       Bilinear ba;
       if (rotated_lookup(x, y, A.n1, n0, P.cA, P.sA, ba)) {
-        const double2 *pa = A.rf + A.nc;
-        const double2 v00 = __ldg(pa + (size_t)ba.i00 * st), v01 = __ldg(pa + (size_t)(ba.i00 + 1) * st);
-        const double2 v10 = __ldg(pa + (size_t)(ba.i00 + n0) * st), v11 = __ldg(pa + (size_t)(ba.i00 + n0 + 1) * st);
+        double2 v00, v01, v10, v11;
+        if (one && inD && ba.i00 == b.i00) {
+          v00 = ca[0];
+          v01 = ca[1];
+          v10 = ca[2];
+          v11 = ca[3];
+        } else {
+          const double2 *pa = A.rf + A.nc;
+          v00 = __ldg(pa + (size_t)ba.i00 * st);
+          v01 = __ldg(pa + (size_t)(ba.i00 + 1) * st);
+          v10 = __ldg(pa + (size_t)(ba.i00 + n0) * st);
+          v11 = __ldg(pa + (size_t)(ba.i00 + n0 + 1) * st);
+        }
         rx = bilerp(v00.x, v01.x, v10.x, v11.x, ba.xf, ba.yf);
         ry = bilerp(v00.y, v01.y, v10.y, v11.y, ba.xf, ba.yf);
       }
@@ -438,8 +489,9 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
 #pragma unroll
     for (int j = 0; j < EMAX; ++j) coh[j] = Cx<R>{R(0), R(0)};
     using Fr = typename FrameOf<R>::type;
-    Fr *fg = A.fg + (size_t)(a - A.slot_base) * nn1;
-    Fr *gi = A.gi + (size_t)(a - A.slot_base) * nn1;
+    Fr *frs = A.fr + (size_t)(a - A.slot_base) * nn1 * 2;  // this angle's records
+    // The value this thread stores when four or more threads share a column.
+    auto *vdst = &frs->x + (lgc >= 2 ? (g >> (lgc - 2)) : 0);
     typedef typename Rec4<R>::type V4;
     const V4 *fb = (const V4 *)A.scratch2 + rec_index(A, lgc, item, 0);
     V4 fr = fb[0];
@@ -520,18 +572,19 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
       double v[4] = {sfr, sfi, sg, -si};
       const int lg = lgc;
       group_sum4_scatter(v, g, lg, gmask);
+      Fr *rec = frs + 2 * fi;
       if (lg == 0) {
         if (accumulate) {
-          const double2 of = as_d2(fg[fi]), og = as_d2(gi[fi]);
+          const double2 of = as_d2(rec[0]), og = as_d2(rec[1]);
           v[0] += of.x;
           v[1] += of.y;
           v[2] += og.x;
           v[3] += og.y;
         }
-        fg[fi] = frame_pair<Fr>(v[0], v[1]);
-        gi[fi] = frame_pair<Fr>(v[2], v[3]);
+        rec[0] = frame_pair<Fr>(v[0], v[1]);
+        rec[1] = frame_pair<Fr>(v[2], v[3]);
       } else if (lg == 1) {
-        Fr *dst = (g ? gi : fg) + fi;
+        Fr *dst = rec + g;
         if (accumulate) {
           const double2 o = as_d2(*dst);
           v[0] += o.x;
@@ -541,10 +594,9 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
       } else {
         const int sh = lg - 2;  // low bits below the two value bits
         if ((g & ((1 << sh) - 1)) == 0) {
-          const int k = g >> sh;  // value index 0..3
-          auto *dst = &((k < 2 ? fg : gi) + fi)->x;
-          if (accumulate) v[0] += (double)dst[k & 1];
-          dst[k & 1] = (decltype(Fr::x))v[0];
+          auto *dst = vdst + 4 * fi;
+          if (accumulate) v[0] += (double)*dst;
+          *dst = (decltype(Fr::x))v[0];
         }
       }
     }
@@ -599,23 +651,23 @@ __global__ void __launch_bounds__(128, MINB) k_sweep_batch(const SweepArgs<R> *_
 template <typename F2>
 __global__ void k_halo(int n_entries, int entry0, int n1, const int *__restrict__ entry_angle,
                        int slot_base, const int *__restrict__ site, const int *__restrict__ off,
-                       const int *__restrict__ src, F2 *fg, F2 *gi) {
+                       const int *__restrict__ src, F2 *fr) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n_entries) return;
   const int e = entry0 + k;
-  const size_t base = (size_t)(entry_angle[e] - slot_base) * n1 * n1;
+  F2 *slot = fr + (size_t)(entry_angle[e] - slot_base) * n1 * n1 * 2;  // records of two F2
   const int b = off[e], en = off[e + 1];
-  double2 f = as_d2(fg[base + src[b]]), q = as_d2(gi[base + src[b]]);
+  double2 f = as_d2(slot[2 * (size_t)src[b]]), q = as_d2(slot[2 * (size_t)src[b] + 1]);
   for (int i = b + 1; i < en; ++i) {
-    const double2 f2 = as_d2(fg[base + src[i]]), q2 = as_d2(gi[base + src[i]]);
+    const double2 f2 = as_d2(slot[2 * (size_t)src[i]]), q2 = as_d2(slot[2 * (size_t)src[i] + 1]);
     f.x = __dadd_rn(f.x, f2.x);
     f.y = __dadd_rn(f.y, f2.y);
     q.x = __dadd_rn(q.x, q2.x);
     q.y = __dadd_rn(q.y, q2.y);
   }
   const double cnt = (double)(en - b);
-  fg[base + site[e]] = frame_pair<F2>(__ddiv_rn(f.x, cnt), __ddiv_rn(f.y, cnt));
-  gi[base + site[e]] = frame_pair<F2>(__ddiv_rn(q.x, cnt), __ddiv_rn(q.y, cnt));
+  slot[2 * (size_t)site[e]] = frame_pair<F2>(__ddiv_rn(f.x, cnt), __ddiv_rn(f.y, cnt));
+  slot[2 * (size_t)site[e] + 1] = frame_pair<F2>(__ddiv_rn(q.x, cnt), __ddiv_rn(q.y, cnt));
 }
 
 // Rotation of the frame Green sums back to the reference grid, accumulated in
@@ -626,18 +678,22 @@ __global__ void k_halo(int n_entries, int entry0, int n1, const int *__restrict_
 // frame of a at the mirrored site (n1-1-x, n1-1-y) with gamma' = conj(gammaTilde),
 // gammaTilde' = conj(gamma): F' = F, Re g' = -Re g, Re I' = Re I.  The angles
 // are then accumulated in the order a, a + pair, a + 1, ...
-template <typename F2>
-__global__ void __launch_bounds__(256) k_rotate_back(int n0, int n1, int nc, int a_begin,
+// NC > 0 fixes the component count at compile time (the sums stay in
+// registers); NC = 0 takes it from nc.  One component: four resident blocks
+// per SM (64 registers) measured fastest on B200; more: three.
+template <typename F2, int NC>
+__global__ void __launch_bounds__(256, NC == 1 ? 4 : 3) k_rotate_back(int n0, int n1, int nc_, int a_begin,
                                                      int a_end, int pair, const AngleParams *__restrict__ ang,
-                                                     const F2 *__restrict__ fg,
-                                                     const F2 *__restrict__ gi,
+                                                     const F2 *__restrict__ fr,
                                                      double *acc_d, double *acc_j, double *acc_fe) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= n0 || y >= n0) return;
   const size_t nn0 = (size_t)n0 * n0, nn1 = (size_t)n1 * n1;
   const size_t i = (size_t)y * n0 + x;
-  double dr[MAX_COMP], di[MAX_COMP];
+  const int nc = NC > 0 ? NC : nc_;
+  double dr[NC > 0 ? NC : MAX_COMP], di[NC > 0 ? NC : MAX_COMP];
+#pragma unroll
   for (int c = 0; c < nc; ++c) {
     dr[c] = acc_d[(size_t)(2 * c) * nn0 + i];
     di[c] = acc_d[(size_t)(2 * c + 1) * nn0 + i];
@@ -657,21 +713,22 @@ __global__ void __launch_bounds__(256) k_rotate_back(int n0, int n1, int nc, int
     const bool inside = rotated_lookup(x, y, n0, n1, P.cB, P.sB, b);
     if (!inside) b = Bilinear{0, 0.0, 0.0};
     const double pw = inside ? P.w : 0.0, psx = inside ? P.sx : 0.0, psy = inside ? P.sy : 0.0;
-    double2 f00, f01, f10, f11, q00, q01, q10, q11;
+    FrameRec r00, r01, r10, r11;
     const size_t slot = (size_t)(a0 - a_begin) * nn1;
     if (!mirrored) {
       const size_t base = slot + b.i00;
-      f00 = as_d2(fg[base]); f01 = as_d2(fg[base + 1]); f10 = as_d2(fg[base + n1]); f11 = as_d2(fg[base + n1 + 1]);
-      q00 = as_d2(gi[base]); q01 = as_d2(gi[base + 1]); q10 = as_d2(gi[base + n1]); q11 = as_d2(gi[base + n1 + 1]);
+      r00 = load_rec(fr, base); r01 = load_rec(fr, base + 1); r10 = load_rec(fr, base + n1); r11 = load_rec(fr, base + n1 + 1);
     } else {
       // corner (xi + dx, yi + dy) of angle a is site nn1 - 1 - i00 - dx - n1 dy of angle a0
       const size_t m = slot + (nn1 - 1 - (size_t)b.i00);
-      f00 = as_d2(fg[m]); f01 = as_d2(fg[m - 1]); f10 = as_d2(fg[m - n1]); f11 = as_d2(fg[m - n1 - 1]);
-      q00 = as_d2(gi[m]); q01 = as_d2(gi[m - 1]); q10 = as_d2(gi[m - n1]); q11 = as_d2(gi[m - n1 - 1]);
-      q00.x = -q00.x; q01.x = -q01.x; q10.x = -q10.x; q11.x = -q11.x;
+      r00 = load_rec(fr, m); r01 = load_rec(fr, m - 1); r10 = load_rec(fr, m - n1); r11 = load_rec(fr, m - n1 - 1);
+      r00.q.x = -r00.q.x; r01.q.x = -r01.q.x; r10.q.x = -r10.q.x; r11.q.x = -r11.q.x;
     }
+    const double2 f00 = r00.f, f01 = r01.f, f10 = r10.f, f11 = r11.f;
+    const double2 q00 = r00.q, q01 = r01.q, q10 = r10.q, q11 = r11.q;
     const double fre = bilerp(f00.x, f01.x, f10.x, f11.x, b.xf, b.yf);
     const double fim = bilerp(f00.y, f01.y, f10.y, f11.y, b.xf, b.yf);
+#pragma unroll
     for (int c = 0; c < nc; ++c) {
       const double et = P.eta[c];
       dr[c] += (fre * et) * pw;
@@ -681,6 +738,7 @@ __global__ void __launch_bounds__(256) k_rotate_back(int n0, int n1, int nc, int
     jy += bilerp(q00.x * psy, q01.x * psy, q10.x * psy, q11.x * psy, b.xf, b.yf);
     fe += bilerp(q00.y * pw, q01.y * pw, q10.y * pw, q11.y * pw, b.xf, b.yf);
   }
+#pragma unroll
   for (int c = 0; c < nc; ++c) {
     acc_d[(size_t)(2 * c) * nn0 + i] = dr[c];
     acc_d[(size_t)(2 * c + 1) * nn0 + i] = di[c];
@@ -1588,7 +1646,7 @@ struct sc_ctx {
   DevArray<double> acc_d, acc_j, acc_fe;
   DevArray<double> bnd;      // boundary storage (4 arrays), R-typed, viewed through pointers
   size_t bnd_off[4] = {0, 0, 0, 0};
-  DevArray<double> scratch, scratch2, fg, gi;
+  DevArray<double> scratch, scratch2, frames;
   DevArray<double> partial_fin, partial_bg, partial_bgt, partial_vp, partial_acc;
   DevArray<double> pois_s;
   // Poisson transform: side P = 32 * 2^a 3^b 5^c (radix plan), twiddles,
@@ -1610,7 +1668,7 @@ struct sc_ctx {
   // write; with one chunk every slot always holds the same angle, so they are
   // cleared once instead of before every sweep.
   bool frames_zeroed = false;
-  double *w_scratch = nullptr, *w_scratch2 = nullptr, *w_fg = nullptr, *w_gi = nullptr;
+  double *w_scratch = nullptr, *w_scratch2 = nullptr, *w_fr = nullptr;
   size_t need_scratch = 0, need_scratch2 = 0, need_frame = 0;  // bytes of each (frame: fg and gi each)
 
   std::unique_ptr<AdjBuffers, AdjDeleter> adj;  // allocated by the first sc_adjoint
@@ -1625,7 +1683,7 @@ struct sc_ctx {
   // Optional CUDA-event timing of individual kernels (0 sweep, 1 rotate back,
   // 2 Poisson, 3 boundary condition), recorded on the launching stream.
   bool profiling = false;
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof[4];
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof[5];
 
   // One steady-state iteration (accelerator step to scalars) captured as a
   // CUDA graph and replayed by sc_compute.  Every call that could change what
@@ -1643,7 +1701,7 @@ struct sc_ctx {
   size_t nn0() const { return (size_t)S.n0 * S.n0; }
   size_t esize() const { return mode == SC_MODE_FP64 ? sizeof(Cx<double>) : sizeof(Cx<float>); }
   // Bytes of one frame-buffer element (FrameOf<R>: float2 for the FP32 sweep).
-  size_t frame_elem() const { return (mode == SC_MODE_MIXED && !S.keldysh) ? sizeof(float2) : sizeof(double2); }
+  size_t frame_rec() const { return (mode == SC_MODE_MIXED && !S.keldysh) ? sizeof(float4) : 2 * sizeof(double2); }
   void *bnd_ptr(int which) const { return (char *)bnd.p + bnd_off[which]; }
   int n_bnd(int which) const {
     return which == 0 ? S.n_in_g : which == 1 ? S.n_out_g : which == 2 ? S.n_in_gt : S.n_out_gt;
@@ -1726,8 +1784,7 @@ SweepArgs<R> sweep_args(sc_ctx *c, const Chunk *ch, int burn_in) {
   A.ldf = c->ldf.p;
   A.scratch = (Cx<R> *)c->w_scratch;
   A.scratch2 = (R *)c->w_scratch2;
-  A.fg = (typename FrameOf<R>::type *)c->w_fg;
-  A.gi = (typename FrameOf<R>::type *)c->w_gi;
+  A.fr = (typename FrameOf<R>::type *)c->w_fr;
   return A;
 }
 
@@ -1736,6 +1793,7 @@ void launch_frame_fields(sc_ctx *c, const Chunk &ch, const SweepArgs<R> &A) {
   if (!A.n_items) return;
   const int rows = 4 * FF_ROWS;  // rows per block, four per thread
   dim3 grid(grid1(A.n_items, FF_COLS), (unsigned)((ch.kmax + rows - 1) / rows));
+  ProfScope prof(c, 4);
   k_frame_fields<R><<<grid, dim3(FF_COLS, FF_ROWS), 0, c->stream>>>(A, rows);
   check_launch(c);
 }
@@ -2050,16 +2108,16 @@ void frame_to_reference(sc_ctx *c, const Chunk &ch) {
   if (h1 > h0) {
     k_halo<<<grid1(h1 - h0, 128), 128, 0, c->stream>>>(h1 - h0, h0, S.n1, c->halo_angle.p, ch.a_begin,
                                                         c->halo_site.p, c->halo_off.p, c->halo_src.p,
-                                                        (Fr *)c->w_fg, (Fr *)c->w_gi);
+                                                        (Fr *)c->w_fr);
     check_launch(c);
   }
   // A warp covers an 8 x 4 patch of the reference grid (its rotated corners
   // share cache lines of the frame).
   dim3 blk(8, 32), grid((S.n0 + 7) / 8, (S.n0 + 31) / 32);
   ProfScope prof(c, 1);
-  k_rotate_back<<<grid, blk, 0, c->stream>>>(S.n0, S.n1, S.nc, ch.a_begin, a_stored, pair, c->ang.p,
-                                             (const Fr *)c->w_fg, (const Fr *)c->w_gi,
-                                             c->acc_d.p, c->acc_j.p, c->acc_fe.p);
+  auto kern = S.nc == 1 ? k_rotate_back<Fr, 1> : S.nc == 2 ? k_rotate_back<Fr, 2> : k_rotate_back<Fr, 0>;
+  kern<<<grid, blk, 0, c->stream>>>(S.n0, S.n1, S.nc, ch.a_begin, a_stored, pair, c->ang.p, (const Fr *)c->w_fr,
+                                    c->acc_d.p, c->acc_j.p, c->acc_fe.p);
   check_launch(c);
 }
 
@@ -2120,8 +2178,7 @@ void run_chunks(sc_ctx *c, int burn_in) {
   for (const Chunk &ch : c->chunks) {
     const int nslots = chunk_slots(c, ch);
     if (!burn_in && clear) {
-      CUDA_TRY(cudaMemsetAsync(c->w_fg, 0, (size_t)nslots * nn1 * c->frame_elem(), c->stream));
-      CUDA_TRY(cudaMemsetAsync(c->w_gi, 0, (size_t)nslots * nn1 * c->frame_elem(), c->stream));
+      CUDA_TRY(cudaMemsetAsync(c->w_fr, 0, (size_t)nslots * nn1 * c->frame_rec(), c->stream));
       c->frames_zeroed = c->chunks.size() == 1;
     }
     launch_sweep<R>(c, ch, burn_in);
@@ -2551,7 +2608,7 @@ void upload_static(sc_ctx *c) {
   }
   c->need_scratch = scr + 8;
   c->need_scratch2 = (scr2 + 1) * sizeof(double);
-  c->need_frame = (size_t)max_slots * n1 * n1 * c->frame_elem();
+  c->need_frame = (size_t)max_slots * n1 * n1 * c->frame_rec();
   if (c->batch_member) {
     // Work buffers come from the batch's pool.
   } else if (S.keldysh) {
@@ -2569,10 +2626,8 @@ void upload_static(sc_ctx *c) {
     c->scratch2.alloc(scr2 + 1);
     c->w_scratch = c->scratch.p;
     c->w_scratch2 = c->scratch2.p;
-    c->fg.alloc((size_t)max_slots * n1 * n1 * 2);
-    c->gi.alloc((size_t)max_slots * n1 * n1 * 2);
-    c->w_fg = c->fg.p;
-    c->w_gi = c->gi.p;
+    c->frames.alloc((size_t)max_slots * n1 * n1 * 4);  // FP64-sized records (the adjoint's buffers too)
+    c->w_fr = c->frames.p;
   }
   c->nb_fin = std::min<int>(592, (int)grid1(nn, REDUCE_THREADS));
   c->nb_bnd = std::min<int>(592, (int)grid1((size_t)std::max(S.n_in_g, S.n_in_gt) * S.ne, REDUCE_THREADS));
@@ -3057,8 +3112,7 @@ int sc_angle_greens(sc_ctx *ctx, int angle, double *f, double *g_re, double *i_r
   const size_t nn1 = (size_t)S.n1 * S.n1;
   extend_reference(ctx);
   ctx->frames_zeroed = false;  // slot 0 now holds this angle
-  CUDA_TRY(cudaMemsetAsync(ctx->w_fg, 0, nn1 * ctx->frame_elem(), ctx->stream));
-  CUDA_TRY(cudaMemsetAsync(ctx->w_gi, 0, nn1 * ctx->frame_elem(), ctx->stream));
+  CUDA_TRY(cudaMemsetAsync(ctx->w_fr, 0, nn1 * ctx->frame_rec(), ctx->stream));
   if (!cols.empty()) {
     // Place the columns at the front of the item array (restored below).
     std::vector<int4> saved(cols.size());
@@ -3071,18 +3125,21 @@ int sc_angle_greens(sc_ctx *ctx, int angle, double *f, double *g_re, double *i_r
     CUDA_TRY(cudaMemcpy(ctx->items.p, saved.data(), cols.size() * sizeof(int4), cudaMemcpyHostToDevice));
   }
   std::vector<double2> hf(nn1), hg(nn1);
-  if (ctx->frame_elem() == sizeof(double2)) {
-    CUDA_TRY(cudaMemcpyAsync(hf.data(), ctx->w_fg, nn1 * sizeof(double2), cudaMemcpyDeviceToHost, ctx->stream));
-    CUDA_TRY(cudaMemcpyAsync(hg.data(), ctx->w_gi, nn1 * sizeof(double2), cudaMemcpyDeviceToHost, ctx->stream));
-    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-  } else {
-    std::vector<float2> sf(nn1), sg(nn1);
-    CUDA_TRY(cudaMemcpyAsync(sf.data(), ctx->w_fg, nn1 * sizeof(float2), cudaMemcpyDeviceToHost, ctx->stream));
-    CUDA_TRY(cudaMemcpyAsync(sg.data(), ctx->w_gi, nn1 * sizeof(float2), cudaMemcpyDeviceToHost, ctx->stream));
+  if (ctx->frame_rec() == 2 * sizeof(double2)) {
+    std::vector<double2> rec(2 * nn1);
+    CUDA_TRY(cudaMemcpyAsync(rec.data(), ctx->w_fr, nn1 * ctx->frame_rec(), cudaMemcpyDeviceToHost, ctx->stream));
     CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     for (size_t i = 0; i < nn1; ++i) {
-      hf[i] = make_double2(sf[i].x, sf[i].y);
-      hg[i] = make_double2(sg[i].x, sg[i].y);
+      hf[i] = rec[2 * i];
+      hg[i] = rec[2 * i + 1];
+    }
+  } else {
+    std::vector<float2> rec(2 * nn1);
+    CUDA_TRY(cudaMemcpyAsync(rec.data(), ctx->w_fr, nn1 * ctx->frame_rec(), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    for (size_t i = 0; i < nn1; ++i) {
+      hf[i] = make_double2(rec[2 * i].x, rec[2 * i].y);
+      hg[i] = make_double2(rec[2 * i + 1].x, rec[2 * i + 1].y);
     }
   }
   for (size_t i = 0; i < nn1; ++i) {
@@ -3161,7 +3218,7 @@ int sc_profile(sc_ctx *ctx, int enable) {
 }
 
 int sc_profile_read(sc_ctx *ctx, int kernel, double *total_ms, long long *launches) {
-  if (!ctx || kernel < 0 || kernel > 3) return SC_ERR_ARG;
+  if (!ctx || kernel < 0 || kernel > 4) return SC_ERR_ARG;
   API_BEGIN
   CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   double t = 0.0;
@@ -3258,7 +3315,7 @@ __global__ void k_gather_scalars(int n, const Scalars *const *src, Scalars *dst)
 
 size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 size_t grain_footprint(const sc_ctx *c) {
-  return align256(c->need_scratch) + align256(c->need_scratch2) + 2 * align256(c->need_frame);
+  return align256(c->need_scratch) + align256(c->need_scratch2) + align256(c->need_frame);
 }
 
 // Packs the active grains into waves (largest first, first fit) and points
@@ -3288,9 +3345,7 @@ void batch_plan(sc_batch *b) {
     base += align256(c->need_scratch);
     c->w_scratch2 = (double *)base;
     base += align256(c->need_scratch2);
-    c->w_fg = (double *)base;
-    base += align256(c->need_frame);
-    c->w_gi = (double *)base;
+    c->w_fr = (double *)base;
     used[w] += f;
     members[w].push_back(g);
   }
@@ -3425,8 +3480,7 @@ void batch_sweeps(sc_batch *b) {
       const size_t nn1 = (size_t)c->S.n1 * c->S.n1;
       const int nslots = chunk_slots(c, ch);
       if (!c->frames_zeroed) {
-        CUDA_TRY(cudaMemsetAsync(c->w_fg, 0, (size_t)nslots * nn1 * c->frame_elem(), c->stream));
-        CUDA_TRY(cudaMemsetAsync(c->w_gi, 0, (size_t)nslots * nn1 * c->frame_elem(), c->stream));
+        CUDA_TRY(cudaMemsetAsync(c->w_fr, 0, (size_t)nslots * nn1 * c->frame_rec(), c->stream));
         c->frames_zeroed = true;
       }
       launch_frame_fields<R>(c, ch, sweep_args<R>(c, &ch, 0));

@@ -189,7 +189,7 @@ class Context:
 
     def profile(self, enable: bool = True):
         """Enables CUDA-event timing of the sweep (0), rotate-back (1), Poisson
-        (2) and boundary (3) kernels."""
+        (2), boundary (3) and frame-field (4) kernels."""
         self._check(_lib.load().sc_profile(self._h, 1 if enable else 0))
 
     def profile_read(self, kernel: int):
