@@ -722,21 +722,23 @@ __global__ void __launch_bounds__(256, NC == 1 ? 4 : 3) k_rotate_back(int n0, in
       // corner (xi + dx, yi + dy) of angle a is site nn1 - 1 - i00 - dx - n1 dy of angle a0
       const size_t m = slot + (nn1 - 1 - (size_t)b.i00);
       r00 = load_rec(fr, m); r01 = load_rec(fr, m - 1); r10 = load_rec(fr, m - n1); r11 = load_rec(fr, m - n1 - 1);
-      r00.q.x = -r00.q.x; r01.q.x = -r01.q.x; r10.q.x = -r10.q.x; r11.q.x = -r11.q.x;
     }
-    const double2 f00 = r00.f, f01 = r01.f, f10 = r10.f, f11 = r11.f;
-    const double2 q00 = r00.q, q01 = r01.q, q10 = r10.q, q11 = r11.q;
-    const double fre = bilerp(f00.x, f01.x, f10.x, f11.x, b.xf, b.yf);
-    const double fim = bilerp(f00.y, f01.y, f10.y, f11.y, b.xf, b.yf);
+    const double fre = bilerp(r00.f.x, r01.f.x, r10.f.x, r11.f.x, b.xf, b.yf);
+    const double fim = bilerp(r00.f.y, r01.f.y, r10.f.y, r11.f.y, b.xf, b.yf);
 #pragma unroll
     for (int c = 0; c < nc; ++c) {
       const double et = P.eta[c];
       dr[c] += (fre * et) * pw;
       di[c] += (fim * et) * pw;
     }
-    jx += bilerp(q00.x * psx, q01.x * psx, q10.x * psx, q11.x * psx, b.xf, b.yf);
-    jy += bilerp(q00.x * psy, q01.x * psy, q10.x * psy, q11.x * psy, b.xf, b.yf);
-    fe += bilerp(q00.y * pw, q01.y * pw, q10.y * pw, q11.y * pw, b.xf, b.yf);
+    // Re g and Re I are interpolated once and weighted afterwards (the same
+    // linear map as weighting the corners; the mirrored angle's Re g is minus
+    // the stored one).
+    const double gq = bilerp(r00.q.x, r01.q.x, r10.q.x, r11.q.x, b.xf, b.yf);
+    const double g = mirrored ? -gq : gq;
+    jx += g * psx;
+    jy += g * psy;
+    fe += bilerp(r00.q.y, r01.q.y, r10.q.y, r11.q.y, b.xf, b.yf) * pw;
   }
 #pragma unroll
   for (int c = 0; c < nc; ++c) {
@@ -1791,7 +1793,12 @@ SweepArgs<R> sweep_args(sc_ctx *c, const Chunk *ch, int burn_in) {
 template <typename R>
 void launch_frame_fields(sc_ctx *c, const Chunk &ch, const SweepArgs<R> &A) {
   if (!A.n_items) return;
-  const int rows = 4 * FF_ROWS;  // rows per block, four per thread
+  // Rows per block: a block's eight columns are walked down by its sixteen
+  // row threads, so its gathers stay within a narrow strip of the reference
+  // grid (L1 reuse) and each thread loads its column and angle once (C2:
+  // 1024 rows per block 0.67 ms mixed, 1.47 ms FP64 against 0.86 and 1.90
+  // with 64, and 1.24 / 2.88 with 16).
+  const int rows = 64 * FF_ROWS;
   dim3 grid(grid1(A.n_items, FF_COLS), (unsigned)((ch.kmax + rows - 1) / rows));
   ProfScope prof(c, 4);
   k_frame_fields<R><<<grid, dim3(FF_COLS, FF_ROWS), 0, c->stream>>>(A, rows);
