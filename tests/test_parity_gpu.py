@@ -634,3 +634,32 @@ def test_mixed_mirror_pairing(engine_lib, monkeypatch):
         (d1, j1, a1), (d2, j2, a2) = out
         assert np.max(np.abs(d1 - d2)) / db <= 1e-5
         assert _rel(j1, j2) <= 1e-4
+
+
+@pytest.mark.parametrize("groups", [1, 2, 4, 8])
+def test_group_sizes_match_oracle(engine_lib, monkeypatch, groups):
+    """Every threads-per-column mapping (SCB_ENERGY_GROUPS: one thread holds
+    all energies and stores the whole frame record; two share the record by
+    halves; four and eight store one value each) against the oracle over two
+    iterations in FP64 (1e-10), and in mixed precision against FP64 (1e-5 of
+    the bulk gap)."""
+    import superconga_b200 as sb
+    cfg, kw = CASES["small_square_d"]
+    monkeypatch.setenv("SCB_ENERGY_GROUPS", str(groups))
+    o, e, db = _pair(cfg, **kw)
+    m = sb.Context(cfg, mode="mixed")
+    m.set_state(*e.state())
+    for it in range(2):
+        o.compute()
+        e.compute(1)
+        m.compute(1)
+        d_o, j_o, _ = o.results()
+        d_e, j_e, _ = e.results()
+        assert _rel(d_e, d_o) < TOL, (groups, it, "delta")
+        assert _rel(j_e, j_o) < TOL, (groups, it, "current")
+        so, se = o.scalars(), e.scalars()
+        assert abs(se["free_energy"] - so["free_energy"]) <= TOL * abs(so["free_energy"]), (groups, it)
+        d_m = m.results()[0]
+        assert np.max(np.abs(d_m - d_e)) / db <= 1e-5, (groups, it)
+    e.close()
+    m.close()
