@@ -115,6 +115,100 @@ __device__ __forceinline__ Cx<R> riccati_step(R dre, R dim, R ere, R eim, Cx<R> 
   return Cx<R>{(c2r * den_re + c2i * den_im) * inv, (c2i * den_re - c2r * den_im) * inv};
 }
 
+// Two energies of one thread, lane by lane in FP32 pairs:
+// re = (Re z_j, Re z_j+1), im = (Im z_j, Im z_j+1).  sm_100 executes one
+// FFMA2 / FMUL2 / FADD2 instruction for both lanes, so the FP32 arithmetic of
+// the mixed-precision sweep takes half the issue slots; the square roots and
+// reciprocals stay one MUFU instruction per lane.  Each lane is rounded as the
+// scalar FP32 operation would be.
+struct Cx2 {
+  float2 re, im;
+};
+__device__ __forceinline__ float2 bc2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ Cx2 pack2(Cx<float> a, Cx<float> b) {
+  return Cx2{make_float2(a.re, b.re), make_float2(a.im, b.im)};
+}
+__device__ __forceinline__ void unpack2(Cx2 v, Cx<float> &a, Cx<float> &b) {
+  a = Cx<float>{v.re.x, v.im.x};
+  b = Cx<float>{v.re.y, v.im.y};
+}
+
+// csqrt_dev of both lanes.
+__device__ __forceinline__ Cx2 csqrt2(float2 x, float2 y) {
+  const float2 xx = fma2(x, x, mul2(y, y));
+  const float2 m = make_float2(sqrt_(xx.x), sqrt_(xx.y));
+  const float2 u = mul2(bc2(0.5f), add2(m, make_float2(fabsf(x.x), fabsf(x.y))));
+  const float2 r = make_float2(rsqrt_(fmaxf(u.x, 1.17549435e-38f)), rsqrt_(fmaxf(u.y, 1.17549435e-38f)));
+  const float2 t = mul2(u, r);
+  const float2 v = mul2(mul2(bc2(0.5f), make_float2(fabsf(y.x), fabsf(y.y))), r);
+  const bool p0 = x.x >= 0.0f, p1 = x.y >= 0.0f;
+  return Cx2{make_float2(p0 ? t.x : v.x, p1 ? t.y : v.y),
+             make_float2(copysignf(p0 ? v.x : t.x, y.x), copysignf(p1 ? v.y : t.y, y.y))};
+}
+
+// riccati_step<float> of two energies e = ere + i eim (ere: the real part
+// with the site's Doppler shift added; Matsubara energies have ere = the
+// shift alone) at the same site fields and step h.
+__device__ __forceinline__ Cx2 riccati_step2(float dre, float dim, float2 ere, float2 eim, Cx2 g, float h) {
+  const float q = 0.25f * h;
+  const float2 ar = bc2(q * dim), ai = bc2(q * dre);
+  const float2 ser = mul2(bc2(-h), eim);  // Re of (i h) * e
+  const float2 sei = mul2(bc2(h), ere);   // Im of (i h) * e
+  const float2 agre = fma2(ar, g.re, mul2(neg2(ai), g.im));
+  const float2 agim = fma2(ar, g.im, mul2(ai, g.re));
+  const float2 bm = add2(ser, bc2(-1.0f));
+  const float2 bre = fma2(bc2(2.0f), agre, bm);
+  const float2 bim = fma2(bc2(2.0f), agim, sei);
+  const float2 tre = add2(agre, add2(ser, bc2(1.0f)));
+  const float2 tim = add2(agim, sei);
+  const float2 cre = fma2(tre, g.re, fma2(neg2(tim), g.im, bc2(-h * dim)));
+  const float2 cim = fma2(tre, g.im, fma2(tim, g.re, bc2(h * dre)));
+  const float2 s0 = fma2(neg2(sei), sei, bc2(h * h * (dre * dre + dim * dim)));
+  const Cx2 disc = csqrt2(fma2(bc2(-8.0f), agre, fma2(bm, bm, s0)),
+                          fma2(bc2(-8.0f), agim, mul2(add2(bm, bm), sei)));
+  const float2 dr = add2(disc.re, neg2(bre)), di = add2(disc.im, neg2(bim));
+  const float2 s = fma2(dr, dr, mul2(di, di));
+  // 2 c / den = 2 c conj(den) / |den|^2 (the factor 2 is exact, so it goes with 1/|den|^2).
+  const float2 inv2 = mul2(bc2(2.0f), make_float2(rcp_(s.x), rcp_(s.y)));
+  return Cx2{mul2(fma2(cre, dr, mul2(cim, di)), inv2), mul2(fma2(cim, dr, mul2(neg2(cre), di)), inv2)};
+}
+
+// local_greens<float> of two energies, before the signs: with p = g gt and
+// w = 2 / |1 + p|^2, fre = w Im p, fim = w (1 + Re p); then
+//   Re g = -fre, f + f~* = (fre ure - fim uim, -(fre vim + fim vre)),
+//   Im I = -(Re D uim + Im D vre),
+// u = gt - g, v = g + gt.  Returns fre, F.re, nfim = fre vim + fim vre
+// (F.im = -nfim) and ni = Re D uim + Im D vre (Im I = -ni).
+__device__ __forceinline__ void local_greens2(Cx2 g, Cx2 gt, float dre, float dim, float2 &fre,
+                                              float2 &Fre, float2 &nfim, float2 &ni) {
+  const float2 pre = fma2(g.re, gt.re, mul2(neg2(g.im), gt.im));
+  const float2 pim = fma2(g.re, gt.im, mul2(g.im, gt.re));
+  const float2 den_re = add2(bc2(1.0f), pre);
+  const float2 s = fma2(den_re, den_re, mul2(pim, pim));
+  const float2 w = mul2(bc2(2.0f), make_float2(rcp_(s.x), rcp_(s.y)));
+  fre = mul2(pim, w);
+  const float2 fim = mul2(den_re, w);
+  const float2 ure = add2(gt.re, neg2(g.re)), uim = add2(gt.im, neg2(g.im));
+  const float2 vre = add2(g.re, gt.re), vim = add2(g.im, gt.im);
+  Fre = fma2(fre, ure, mul2(neg2(fim), uim));
+  nfim = fma2(fre, vim, mul2(fim, vre));
+  ni = fma2(bc2(dre), uim, mul2(bc2(dim), vre));
+}
+
+// greens_g_im<float> of two real energies: Im g = -[(1 - Re p)(1 + Re p) - (Im p)^2] / |1 + p|^2.
+__device__ __forceinline__ float2 greens_g_im2(Cx2 g, Cx2 gt) {
+  const float2 pre = fma2(g.re, gt.re, mul2(neg2(g.im), gt.im));
+  const float2 pim = fma2(g.re, gt.im, mul2(g.im, gt.re));
+  const float2 den_re = add2(bc2(1.0f), pre), nr = add2(bc2(1.0f), neg2(pre));
+  const float2 s = fma2(den_re, den_re, mul2(pim, pim));
+  const float2 inv = make_float2(rcp_(s.x), rcp_(s.y));
+  return mul2(fma2(nr, den_re, mul2(neg2(pim), pim)), neg2(inv));
+}
+
 // Homogeneous solutions, riccati::computeHomogeneous (RiccatiSolutions.h:36-54).
 template <typename R>
 __device__ __forceinline__ void riccati_homogeneous(R dre, R dim, R ere, R eim, Cx<R> &g,

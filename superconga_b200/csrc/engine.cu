@@ -29,6 +29,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/scb200.h"
@@ -170,6 +171,15 @@ __device__ __forceinline__ size_t scratch_index(const SweepArgs<R> &A, int lg, i
   const int sh = 5 - lg;
   const size_t tile = (size_t)(item >> sh), k = (size_t)(item & ((1 << sh) - 1));
   return (((tile * A.kmax + r) * A.ne + e) << sh) + k;
+}
+// The packed FP32 sweep keeps energies 2p and 2p + 1 together as one 16-byte
+// record (Re, Re, Im, Im): [tile][row][energy pair][column of tile], so a
+// thread stores and loads both of its energies with one vector access.
+template <typename R>
+__device__ __forceinline__ size_t scratch_pair_index(const SweepArgs<R> &A, int lg, int item, int r, int p) {
+  const int sh = 5 - lg;
+  const size_t tile = (size_t)(item >> sh), k = (size_t)(item & ((1 << sh) - 1));
+  return (((tile * A.kmax + r) * (size_t)((A.ne + 1) >> 1) + p) << sh) + k;
 }
 // Frame-field records, one per column site in the same tiles: (Re D, Im D,
 // energy shift, frame label), [tile][row][column of tile], read by the sweep
@@ -385,6 +395,83 @@ __device__ __forceinline__ void interior_step(R dre, R dim, R es, R pdre, R pdim
     if (j < ept) coh[j] = riccati_step<R>(sdre, sdim, KEL ? ses + ere[j] : ses, eim[j], coh[j], h);
 }
 
+// site_step and interior_step of the packed FP32 sweep: energies in pairs
+// (riccati_step2), every thread with its full EMAX energies (the launch
+// guarantees ept = EMAX).
+// The real parts of energies j, j + 1 with the Doppler shift es added (KEL:
+// real energies; Matsubara energies have none).
+template <bool KEL>
+__device__ __forceinline__ float2 ere_pair(const float *ere, int j, float es) {
+  return KEL ? make_float2(es + ere[j], es + ere[j + 1]) : bc2(es);
+}
+template <int EMAX, bool KEL>
+__device__ __forceinline__ void site_step_x2(uint8_t l, uint8_t l_entry, uint8_t l_exit, float dre, float dim,
+                                             float es, float pdre, float pdim, float pes, const float *ere,
+                                             const float *eim, Cx<float> *coh, int ecount, float h,
+                                             float dist_in, const Cx<float> *bin, float dist_out,
+                                             Cx<float> *bout) {
+  const bool entry = l == l_entry;
+  const float sdre = entry ? dre : (dre + pdre) * 0.5f;
+  const float sdim = entry ? dim : (dim + pdim) * 0.5f;
+  const float ses = entry ? es : (es + pes) * 0.5f;
+  const float st = entry ? dist_in * h : h;
+  const Cx<float> zero{0.0f, 0.0f};
+#pragma unroll
+  for (int j = 0; j < EMAX; j += 2) {
+    Cx2 g0 = pack2(coh[j], coh[j + 1]);
+    if (entry) g0 = pack2(j < ecount ? bin[j] : zero, j + 1 < ecount ? bin[j + 1] : zero);
+    unpack2(riccati_step2(sdre, sdim, ere_pair<KEL>(ere, j, ses), make_float2(eim[j], eim[j + 1]), g0, st), coh[j],
+            coh[j + 1]);
+  }
+  if (l == l_exit) {
+    const float sb = dist_out * h;
+#pragma unroll
+    for (int j = 0; j < EMAX; j += 2) {
+      Cx<float> b0, b1;
+      unpack2(riccati_step2(dre, dim, ere_pair<KEL>(ere, j, es), make_float2(eim[j], eim[j + 1]),
+                            pack2(coh[j], coh[j + 1]), sb),
+              b0, b1);
+      if (j < ecount) bout[j] = b0;
+      if (j + 1 < ecount) bout[j + 1] = b1;
+    }
+  }
+  if (l == 0) {
+#pragma unroll
+    for (int j = 0; j < EMAX; ++j) coh[j] = zero;
+  }
+}
+template <int EMAX, bool KEL>
+__device__ __forceinline__ void interior_step_x2(float dre, float dim, float es, float pdre, float pdim, float pes,
+                                                 const float *ere, const float *eim, Cx<float> *coh, float h) {
+  const float sdre = (dre + pdre) * 0.5f;
+  const float sdim = (dim + pdim) * 0.5f;
+  const float ses = (es + pes) * 0.5f;
+#pragma unroll
+  for (int j = 0; j < EMAX; j += 2)
+    unpack2(riccati_step2(sdre, sdim, ere_pair<KEL>(ere, j, ses), make_float2(eim[j], eim[j + 1]),
+                          pack2(coh[j], coh[j + 1]), h),
+            coh[j], coh[j + 1]);
+}
+
+// Dispatch of one site's steps to the packed (PK) or the scalar form.
+template <typename R, int EMAX, bool KEL, bool PK>
+__device__ __forceinline__ void interior_any(R dre, R dim, R es, R pdre, R pdim, R pes, const R *ere,
+                                             const R *eim, Cx<R> *coh, int ept, R h) {
+  if constexpr (PK) interior_step_x2<EMAX, KEL>(dre, dim, es, pdre, pdim, pes, ere, eim, coh, h);
+  else interior_step<R, EMAX, KEL>(dre, dim, es, pdre, pdim, pes, ere, eim, coh, ept, h);
+}
+template <typename R, int EMAX, bool KEL, bool PK>
+__device__ __forceinline__ void site_any(uint8_t l, uint8_t l_entry, uint8_t l_exit, R dre, R dim, R es, R pdre,
+                                         R pdim, R pes, const R *ere, const R *eim, Cx<R> *coh, int ept,
+                                         int ecount, R h, R dist_in, const Cx<R> *bin, R dist_out, Cx<R> *bout) {
+  if constexpr (PK)
+    site_step_x2<EMAX, KEL>(l, l_entry, l_exit, dre, dim, es, pdre, pdim, pes, ere, eim, coh, ecount, h, dist_in,
+                            bin, dist_out, bout);
+  else
+    site_step<R, EMAX, KEL>(l, l_entry, l_exit, dre, dim, es, pdre, pdim, pes, ere, eim, coh, ept, ecount, h,
+                            dist_in, bin, dist_out, bout);
+}
+
 // The fused Riccati sweep of one chunk of angles.  G = 2^log_groups threads
 // share one trajectory column (angle, x); thread g integrates Ozaki energies
 // [g*ept, g*ept + ept).  gammaTilde runs down the column first and is kept in
@@ -400,9 +487,13 @@ __device__ __forceinline__ void interior_step(R dre, R dim, R es, R pdre, R pdim
 // STEP_PER_ANGLE: the Riccati step h/|v_F| is read per angle (a non-circular
 // Fermi surface, and the batch); otherwise it is the uniform lattice spacing h
 // of the circle, which stays a kernel parameter.
-template <typename R, int EMAX, bool KEL, bool STEP_PER_ANGLE, int LG = -1>
+// PK: the packed FP32 form (energies in pairs: riccati_step2, local_greens2 or
+// greens_g_im2, the scratch in energy-pair records); the launch guarantees
+// ept = EMAX (even) so that every thread's first energy is even.
+template <typename R, int EMAX, bool KEL, bool STEP_PER_ANGLE, int LG = -1, bool PK = false>
 __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double *s_res, int item,
                                              int g, unsigned gmask) {
+  static_assert(!PK || (std::is_same<R, float>::value && EMAX % 2 == 0), "packed sweep: FP32 pairs");
   const int lgc = LG >= 0 ? LG : A.log_groups;  // a compile-time group size when the launch knows it
   const int4 it = A.items[item];
   const int a = it.x, x = it.y, lo = it.z, hi = it.w;
@@ -412,7 +503,7 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
   const R h = STEP_PER_ANGLE ? (R)A.ang[a].hs : (R)A.h;  // h / |v_F| of this angle
   // A compile-time group size comes with a full load (EMAX energies per
   // thread), a sweep that stores its frame sums, and no energy passes.
-  const int ept = LG >= 0 ? EMAX : A.ept;
+  const int ept = (LG >= 0 || PK) ? EMAX : A.ept;
   const bool burn_in = LG >= 0 ? false : A.burn_in != 0;
   const bool accumulate = LG >= 0 ? false : A.accumulate != 0;
   const int e0 = g * ept;
@@ -428,7 +519,8 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
   }
 
   Cx<R> coh[EMAX];
-  const size_t sb0 = scratch_index(A, lgc, item, 0, e0), s_row = (size_t)ne * T;
+  const size_t sb0 = PK ? scratch_pair_index(A, lgc, item, 0, e0 >> 1) : scratch_index(A, lgc, item, 0, e0);
+  const size_t s_row = PK ? (size_t)((ne + 1) >> 1) * T : (size_t)ne * T;
   const size_t ax = (size_t)a * n1 + x;
   // Mirrored partner column (angle + pi, x -> n1 - 1 - x) when paired.
   const size_t pax = (size_t)(a + A.pair) * n1 + (n1 - 1 - x);
@@ -451,14 +543,14 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
       const R dre = (R)(-fr.x), dim = (R)fr.y, es = (R)fr.z;
       if (y > lo) fr = fb[(size_t)(r - 1) * T];
       if (l == 1) {
-        interior_step<R, EMAX, KEL>(dre, dim, es, pdre, pdim, pes, ere, eim, coh, ept, h);
+        interior_any<R, EMAX, KEL, PK>(dre, dim, es, pdre, pdim, pes, ere, eim, coh, ept, h);
       } else {
         const bool entry = l == 3, exit = l == 2;
         const R din = entry ? (R)A.dist_in_gt[in_base + nin] : R(0);
         const R dout = exit ? (R)A.dist_out_gt[out_base + nout] : R(0);
-        site_step<R, EMAX, KEL>(l, 3, 2, dre, dim, es, pdre, pdim, pes, ere, eim, coh, ept, ecount, h,
-                                din, A.bin_gt + (size_t)(in_base + nin) * A.ne_stride + e0, dout,
-                                A.bout_gt + (size_t)(out_base + nout) * A.ne_stride + e0);
+        site_any<R, EMAX, KEL, PK>(l, 3, 2, dre, dim, es, pdre, pdim, pes, ere, eim, coh, ept, ecount, h,
+                                   din, A.bin_gt + (size_t)(in_base + nin) * A.ne_stride + e0, dout,
+                                   A.bout_gt + (size_t)(out_base + nout) * A.ne_stride + e0);
         if (A.pair && exit) {
           // gamma of the partner angle at its exit is conj(gammaTilde) here.
           const Cx<R> *src = A.bout_gt + (size_t)(out_base + nout) * A.ne_stride + e0;
@@ -471,10 +563,17 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
         nout += exit;
       }
       if (!burn_in) {
-        Cx<R> *sc = A.scratch + sb0 + (size_t)r * s_row;
+        if constexpr (PK) {
+          float4 *sc = (float4 *)A.scratch + sb0 + (size_t)r * s_row;
 #pragma unroll
-        for (int j = 0; j < EMAX; ++j)
-          if (j < ecount) sc[(size_t)j * T] = coh[j];
+          for (int j = 0; j < EMAX; j += 2)
+            if (j < ecount) sc[(size_t)(j >> 1) * T] = make_float4(coh[j].re, coh[j + 1].re, coh[j].im, coh[j + 1].im);
+        } else {
+          Cx<R> *sc = A.scratch + sb0 + (size_t)r * s_row;
+#pragma unroll
+          for (int j = 0; j < EMAX; ++j)
+            if (j < ecount) sc[(size_t)j * T] = coh[j];
+        }
       }
       pdre = dre;
       pdim = dim;
@@ -496,12 +595,25 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
     const V4 *fb = (const V4 *)A.scratch2 + rec_index(A, lgc, item, 0);
     V4 fr = fb[0];
     Cx<R> gt_nx[EMAX];
-    if (!burn_in) {
-      const Cx<R> *sc = A.scratch + sb0;
+    // The stored gammaTilde of row r into gt_nx.
+    auto load_gt = [&](int r) {
+      if constexpr (PK) {
+        const float4 *sc = (const float4 *)A.scratch + sb0 + (size_t)r * s_row;
 #pragma unroll
-      for (int j = 0; j < EMAX; ++j)
-        if (j < ecount) gt_nx[j] = sc[(size_t)j * T];
-    }
+        for (int j = 0; j < EMAX; j += 2)
+          if (j < ecount) {
+            const float4 v = sc[(size_t)(j >> 1) * T];
+            gt_nx[j] = Cx<R>{v.x, v.z};
+            gt_nx[j + 1] = Cx<R>{v.y, v.w};
+          }
+      } else {
+        const Cx<R> *sc = A.scratch + sb0 + (size_t)r * s_row;
+#pragma unroll
+        for (int j = 0; j < EMAX; ++j)
+          if (j < ecount) gt_nx[j] = sc[(size_t)j * T];
+      }
+    };
+    if (!burn_in) load_gt(0);
     for (int y = lo; y <= hi; ++y) {
       const int r = y - lo;
       const uint8_t l = (uint8_t)fr.w;
@@ -511,22 +623,17 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
       for (int j = 0; j < EMAX; ++j) gt[j] = gt_nx[j];
       if (y < hi) {
         fr = fb[(size_t)(r + 1) * T];
-        if (!burn_in) {
-          const Cx<R> *sc = A.scratch + sb0 + (size_t)(r + 1) * s_row;
-#pragma unroll
-          for (int j = 0; j < EMAX; ++j)
-            if (j < ecount) gt_nx[j] = sc[(size_t)j * T];
-        }
+        if (!burn_in) load_gt(r + 1);
       }
       if (l == 1) {
-        interior_step<R, EMAX, KEL>(dre, dim, es, pdre, pdim, pes, ere, eim, coh, ept, h);
+        interior_any<R, EMAX, KEL, PK>(dre, dim, es, pdre, pdim, pes, ere, eim, coh, ept, h);
       } else {
         const bool entry = l == 2, exit = l == 3;
         const R din = entry ? (R)A.dist_in_g[in_base + nin] : R(0);
         const R dout = exit ? (R)A.dist_out_g[out_base + nout] : R(0);
-        site_step<R, EMAX, KEL>(l, 2, 3, dre, dim, es, pdre, pdim, pes, ere, eim, coh, ept, ecount, h,
-                                din, A.bin_g + (size_t)(in_base + nin) * A.ne_stride + e0, dout,
-                                A.bout_g + (size_t)(out_base + nout) * A.ne_stride + e0);
+        site_any<R, EMAX, KEL, PK>(l, 2, 3, dre, dim, es, pdre, pdim, pes, ere, eim, coh, ept, ecount, h,
+                                   din, A.bin_g + (size_t)(in_base + nin) * A.ne_stride + e0, dout,
+                                   A.bout_g + (size_t)(out_base + nout) * A.ne_stride + e0);
         if (A.pair && exit) {
           // gammaTilde of the partner angle at its exit is conj(gamma) here.
           const Cx<R> *src = A.bout_g + (size_t)(out_base + nout) * A.ne_stride + e0;
@@ -545,14 +652,47 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
       if constexpr (KEL) {
         if (l != 0) {
           double *o = A.ldf + ((size_t)(a - A.slot_base) * nn1 + (size_t)y * n1 + x) * A.ne_stride + e0;
+          if constexpr (PK) {
 #pragma unroll
-          for (int j = 0; j < EMAX; ++j)
-            if (j < ecount) o[j] = (double)greens_g_im<R>(coh[j], gt[j]);
+            for (int j = 0; j < EMAX; j += 2)
+              if (j < ecount) {
+                const float2 v = greens_g_im2(pack2(coh[j], coh[j + 1]), pack2(gt[j], gt[j + 1]));
+                o[j] = (double)v.x;
+                if (j + 1 < ecount) o[j + 1] = (double)v.y;
+              }
+          } else {
+#pragma unroll
+            for (int j = 0; j < EMAX; ++j)
+              if (j < ecount) o[j] = (double)greens_g_im<R>(coh[j], gt[j]);
+          }
         }
         continue;
       }
       double sfr = 0.0, sfi = 0.0, sg = 0.0, si = 0.0;
-      if (l != 0) {
+      if constexpr (PK) {
+        if (l != 0) {
+          // Signs folded into the FP64 accumulation: sg = -sum r fre,
+          // sfi = -sum r nfim, si = -sum r ni.
+#pragma unroll
+          for (int j = 0; j < EMAX; j += 2)
+            if (j < ecount) {
+              float2 fre, Fre, nfim, ni;
+              local_greens2(pack2(coh[j], coh[j + 1]), pack2(gt[j], gt[j + 1]), dre, dim, fre, Fre, nfim, ni);
+              const double r0 = s_res[e0 + j];
+              sfr += r0 * (double)Fre.x;
+              sfi -= r0 * (double)nfim.x;
+              sg -= r0 * (double)fre.x;
+              si -= r0 * (double)ni.x;
+              if (j + 1 < ecount) {
+                const double r1 = s_res[e0 + j + 1];
+                sfr += r1 * (double)Fre.y;
+                sfi -= r1 * (double)nfim.y;
+                sg -= r1 * (double)fre.y;
+                si -= r1 * (double)ni.y;
+              }
+            }
+        }
+      } else if (l != 0) {
 #pragma unroll
         for (int j = 0; j < EMAX; ++j)
           if (j < ecount) {
@@ -603,7 +743,7 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
   }
 }
 
-template <typename R, int EMAX, int MINB, bool KEL, bool STEP_PER_ANGLE = false, int LG = -1>
+template <typename R, int EMAX, int MINB, bool KEL, bool STEP_PER_ANGLE = false, int LG = -1, bool PK = false>
 __global__ void __launch_bounds__(128, MINB) k_sweep(const SweepArgs<R> A) {
   __shared__ double s_res[SWEEP_MAX_ENERGIES];  // residues of this pass's energies
   for (int e = threadIdx.x; e < A.ne && e < SWEEP_MAX_ENERGIES; e += blockDim.x) s_res[e] = A.res[e];
@@ -615,7 +755,7 @@ __global__ void __launch_bounds__(128, MINB) k_sweep(const SweepArgs<R> A) {
   const int lane = threadIdx.x & 31;
   const unsigned gmask = ((groups == 32) ? 0xffffffffu : ((1u << groups) - 1u)) << (lane & ~(groups - 1));
   if (item >= A.n_items) return;  // whole groups leave together (groups divide the warp)
-  sweep_column<R, EMAX, KEL, STEP_PER_ANGLE, LG>(A, s_res, item, g, gmask);
+  sweep_column<R, EMAX, KEL, STEP_PER_ANGLE, LG, PK>(A, s_res, item, g, gmask);
 }
 
 // The sweep of many grains in one persistent launch.  A work unit is one
@@ -1832,12 +1972,35 @@ void launch_sweep_pass(sc_ctx *c, const SweepArgs<R> &A, unsigned blocks) {
       else k_sweep<R, 16, 1, false, true><<<blocks, 128, 0, c->stream>>>(A);
     }
   } else if (c->S.keldysh) {
+    static const bool no_packed_kel = std::getenv("SCB_NO_PACKED") != nullptr;
+    if constexpr (std::is_same<R, float>::value) {
+      // Mixed-precision LDOS: four real energies per thread in two FP32 pairs.
+      if (!no_packed_kel && c->ept == 4) {
+        if (plain && c->log_groups == 3) k_sweep<R, 4, 1, true, false, 3, true><<<blocks, 128, 0, c->stream>>>(A);
+        else k_sweep<R, 4, 1, true, false, -1, true><<<blocks, 128, 0, c->stream>>>(A);
+        check_launch(c);
+        return;
+      }
+    }
     if (plain && c->ept == 4 && c->log_groups == 3) k_sweep<R, 4, 1, true, false, 3><<<blocks, 128, 0, c->stream>>>(A);
     else if (c->ept <= 4) k_sweep<R, 4, 1, true><<<blocks, 128, 0, c->stream>>>(A);
     else if (c->ept <= 8) k_sweep<R, 8, 1, true><<<blocks, 128, 0, c->stream>>>(A);
     else k_sweep<R, 16, 1, true><<<blocks, 128, 0, c->stream>>>(A);
   } else if (c->ept <= 2 && c->emax2) {
     const bool g8 = plain && c->log_groups == 3 && c->ept == 2;
+    if constexpr (std::is_same<R, float>::value) {
+      // Two energies per thread: the packed FP32 form (both energies in one
+      // FFMA2 / FMUL2 / FADD2 per operation).
+      static const bool no_packed = std::getenv("SCB_NO_PACKED") != nullptr;
+      if (!no_packed && c->ept == 2 && (variant >= 6 || variant == 4)) {
+        if (variant >= 6 && g8) k_sweep<R, 2, 6, false, false, 3, true><<<blocks, 128, 0, c->stream>>>(A);
+        else if (variant >= 6) k_sweep<R, 2, 6, false, false, -1, true><<<blocks, 128, 0, c->stream>>>(A);
+        else if (g8) k_sweep<R, 2, 4, false, false, 3, true><<<blocks, 128, 0, c->stream>>>(A);
+        else k_sweep<R, 2, 4, false, false, -1, true><<<blocks, 128, 0, c->stream>>>(A);
+        check_launch(c);
+        return;
+      }
+    }
     if (variant >= 6 && g8) k_sweep<R, 2, 6, false, false, 3><<<blocks, 128, 0, c->stream>>>(A);
     else if (variant >= 6) k_sweep<R, 2, 6, false><<<blocks, 128, 0, c->stream>>>(A);
     else if (variant == 4 && g8) k_sweep<R, 2, 4, false, false, 3><<<blocks, 128, 0, c->stream>>>(A);
@@ -2609,7 +2772,8 @@ void upload_static(sc_ctx *c) {
   for (const Chunk &ch : c->chunks) {
     const size_t ni = (size_t)(ch.item_end - ch.item_begin);
     const size_t ni32 = (ni + 31) / 32 * 32;  // whole scratch tiles
-    scr = std::max(scr, ni32 * ch.kmax * c->e_pass * c->esize());
+    // Energies per row rounded up to even: the packed FP32 sweep stores them in pairs.
+    scr = std::max(scr, ni32 * ch.kmax * (size_t)((c->e_pass + 1) & ~1) * c->esize());
     scr2 = std::max(scr2, ni32 * ch.kmax * 4);
     max_slots = std::max(max_slots, chunk_slots(c, ch));
   }
