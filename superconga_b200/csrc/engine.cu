@@ -407,7 +407,7 @@ __device__ __forceinline__ float2 ere_pair(const float *ere, int j, float es) {
 template <int EMAX, bool KEL>
 __device__ __forceinline__ void site_step_x2(uint8_t l, uint8_t l_entry, uint8_t l_exit, float dre, float dim,
                                              float es, float pdre, float pdim, float pes, const float *ere,
-                                             const float *eim, Cx<float> *coh, int ecount, float h,
+                                             const float *eim, Cx<float> *coh, int ept, int ecount, float h,
                                              float dist_in, const Cx<float> *bin, float dist_out,
                                              Cx<float> *bout) {
   const bool entry = l == l_entry;
@@ -418,6 +418,7 @@ __device__ __forceinline__ void site_step_x2(uint8_t l, uint8_t l_entry, uint8_t
   const Cx<float> zero{0.0f, 0.0f};
 #pragma unroll
   for (int j = 0; j < EMAX; j += 2) {
+    if (j >= ept) break;
     Cx2 g0 = pack2(coh[j], coh[j + 1]);
     if (entry) g0 = pack2(j < ecount ? bin[j] : zero, j + 1 < ecount ? bin[j + 1] : zero);
     unpack2(riccati_step2(sdre, sdim, ere_pair<KEL>(ere, j, ses), make_float2(eim[j], eim[j + 1]), g0, st), coh[j],
@@ -427,6 +428,7 @@ __device__ __forceinline__ void site_step_x2(uint8_t l, uint8_t l_entry, uint8_t
     const float sb = dist_out * h;
 #pragma unroll
     for (int j = 0; j < EMAX; j += 2) {
+      if (j >= ept) break;
       Cx<float> b0, b1;
       unpack2(riccati_step2(dre, dim, ere_pair<KEL>(ere, j, es), make_float2(eim[j], eim[j + 1]),
                             pack2(coh[j], coh[j + 1]), sb),
@@ -442,22 +444,24 @@ __device__ __forceinline__ void site_step_x2(uint8_t l, uint8_t l_entry, uint8_t
 }
 template <int EMAX, bool KEL>
 __device__ __forceinline__ void interior_step_x2(float dre, float dim, float es, float pdre, float pdim, float pes,
-                                                 const float *ere, const float *eim, Cx<float> *coh, float h) {
+                                                 const float *ere, const float *eim, Cx<float> *coh, int ept,
+                                                 float h) {
   const float sdre = (dre + pdre) * 0.5f;
   const float sdim = (dim + pdim) * 0.5f;
   const float ses = (es + pes) * 0.5f;
 #pragma unroll
   for (int j = 0; j < EMAX; j += 2)
-    unpack2(riccati_step2(sdre, sdim, ere_pair<KEL>(ere, j, ses), make_float2(eim[j], eim[j + 1]),
-                          pack2(coh[j], coh[j + 1]), h),
-            coh[j], coh[j + 1]);
+    if (j < ept)
+      unpack2(riccati_step2(sdre, sdim, ere_pair<KEL>(ere, j, ses), make_float2(eim[j], eim[j + 1]),
+                            pack2(coh[j], coh[j + 1]), h),
+              coh[j], coh[j + 1]);
 }
 
 // Dispatch of one site's steps to the packed (PK) or the scalar form.
 template <typename R, int EMAX, bool KEL, bool PK>
 __device__ __forceinline__ void interior_any(R dre, R dim, R es, R pdre, R pdim, R pes, const R *ere,
                                              const R *eim, Cx<R> *coh, int ept, R h) {
-  if constexpr (PK) interior_step_x2<EMAX, KEL>(dre, dim, es, pdre, pdim, pes, ere, eim, coh, h);
+  if constexpr (PK) interior_step_x2<EMAX, KEL>(dre, dim, es, pdre, pdim, pes, ere, eim, coh, ept, h);
   else interior_step<R, EMAX, KEL>(dre, dim, es, pdre, pdim, pes, ere, eim, coh, ept, h);
 }
 template <typename R, int EMAX, bool KEL, bool PK>
@@ -465,8 +469,8 @@ __device__ __forceinline__ void site_any(uint8_t l, uint8_t l_entry, uint8_t l_e
                                          R pdim, R pes, const R *ere, const R *eim, Cx<R> *coh, int ept,
                                          int ecount, R h, R dist_in, const Cx<R> *bin, R dist_out, Cx<R> *bout) {
   if constexpr (PK)
-    site_step_x2<EMAX, KEL>(l, l_entry, l_exit, dre, dim, es, pdre, pdim, pes, ere, eim, coh, ecount, h, dist_in,
-                            bin, dist_out, bout);
+    site_step_x2<EMAX, KEL>(l, l_entry, l_exit, dre, dim, es, pdre, pdim, pes, ere, eim, coh, ept, ecount, h,
+                            dist_in, bin, dist_out, bout);
   else
     site_step<R, EMAX, KEL>(l, l_entry, l_exit, dre, dim, es, pdre, pdim, pes, ere, eim, coh, ept, ecount, h,
                             dist_in, bin, dist_out, bout);
@@ -488,8 +492,9 @@ __device__ __forceinline__ void site_any(uint8_t l, uint8_t l_entry, uint8_t l_e
 // Fermi surface, and the batch); otherwise it is the uniform lattice spacing h
 // of the circle, which stays a kernel parameter.
 // PK: the packed FP32 form (energies in pairs: riccati_step2, local_greens2 or
-// greens_g_im2, the scratch in energy-pair records); the launch guarantees
-// ept = EMAX (even) so that every thread's first energy is even.
+// greens_g_im2, the scratch in energy-pair records).  Each thread takes an
+// even number of energies (the mapping's count rounded up, at most EMAX), so
+// that every thread's first energy is even.
 template <typename R, int EMAX, bool KEL, bool STEP_PER_ANGLE, int LG = -1, bool PK = false>
 __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double *s_res, int item,
                                              int g, unsigned gmask) {
@@ -503,7 +508,7 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
   const R h = STEP_PER_ANGLE ? (R)A.ang[a].hs : (R)A.h;  // h / |v_F| of this angle
   // A compile-time group size comes with a full load (EMAX energies per
   // thread), a sweep that stores its frame sums, and no energy passes.
-  const int ept = (LG >= 0 || PK) ? EMAX : A.ept;
+  const int ept = LG >= 0 ? EMAX : (PK ? ((A.ept + 1) & ~1) : A.ept);
   const bool burn_in = LG >= 0 ? false : A.burn_in != 0;
   const bool accumulate = LG >= 0 ? false : A.accumulate != 0;
   const int e0 = g * ept;
@@ -764,7 +769,7 @@ __global__ void __launch_bounds__(128, MINB) k_sweep(const SweepArgs<R> A) {
 // by the host), so ragged grains share the GPU without a tail per grain.  All
 // grain has its own G = 2^log_groups threads per column (the warp's unit
 // belongs to one grain, so the mapping is uniform within a warp).
-template <typename R, int EMAX, int MINB>
+template <typename R, int EMAX, int MINB, bool PK = false>
 __global__ void __launch_bounds__(128, MINB) k_sweep_batch(const SweepArgs<R> *__restrict__ args,
                                                            const int2 *__restrict__ units, int n_units,
                                                            int *counter) {
@@ -781,7 +786,7 @@ __global__ void __launch_bounds__(128, MINB) k_sweep_batch(const SweepArgs<R> *_
     const int sub = lane >> lg;
     const unsigned gmask = ((groups == 32) ? 0xffffffffu : ((1u << groups) - 1u)) << (lane & ~(groups - 1));
     const int item = wu.y + sub;
-    if (item < A.n_items) sweep_column<R, EMAX, false, true>(A, A.res, item, g, gmask);
+    if (item < A.n_items) sweep_column<R, EMAX, false, true, -1, PK>(A, A.res, item, g, gmask);
   }
 }
 
@@ -2009,6 +2014,20 @@ void launch_sweep_pass(sc_ctx *c, const SweepArgs<R> &A, unsigned blocks) {
     else if (variant == 3) k_sweep<R, 2, 3, false><<<blocks, 128, 0, c->stream>>>(A);
     else k_sweep<R, 2, 4, false><<<blocks, 128, 0, c->stream>>>(A);
   } else if (c->ept <= 4) {
+    if constexpr (std::is_same<R, float>::value) {
+      // Four energies per thread in mixed precision (energy passes of low
+      // temperatures, or a mapping chosen by SCB_ENERGY_GROUPS): two FP32 pairs.
+      static const bool no_packed4 = std::getenv("SCB_NO_PACKED") != nullptr;
+      if (!no_packed4 && c->ept == 4) {
+        const bool g4 = plain && c->log_groups == 2;
+        if (variant == 3 && g4) k_sweep<R, 4, 3, false, false, 2, true><<<blocks, 128, 0, c->stream>>>(A);
+        else if (variant == 3) k_sweep<R, 4, 3, false, false, -1, true><<<blocks, 128, 0, c->stream>>>(A);
+        else if (g4) k_sweep<R, 4, 4, false, false, 2, true><<<blocks, 128, 0, c->stream>>>(A);
+        else k_sweep<R, 4, 4, false, false, -1, true><<<blocks, 128, 0, c->stream>>>(A);
+        check_launch(c);
+        return;
+      }
+    }
     if (variant == 4 && plain && c->log_groups == 2 && c->ept == 4) k_sweep<R, 4, 4, false, false, 2><<<blocks, 128, 0, c->stream>>>(A);
     else if (variant == 4) k_sweep<R, 4, 4, false><<<blocks, 128, 0, c->stream>>>(A);
     else if (variant == 5) k_sweep<R, 4, 5, false><<<blocks, 128, 0, c->stream>>>(A);
@@ -3600,7 +3619,22 @@ void launch_batch_sweep(sc_batch *b, sc_batch::Wave &w, int wi) {
       const int blocks = std::max(1, per_sm) * b->n_sm;
       kernel<<<blocks, 128, 0, b->stream>>>(args, ps.units.p, ps.n_units, counter);
     };
-    if (ept <= 2 && b->minb == 6) {
+    // Mixed precision with an even cap of energies per thread: the packed
+    // FP32 sweep (each grain's count rounded up to even).
+    static const bool no_packed = std::getenv("SCB_NO_PACKED") != nullptr;
+    bool packed = false;
+    if constexpr (std::is_same<R, float>::value) packed = !no_packed && b->ept_max % 2 == 0 && b->ept_max <= 4;
+    if constexpr (std::is_same<R, float>::value) {
+      if (packed) {
+        if (ept <= 2 && b->minb == 6) run(k_sweep_batch<R, 2, 6, true>);
+        else if (ept <= 2) run(k_sweep_batch<R, 2, 4, true>);
+        else if (b->minb == 4) run(k_sweep_batch<R, 4, 4, true>);
+        else if (b->minb == 3) run(k_sweep_batch<R, 4, 3, true>);
+        else run(k_sweep_batch<R, 4, 1, true>);
+      }
+    }
+    if (packed) {
+    } else if (ept <= 2 && b->minb == 6) {
       run(k_sweep_batch<R, 2, 6>);
     } else if (ept <= 2 && b->minb == 4) {
       run(k_sweep_batch<R, 2, 4>);
