@@ -281,8 +281,10 @@ int sc_batch_set_graph(sc_batch *b, int enable);
  * trajectory column (1, 2, 4 or 8) that keep at most energies_per_thread
  * energies on a thread, and minb selects the resident-block variant (1: up
  * to 255 registers per thread, 3: at most 168, 4: at most 128, 6: at most 80;
- * 3 with at most four energies per thread, 6 with at most two).  sc_batch_autotune times the feasible choices on the
- * current state (after at least one iteration) and keeps the fastest. */
+ * 3 with at most four energies per thread, 6 with at most two; the default is four energies per thread and
+ * minb 4).  In mixed precision a cap of two or four runs the packed FP32 sweep (each grain's energies per thread
+ * rounded up to even).  sc_batch_autotune times the feasible choices on the current state (after at least one
+ * iteration) and keeps the fastest. */
 int sc_batch_config(sc_batch *b, int energies_per_thread, int minb);
 int sc_batch_get_config(const sc_batch *b, int *energies_per_thread, int *minb, int *n_waves);
 int sc_batch_autotune(sc_batch *b, int *energies_per_thread, int *minb, double *best_ms);

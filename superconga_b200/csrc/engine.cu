@@ -106,6 +106,16 @@ template <>
 struct FrameOf<float> {
   using type = float2;
 };
+// LDOS frame element: FP64 in the plain form; FP32 in mixed precision, which
+// holds the FP32 sweep's Im g exactly and halves the frame traffic.
+template <typename R>
+struct LdosOf {
+  using type = double;
+};
+template <>
+struct LdosOf<float> {
+  using type = float;
+};
 template <typename F2>
 __device__ __forceinline__ F2 frame_pair(double a, double b) {
   return F2{(decltype(F2::x))a, (decltype(F2::x))b};
@@ -159,7 +169,7 @@ struct SweepArgs {
   Cx<R> *scratch;   // [tile][row][energy][item of tile]
   R *scratch2;      // frame-field records [tile][row][item of tile] of (Re D, Im D, energy shift, label), in R
   typename FrameOf<R>::type *fr;  // frame records [slot][n1*n1][2]: (Re F, Im F), (Re g, Re I)
-  double *ldf;      // LDOS frame buffer [slot][n1*n1][energy]: Im g per real energy
+  typename LdosOf<R>::type *ldf;  // LDOS frame buffer [slot][n1*n1][energy]: Im g per real energy
 };
 
 // Scratch tiles: the items of one warp (32 / G trajectory columns, G = 2^lg
@@ -656,19 +666,19 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
       if (burn_in) continue;
       if constexpr (KEL) {
         if (l != 0) {
-          double *o = A.ldf + ((size_t)(a - A.slot_base) * nn1 + (size_t)y * n1 + x) * A.ne_stride + e0;
+          typename LdosOf<R>::type *o = A.ldf + ((size_t)(a - A.slot_base) * nn1 + (size_t)y * n1 + x) * A.ne_stride + e0;
           if constexpr (PK) {
 #pragma unroll
             for (int j = 0; j < EMAX; j += 2)
               if (j < ecount) {
                 const float2 v = greens_g_im2(pack2(coh[j], coh[j + 1]), pack2(gt[j], gt[j + 1]));
-                o[j] = (double)v.x;
-                if (j + 1 < ecount) o[j + 1] = (double)v.y;
+                o[j] = v.x;
+                if (j + 1 < ecount) o[j + 1] = v.y;
               }
           } else {
 #pragma unroll
             for (int j = 0; j < EMAX; ++j)
-              if (j < ecount) o[j] = (double)greens_g_im<R>(coh[j], gt[j]);
+              if (j < ecount) o[j] = greens_g_im<R>(coh[j], gt[j]);
           }
         }
         continue;
@@ -897,21 +907,22 @@ __global__ void __launch_bounds__(256, NC == 1 ? 4 : 3) k_rotate_back(int n0, in
 
 // LDOS frame extension next to the boundary, every energy of the block
 // (ComputeLDOS.h:137-138 through domain_ops.h:11-69).
+template <typename LF>
 __global__ void k_halo_ldos(int n_entries, int entry0, int n1, int ne,
                             const int *__restrict__ entry_angle, int slot_base,
                             const int *__restrict__ site, const int *__restrict__ off,
-                            const int *__restrict__ src, double *ldf) {
+                            const int *__restrict__ src, LF *ldf) {
   // one thread per (entry, energy), energy fastest: the LDOS frame is
   // [slot][site][energy]
   const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (t >= (size_t)n_entries * ne) return;
   const int k = (int)(t / ne), en_ = (int)(t % ne);
   const int e = entry0 + k;
-  double *f = ldf + (size_t)(entry_angle[e] - slot_base) * n1 * n1 * ne + en_;
+  LF *f = ldf + (size_t)(entry_angle[e] - slot_base) * n1 * n1 * ne + en_;
   const int b = off[e], en = off[e + 1];
   double v = f[(size_t)src[b] * ne];
-  for (int i = b + 1; i < en; ++i) v = __dadd_rn(v, f[(size_t)src[i] * ne]);
-  f[(size_t)site[e] * ne] = __ddiv_rn(v, (double)(en - b));
+  for (int i = b + 1; i < en; ++i) v = __dadd_rn(v, (double)f[(size_t)src[i] * ne]);
+  f[(size_t)site[e] * ne] = (LF)__ddiv_rn(v, (double)(en - b));
 }
 
 // LDOS frames rotated back onto the reference grid and accumulated in angle
@@ -928,10 +939,10 @@ __global__ void k_halo_ldos(int n_entries, int entry0, int n1, int ne,
 // same sums as skipping it, with a loop free of branches so that the loads of
 // consecutive angles overlap.
 constexpr int RB_ANGLES = 32;
-template <int EL, int TX>
+template <int EL, int TX, typename LF>
 __global__ void __launch_bounds__(256) k_rotate_back_ldos(int n0, int n1, int ne, int a_begin, int a_end,
                                                           const AngleParams *__restrict__ ang,
-                                                          const double *__restrict__ ldf, double *acc) {
+                                                          const LF *__restrict__ ldf, double *acc) {
   constexpr int SPB = 256 / EL, TY = SPB / TX;
   static_assert(SPB % TX == 0, "the site tile must fill the block");
   __shared__ int s_i00[RB_ANGLES][SPB];
@@ -961,13 +972,13 @@ __global__ void __launch_bounds__(256) k_rotate_back_ldos(int n0, int n1, int ne
     }
     __syncthreads();
     if (!valid) continue;
-    const double *f = ldf + (size_t)(ab - a_begin) * nn1 * ne + e;
+    const LF *f = ldf + (size_t)(ab - a_begin) * nn1 * ne + e;
 #pragma unroll 4
     for (int ka = 0; ka < na; ++ka) {
       const double2 fxy = s_fxy[ka][s];
       const double w = s_w[ka][s];
-      const double *c = f + (size_t)ka * nn1 * ne + (size_t)s_i00[ka][s] * ne;
-      v += bilerp(c[0] * w, c[dx] * w, c[dy] * w, c[dy + dx] * w, fxy.x, fxy.y);
+      const LF *c = f + (size_t)ka * nn1 * ne + (size_t)s_i00[ka][s] * ne;
+      v += bilerp((double)c[0] * w, (double)c[dx] * w, (double)c[dy] * w, (double)c[dy + dx] * w, fxy.x, fxy.y);
     }
   }
   if (valid) acc[(size_t)e * nn0 + i] = v;
@@ -1847,6 +1858,7 @@ struct sc_ctx {
 
   size_t nn0() const { return (size_t)S.n0 * S.n0; }
   size_t esize() const { return mode == SC_MODE_FP64 ? sizeof(Cx<double>) : sizeof(Cx<float>); }
+  size_t ldos_esize() const { return mode == SC_MODE_FP64 ? sizeof(double) : sizeof(float); }
   // Bytes of one frame-buffer element (FrameOf<R>: float2 for the FP32 sweep).
   size_t frame_rec() const { return (mode == SC_MODE_MIXED && !S.keldysh) ? sizeof(float4) : 2 * sizeof(double2); }
   void *bnd_ptr(int which) const { return (char *)bnd.p + bnd_off[which]; }
@@ -1928,7 +1940,7 @@ SweepArgs<R> sweep_args(sc_ctx *c, const Chunk *ch, int burn_in) {
   A.e_re = c->e_re.p;
   A.e_im = c->e_im.p;
   A.res = c->res.p;
-  A.ldf = c->ldf.p;
+  A.ldf = (typename LdosOf<R>::type *)c->ldf.p;
   A.scratch = (Cx<R> *)c->w_scratch;
   A.scratch2 = (R *)c->w_scratch2;
   A.fr = (typename FrameOf<R>::type *)c->w_fr;
@@ -1955,9 +1967,10 @@ void launch_sweep_pass(sc_ctx *c, const SweepArgs<R> &A, unsigned blocks) {
   // Resident blocks per SM, fastest measured on B200 (606 x 606 d-wave square,
   // 256 angles, 14 energies, fixed-group kernels): FP64 three (four energies
   // per thread, 168 registers: 21.8 ms against 22.1 with four blocks and 24.4
-  // with two), mixed six (two energies per thread: 6.72 ms against 6.74 with
-  // four and 6.82 with five).
-  // The common mappings (FP64: four energies per thread, four threads per
+  // with two); mixed in the packed FP32 form four (four energies per thread
+  // in two pairs, four threads per column: 5.70 ms, 5.68 with three), or six
+  // with two energies per thread.
+  // The common mappings (four energies per thread and four threads per
   // column; mixed and LDOS: eight threads per column) are compiled with the
   // group size fixed, which turns the per-site group reduction, frame store
   // and tile addressing into straight-line code (C2: FP64 sweep -5%, mixed
@@ -2312,20 +2325,21 @@ void frame_to_reference(sc_ctx *c, const Chunk &ch) {
 
 // Lanes per reference site: the smallest of 8, 16, 32 that holds the block's
 // energies (more energies take several blocks along z).
+template <typename LF>
 static void launch_rotate_back_ldos(sc_ctx *c, const Chunk &ch) {
   const HostSetup &S = c->S;
   auto go = [&](auto kern, int el, int tx) {
     const int ty = 256 / el / tx;
     dim3 grid((S.n0 + tx - 1) / tx, (S.n0 + ty - 1) / ty, (S.ne + el - 1) / el);
-    kern<<<grid, 256, 0, c->stream>>>(S.n0, S.n1, S.ne, ch.a_begin, ch.a_end, c->ang.p, c->ldf.p,
+    kern<<<grid, 256, 0, c->stream>>>(S.n0, S.n1, S.ne, ch.a_begin, ch.a_end, c->ang.p, (const LF *)c->ldf.p,
                                       c->ldos_acc.p);
   };
   if (S.ne <= 8)
-    go(k_rotate_back_ldos<8, 8>, 8, 8);
+    go(k_rotate_back_ldos<8, 8, LF>, 8, 8);
   else if (S.ne <= 16)
-    go(k_rotate_back_ldos<16, 4>, 16, 4);
+    go(k_rotate_back_ldos<16, 4, LF>, 16, 4);
   else
-    go(k_rotate_back_ldos<32, 4>, 32, 4);
+    go(k_rotate_back_ldos<32, 4, LF>, 32, 4);
   check_launch(c);
 }
 
@@ -2345,13 +2359,14 @@ void run_chunks_ldos(sc_ctx *c, int burn_in) {
     if (burn_in) continue;
     const int h0 = S.halo_angle_off[ch.a_begin], h1 = S.halo_angle_off[ch.a_end];
     if (h1 > h0) {
-      k_halo_ldos<<<grid1((size_t)(h1 - h0) * S.ne, 128), 128, 0, c->stream>>>(
+      using LF = typename LdosOf<R>::type;
+      k_halo_ldos<LF><<<grid1((size_t)(h1 - h0) * S.ne, 128), 128, 0, c->stream>>>(
           h1 - h0, h0, S.n1, S.ne, c->halo_angle.p, ch.a_begin, c->halo_site.p, c->halo_off.p, c->halo_src.p,
-          c->ldf.p);
+          (LF *)c->ldf.p);
       check_launch(c);
     }
     ProfScope prof(c, 1);
-    launch_rotate_back_ldos(c, ch);
+    launch_rotate_back_ldos<typename LdosOf<R>::type>(c, ch);
   }
 }
 
@@ -2572,7 +2587,7 @@ void plan_chunks(sc_ctx *c, std::vector<int4> &items) {
   // A batch grain sweeps all its angles in one chunk (the batch pools memory).
   const double budget = c->batch_member ? 1e300 : budget_mb * 1048576.0;
   const size_t per_row = (size_t)c->e_pass * c->esize() + 3 * sizeof(double);
-  const size_t frame_slot = S.keldysh ? (size_t)n1 * n1 * S.ne * sizeof(double)
+  const size_t frame_slot = S.keldysh ? (size_t)n1 * n1 * S.ne * c->ldos_esize()
                                       : (size_t)n1 * n1 * 2 * sizeof(double2);
   items.clear();
   if (c->pair) {
@@ -2738,11 +2753,14 @@ void upload_static(sc_ctx *c) {
   c->groups = 1;
   c->log_groups = 0;
   const char *eg = std::getenv("SCB_ENERGY_GROUPS");
-  // Default (fastest measured on B200 for 7-14 Ozaki energies): FP64 the fewest
-  // threads per column that keep at most four energies per thread; mixed
-  // precision at most two; three (FP64) or four (mixed) resident blocks per SM.
+  // Default (fastest measured on B200 for 7-14 Ozaki energies): the fewest
+  // threads per column that keep at most four energies per thread; three
+  // (FP64) or four (mixed) resident blocks per SM.  Mixed precision prefers an
+  // even count, which the packed FP32 sweep takes in pairs (C2, 14 energies:
+  // four threads of four energies, sweep 5.70 ms, against eight threads of two
+  // 6.07 ms).
   const bool fp32_sweep = c->mode == SC_MODE_MIXED && !S.keldysh;
-  const int per_thread = fp32_sweep ? 2 : 4;
+  const int per_thread = 4;
   int want = 1;
   if (eg) want = std::atoi(eg);
   else {
@@ -2756,6 +2774,8 @@ void upload_static(sc_ctx *c) {
     size_t max_items = 0;
     for (const Chunk &ch : c->chunks) max_items = std::max(max_items, (size_t)(ch.item_end - ch.item_begin));
     while ((double)max_items * want < 2.0 * resident && want < 8 && (c->e_pass + want - 1) / want > 1) want *= 2;
+    const int ept_w = (c->e_pass + want - 1) / want;
+    if (fp32_sweep && ept_w > 1 && ept_w % 2 == 1 && want < 8) want *= 2;
   }
   while (c->groups < want && c->groups < 8) {
     c->groups *= 2;
@@ -2806,7 +2826,7 @@ void upload_static(sc_ctx *c) {
     c->scratch2.alloc(scr2 + 1);
     c->w_scratch = c->scratch.p;
     c->w_scratch2 = c->scratch2.p;
-    c->ldf.alloc((size_t)max_slots * S.ne * n1 * n1);
+    c->ldf.alloc(((size_t)max_slots * S.ne * n1 * n1 * c->ldos_esize() + 7) / 8);  // as doubles
     c->ldf.zero(s);  // once: afterwards every slot holds finite values (see run_chunks_ldos)
     c->ldos_acc.alloc((size_t)S.ne * nn);
     c->ldos_all.alloc((size_t)S.ldos_n_blocks * S.ldos_block * nn);
@@ -3619,11 +3639,12 @@ void launch_batch_sweep(sc_batch *b, sc_batch::Wave &w, int wi) {
       const int blocks = std::max(1, per_sm) * b->n_sm;
       kernel<<<blocks, 128, 0, b->stream>>>(args, ps.units.p, ps.n_units, counter);
     };
-    // Mixed precision with an even cap of energies per thread: the packed
-    // FP32 sweep (each grain's count rounded up to even).
+    // Mixed precision with at most four energies per thread in the pass: the
+    // packed FP32 sweep (each grain's count rounded up to even; a cap of one
+    // energy per thread keeps the scalar form, which that mapping is for).
     static const bool no_packed = std::getenv("SCB_NO_PACKED") != nullptr;
     bool packed = false;
-    if constexpr (std::is_same<R, float>::value) packed = !no_packed && b->ept_max % 2 == 0 && b->ept_max <= 4;
+    if constexpr (std::is_same<R, float>::value) packed = !no_packed && b->ept_max >= 2 && ept <= 4;
     if constexpr (std::is_same<R, float>::value) {
       if (packed) {
         if (ept <= 2 && b->minb == 6) run(k_sweep_batch<R, 2, 6, true>);
@@ -3857,9 +3878,9 @@ int sc_batch_create(const char *const *configs, int n, int mode, sc_batch **out)
     b->scalar_src.upload(src, b->stream);
     b->scalars.alloc(n);
     b->host_scalars.resize(n);
-    // Threads per column, per grain: the fewest that keep at most four (FP64)
-    // or two (mixed) energies per thread.
-    b->ept_max = mode == SC_MODE_FP64 ? 4 : 2;
+    // Threads per column, per grain: the fewest that keep at most four
+    // energies per thread (mixed precision: the packed FP32 sweep).
+    b->ept_max = 4;
     b->minb = 4;
     if (mode == SC_MODE_FP64) batch_plan<double>(b);
     else batch_plan<float>(b);
