@@ -529,6 +529,39 @@ __device__ __forceinline__ void site_any(uint8_t l, uint8_t l_entry, uint8_t l_e
 // STEP_PER_ANGLE: the Riccati step h/|v_F| is read per angle (a non-circular
 // Fermi surface, and the batch); otherwise it is the uniform lattice spacing h
 // of the circle, which stays a kernel parameter.
+// Asynchronous global-to-shared copies of 16 bytes (cp.async.cg, through L2);
+// with pred false nothing is read (the source must still be a valid address)
+// and the 16 bytes are zero-filled.  Each thread waits only for its own
+// copies (cp.async.wait_group), so no barrier is involved.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, bool pred) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(pred ? 16 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// The sweep's staging ring: every thread keeps the inputs of the next NS - 1
+// sites of its column in flight (the site's frame-field record and, going up,
+// the gammaTilde stored going down), copied asynchronously into shared memory
+// ring[stage][16-byte unit][thread], so that the latency of these loads spans
+// several sites' Riccati steps instead of one.  Used by the packed FP32 sweep
+// and the FP64 sweep with at most four energies per thread (128 threads per
+// block); about 40 KB of shared memory per block.
+template <typename R, int EMAX, bool PK>
+struct SweepRing {
+  static constexpr bool on = (PK || sizeof(R) == 8) && EMAX <= 4;
+  static constexpr int NV_REC = sizeof(R) == 8 ? 2 : 1;  // record: 32 or 16 bytes
+  static constexpr int NV_GT = PK ? EMAX / 2 : EMAX;      // gammaTilde: one pair or one FP64 energy per unit
+  static constexpr int NV = NV_REC + NV_GT;
+  static constexpr int NS_FIT = (40 * 1024) / (NV * 128 * 16);
+  static constexpr int NS = on ? (NS_FIT < 2 ? 2 : (NS_FIT > 8 ? 8 : NS_FIT)) : 1;
+  static constexpr int NVD = on ? NV : 1;
+};
+
 // PK: the packed FP32 form (energies in pairs: riccati_step2, local_greens2 or
 // greens_g_im2, the scratch in energy-pair records).  Each thread takes an
 // even number of energies (the mapping's count rounded up, at most EMAX), so
@@ -567,8 +600,77 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
   const size_t ax = (size_t)a * n1 + x;
   // Mirrored partner column (angle + pi, x -> n1 - 1 - x) when paired.
   const size_t pax = (size_t)(a + A.pair) * n1 + (n1 - 1 - x);
-  // The next site's label, fields and stored gammaTilde are loaded one site
-  // ahead so that their latency overlaps the current site's Riccati steps.
+  // Without the staging ring, the next site's label, fields and stored
+  // gammaTilde are loaded one site ahead so that their latency overlaps the
+  // current site's Riccati steps.
+  typedef typename Rec4<R>::type V4;
+  using RG = SweepRing<R, EMAX, PK>;
+  constexpr bool RING = RG::on;
+  constexpr int NS = RG::NS;
+  __shared__ float4 ring[NS][RG::NVD][128];
+  const int tid = threadIdx.x;
+  const int n_rows = hi - lo + 1;
+  const V4 *fb = (const V4 *)A.scratch2 + rec_index(A, lgc, item, 0);
+  // Copies of row `row` (record, and gammaTilde when with_gt) into the stage
+  // of step `step`; one commit group per step, empty outside the column.
+  auto ring_issue = [&](int step, int row, bool with_gt) {
+    if constexpr (RING) {
+      if (row >= 0 && row < n_rows) {
+        const int sl = step % NS;
+        const char *rp = (const char *)(fb + (size_t)row * T);
+#pragma unroll
+        for (int v = 0; v < RG::NV_REC; ++v) cp_async16(&ring[sl][v][tid], rp + 16 * v, true);
+        if (with_gt) {
+          if constexpr (PK) {
+            const float4 *sc = (const float4 *)A.scratch + sb0 + (size_t)row * s_row;
+#pragma unroll
+            for (int jp = 0; jp < RG::NV_GT; ++jp) {
+              const bool ok = 2 * jp < ecount;
+              cp_async16(&ring[sl][RG::NV_REC + jp][tid], ok ? (const void *)(sc + (size_t)jp * T) : (const void *)rp,
+                         ok);
+            }
+          } else {
+            const Cx<R> *sc = A.scratch + sb0 + (size_t)row * s_row;
+#pragma unroll
+            for (int j = 0; j < RG::NV_GT; ++j) {
+              const bool ok = j < ecount;
+              cp_async16(&ring[sl][RG::NV_REC + j][tid], ok ? (const void *)(sc + (size_t)j * T) : (const void *)rp,
+                         ok);
+            }
+          }
+        }
+      }
+      cp_async_commit();
+    }
+  };
+  auto ring_rec = [&](int step) -> V4 {
+    const int sl = step % NS;
+    if constexpr (sizeof(R) == 4) {
+      const float4 v = ring[sl][0][tid];
+      return V4{(R)v.x, (R)v.y, (R)v.z, (R)v.w};
+    } else {
+      const double2 u = *reinterpret_cast<const double2 *>(&ring[sl][0][tid]);
+      const double2 w = *reinterpret_cast<const double2 *>(&ring[sl][RG::NV_REC - 1][tid]);
+      return V4{(R)u.x, (R)u.y, (R)w.x, (R)w.y};
+    }
+  };
+  auto ring_gt = [&](int step, Cx<R> *gt) {
+    const int sl = step % NS;
+    if constexpr (PK) {
+#pragma unroll
+      for (int jp = 0; jp < RG::NV_GT; ++jp) {
+        const float4 v = ring[sl][RG::NV_REC + jp][tid];
+        gt[2 * jp] = Cx<R>{(R)v.x, (R)v.z};
+        gt[2 * jp + 1] = Cx<R>{(R)v.y, (R)v.w};
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < RG::NV_GT; ++j) {
+        const double2 v = *reinterpret_cast<const double2 *>(&ring[sl][RG::NV_REC + j][tid]);
+        gt[j] = Cx<R>{(R)v.x, (R)v.y};
+      }
+    }
+  };
   // ------------------------------------------------------ gammaTilde, down --
   {
     const int in_base = A.idx_in_gt[ax], out_base = A.idx_out_gt[ax];
@@ -576,15 +678,26 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
     R pdre = 0, pdim = 0, pes = 0;
 #pragma unroll
     for (int j = 0; j < EMAX; ++j) coh[j] = Cx<R>{R(0), R(0)};
-    typedef typename Rec4<R>::type V4;
-    const V4 *fb = (const V4 *)A.scratch2 + rec_index(A, lgc, item, 0);
-    V4 fr = fb[(size_t)(hi - lo) * T];
+    V4 fr;
+    if constexpr (RING) {
+      for (int st = 0; st < NS - 1; ++st) ring_issue(st, n_rows - 1 - st, false);
+    } else {
+      fr = fb[(size_t)(hi - lo) * T];
+    }
     for (int y = hi; y >= lo; --y) {
       const int r = y - lo;
+      if constexpr (RING) {
+        const int st = hi - y;
+        ring_issue(st + NS - 1, r - (NS - 1), false);
+        cp_async_wait<NS - 1>();
+        fr = ring_rec(st);
+      }
       const uint8_t l = (uint8_t)fr.w;
       // gammaTilde uses -conj(Delta) (RiccatiSolverConfined.h:74-79).
       const R dre = (R)(-fr.x), dim = (R)fr.y, es = (R)fr.z;
-      if (y > lo) fr = fb[(size_t)(r - 1) * T];
+      if constexpr (!RING) {
+        if (y > lo) fr = fb[(size_t)(r - 1) * T];
+      }
       if (l == 1) {
         interior_any<R, EMAX, KEL, PK>(dre, dim, es, pdre, pdim, pes, ere, eim, coh, ept, h);
       } else {
@@ -622,6 +735,7 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
       pdim = dim;
       pes = es;
     }
+    if constexpr (RING) cp_async_wait<0>();
   }
   // ----------------------------------------------------------- gamma, up --
   {
@@ -634,9 +748,7 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
     Fr *frs = A.fr + (size_t)(a - A.slot_base) * nn1 * 2;  // this angle's records
     // The value this thread stores when four or more threads share a column.
     auto *vdst = &frs->x + (lgc >= 2 ? (g >> (lgc - 2)) : 0);
-    typedef typename Rec4<R>::type V4;
-    const V4 *fb = (const V4 *)A.scratch2 + rec_index(A, lgc, item, 0);
-    V4 fr = fb[0];
+    V4 fr;
     Cx<R> gt_nx[EMAX];
     // The stored gammaTilde of row r into gt_nx.
     auto load_gt = [&](int r) {
@@ -656,17 +768,30 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
           if (j < ecount) gt_nx[j] = sc[(size_t)j * T];
       }
     };
-    if (!burn_in) load_gt(0);
+    if constexpr (RING) {
+      for (int st = 0; st < NS - 1; ++st) ring_issue(st, st, !burn_in);
+    } else {
+      fr = fb[0];
+      if (!burn_in) load_gt(0);
+    }
     for (int y = lo; y <= hi; ++y) {
       const int r = y - lo;
+      Cx<R> gt[EMAX];
+      if constexpr (RING) {
+        ring_issue(r + NS - 1, r + NS - 1, !burn_in);
+        cp_async_wait<NS - 1>();
+        fr = ring_rec(r);
+        if (!burn_in) ring_gt(r, gt);
+      }
       const uint8_t l = (uint8_t)fr.w;
       const R dre = (R)fr.x, dim = (R)fr.y, es = (R)fr.z;
-      Cx<R> gt[EMAX];
+      if constexpr (!RING) {
 #pragma unroll
-      for (int j = 0; j < EMAX; ++j) gt[j] = gt_nx[j];
-      if (y < hi) {
-        fr = fb[(size_t)(r + 1) * T];
-        if (!burn_in) load_gt(r + 1);
+        for (int j = 0; j < EMAX; ++j) gt[j] = gt_nx[j];
+        if (y < hi) {
+          fr = fb[(size_t)(r + 1) * T];
+          if (!burn_in) load_gt(r + 1);
+        }
       }
       if (l == 1) {
         interior_any<R, EMAX, KEL, PK>(dre, dim, es, pdre, pdim, pes, ere, eim, coh, ept, h);
@@ -783,6 +908,7 @@ __device__ __forceinline__ void sweep_column(const SweepArgs<R> &A, const double
         }
       }
     }
+    if constexpr (RING) cp_async_wait<0>();
   }
 }
 
