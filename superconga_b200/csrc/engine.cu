@@ -364,7 +364,7 @@ __device__ __forceinline__ void group_sum4_scatter(double v[4], int g, int log_g
 // compact patch of the frame whose rotated corners fall on few cache lines of
 // the reference grid (a warp along one row touched ~20 sectors per gather).
 constexpr int FF_COLS = 8, FF_ROWS = 16;
-template <typename R>
+template <typename R, int UNR = 1>
 __global__ void __launch_bounds__(FF_COLS * FF_ROWS) k_frame_fields(const SweepArgs<R> A, int rows_per_block) {
   const int item = blockIdx.x * FF_COLS + threadIdx.x;
   if (item >= A.n_items) return;
@@ -373,6 +373,7 @@ __global__ void __launch_bounds__(FF_COLS * FF_ROWS) k_frame_fields(const SweepA
   const AngleParams &P = A.ang[a];  // read in place (a local copy went to the stack)
   const int r0 = blockIdx.y * rows_per_block;
   const int r1 = min(r0 + rows_per_block, hi - lo + 1);
+#pragma unroll UNR
   for (int r = r0 + threadIdx.y; r < r1; r += FF_ROWS) {
     double dre, dim, es;
     frame_fields(A, P, x, lo + r, dre, dim, es);
@@ -549,11 +550,14 @@ __device__ __forceinline__ void cp_async_wait() {
 // the gammaTilde stored going down), copied asynchronously into shared memory
 // ring[stage][16-byte unit][thread], so that the latency of these loads spans
 // several sites' Riccati steps instead of one.  Used by the packed FP32 sweep
-// and the FP64 sweep with at most four energies per thread (128 threads per
-// block); about 40 KB of shared memory per block.
+// with at most four energies per thread (128 threads per block; about 40 KB
+// of shared memory per block).  Measured on B200: C2 mixed sweep 5.69 ->
+// 5.30 ms, C5 mixed LDOS sweep 79.5 -> 74.9 ms; the FP64 sweep, whose larger
+// records leave room for three stages only, ran 2% (C2) to 18% (C5 LDOS)
+// slower with it and keeps the one-site-ahead register prefetch.
 template <typename R, int EMAX, bool PK>
 struct SweepRing {
-  static constexpr bool on = (PK || sizeof(R) == 8) && EMAX <= 4;
+  static constexpr bool on = PK && EMAX <= 4;
   static constexpr int NV_REC = sizeof(R) == 8 ? 2 : 1;  // record: 32 or 16 bytes
   static constexpr int NV_GT = PK ? EMAX / 2 : EMAX;      // gammaTilde: one pair or one FP64 energy per unit
   static constexpr int NV = NV_REC + NV_GT;
@@ -990,8 +994,8 @@ __global__ void k_halo(int n_entries, int entry0, int n1, const int *__restrict_
 // NC > 0 fixes the component count at compile time (the sums stay in
 // registers); NC = 0 takes it from nc.  One component: four resident blocks
 // per SM (64 registers) measured fastest on B200; more: three.
-template <typename F2, int NC>
-__global__ void __launch_bounds__(256, NC == 1 ? 4 : 3) k_rotate_back(int n0, int n1, int nc_, int a_begin,
+template <typename F2, int NC, int UNR = 1>
+__global__ void __launch_bounds__(256, UNR == 1 ? (NC == 1 ? 4 : 3) : (UNR == 2 ? 3 : 2)) k_rotate_back(int n0, int n1, int nc_, int a_begin,
                                                      int a_end, int pair, const AngleParams *__restrict__ ang,
                                                      const F2 *__restrict__ fr,
                                                      double *acc_d, double *acc_j, double *acc_fe) {
@@ -1009,6 +1013,7 @@ __global__ void __launch_bounds__(256, NC == 1 ? 4 : 3) k_rotate_back(int n0, in
   }
   double jx = acc_j[i], jy = acc_j[nn0 + i], fe = acc_fe[i];
   const int last = (pair ? 2 : 1) * (a_end - a_begin);
+#pragma unroll UNR
   for (int k = 0; k < last; ++k) {
     const int a0 = a_begin + (pair ? k >> 1 : k);
     const bool mirrored = pair && (k & 1);
@@ -2114,7 +2119,10 @@ void launch_frame_fields(sc_ctx *c, const Chunk &ch, const SweepArgs<R> &A) {
   const int rows = 64 * FF_ROWS;
   dim3 grid(grid1(A.n_items, FF_COLS), (unsigned)((ch.kmax + rows - 1) / rows));
   ProfScope prof(c, 4);
-  k_frame_fields<R><<<grid, dim3(FF_COLS, FF_ROWS), 0, c->stream>>>(A, rows);
+  static const int ffv = std::getenv("SCB_FF_UNROLL") ? std::atoi(std::getenv("SCB_FF_UNROLL")) : 1;
+  if (ffv == 4) k_frame_fields<R, 4><<<grid, dim3(FF_COLS, FF_ROWS), 0, c->stream>>>(A, rows);
+  else if (ffv == 2) k_frame_fields<R, 2><<<grid, dim3(FF_COLS, FF_ROWS), 0, c->stream>>>(A, rows);
+  else k_frame_fields<R><<<grid, dim3(FF_COLS, FF_ROWS), 0, c->stream>>>(A, rows);
   check_launch(c);
 }
 
@@ -2479,7 +2487,9 @@ void frame_to_reference(sc_ctx *c, const Chunk &ch) {
   // share cache lines of the frame).
   dim3 blk(8, 32), grid((S.n0 + 7) / 8, (S.n0 + 31) / 32);
   ProfScope prof(c, 1);
-  auto kern = S.nc == 1 ? k_rotate_back<Fr, 1> : S.nc == 2 ? k_rotate_back<Fr, 2> : k_rotate_back<Fr, 0>;
+  static const int rbv = std::getenv("SCB_RB_UNROLL") ? std::atoi(std::getenv("SCB_RB_UNROLL")) : 1;
+  auto kern = S.nc == 1 ? (rbv == 4 ? k_rotate_back<Fr, 1, 4> : rbv == 2 ? k_rotate_back<Fr, 1, 2> : k_rotate_back<Fr, 1>)
+              : S.nc == 2 ? k_rotate_back<Fr, 2> : k_rotate_back<Fr, 0>;
   kern<<<grid, blk, 0, c->stream>>>(S.n0, S.n1, S.nc, ch.a_begin, a_stored, pair, c->ang.p, (const Fr *)c->w_fr,
                                     c->acc_d.p, c->acc_j.p, c->acc_fe.p);
   check_launch(c);
