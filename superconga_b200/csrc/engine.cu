@@ -364,7 +364,7 @@ __device__ __forceinline__ void group_sum4_scatter(double v[4], int g, int log_g
 // compact patch of the frame whose rotated corners fall on few cache lines of
 // the reference grid (a warp along one row touched ~20 sectors per gather).
 constexpr int FF_COLS = 8, FF_ROWS = 16;
-template <typename R, int UNR = 1>
+template <typename R>
 __global__ void __launch_bounds__(FF_COLS * FF_ROWS) k_frame_fields(const SweepArgs<R> A, int rows_per_block) {
   const int item = blockIdx.x * FF_COLS + threadIdx.x;
   if (item >= A.n_items) return;
@@ -373,7 +373,6 @@ __global__ void __launch_bounds__(FF_COLS * FF_ROWS) k_frame_fields(const SweepA
   const AngleParams &P = A.ang[a];  // read in place (a local copy went to the stack)
   const int r0 = blockIdx.y * rows_per_block;
   const int r1 = min(r0 + rows_per_block, hi - lo + 1);
-#pragma unroll UNR
   for (int r = r0 + threadIdx.y; r < r1; r += FF_ROWS) {
     double dre, dim, es;
     frame_fields(A, P, x, lo + r, dre, dim, es);
@@ -994,8 +993,8 @@ __global__ void k_halo(int n_entries, int entry0, int n1, const int *__restrict_
 // NC > 0 fixes the component count at compile time (the sums stay in
 // registers); NC = 0 takes it from nc.  One component: four resident blocks
 // per SM (64 registers) measured fastest on B200; more: three.
-template <typename F2, int NC, int UNR = 1>
-__global__ void __launch_bounds__(256, UNR == 1 ? (NC == 1 ? 4 : 3) : (UNR == 2 ? 3 : 2)) k_rotate_back(int n0, int n1, int nc_, int a_begin,
+template <typename F2, int NC>
+__global__ void __launch_bounds__(256, NC == 1 ? 4 : 3) k_rotate_back(int n0, int n1, int nc_, int a_begin,
                                                      int a_end, int pair, const AngleParams *__restrict__ ang,
                                                      const F2 *__restrict__ fr,
                                                      double *acc_d, double *acc_j, double *acc_fe) {
@@ -1013,7 +1012,6 @@ __global__ void __launch_bounds__(256, UNR == 1 ? (NC == 1 ? 4 : 3) : (UNR == 2 
   }
   double jx = acc_j[i], jy = acc_j[nn0 + i], fe = acc_fe[i];
   const int last = (pair ? 2 : 1) * (a_end - a_begin);
-#pragma unroll UNR
   for (int k = 0; k < last; ++k) {
     const int a0 = a_begin + (pair ? k >> 1 : k);
     const bool mirrored = pair && (k & 1);
@@ -2119,10 +2117,7 @@ void launch_frame_fields(sc_ctx *c, const Chunk &ch, const SweepArgs<R> &A) {
   const int rows = 64 * FF_ROWS;
   dim3 grid(grid1(A.n_items, FF_COLS), (unsigned)((ch.kmax + rows - 1) / rows));
   ProfScope prof(c, 4);
-  static const int ffv = std::getenv("SCB_FF_UNROLL") ? std::atoi(std::getenv("SCB_FF_UNROLL")) : 1;
-  if (ffv == 4) k_frame_fields<R, 4><<<grid, dim3(FF_COLS, FF_ROWS), 0, c->stream>>>(A, rows);
-  else if (ffv == 2) k_frame_fields<R, 2><<<grid, dim3(FF_COLS, FF_ROWS), 0, c->stream>>>(A, rows);
-  else k_frame_fields<R><<<grid, dim3(FF_COLS, FF_ROWS), 0, c->stream>>>(A, rows);
+  k_frame_fields<R><<<grid, dim3(FF_COLS, FF_ROWS), 0, c->stream>>>(A, rows);
   check_launch(c);
 }
 
@@ -2487,9 +2482,7 @@ void frame_to_reference(sc_ctx *c, const Chunk &ch) {
   // share cache lines of the frame).
   dim3 blk(8, 32), grid((S.n0 + 7) / 8, (S.n0 + 31) / 32);
   ProfScope prof(c, 1);
-  static const int rbv = std::getenv("SCB_RB_UNROLL") ? std::atoi(std::getenv("SCB_RB_UNROLL")) : 1;
-  auto kern = S.nc == 1 ? (rbv == 4 ? k_rotate_back<Fr, 1, 4> : rbv == 2 ? k_rotate_back<Fr, 1, 2> : k_rotate_back<Fr, 1>)
-              : S.nc == 2 ? k_rotate_back<Fr, 2> : k_rotate_back<Fr, 0>;
+  auto kern = S.nc == 1 ? k_rotate_back<Fr, 1> : S.nc == 2 ? k_rotate_back<Fr, 2> : k_rotate_back<Fr, 0>;
   kern<<<grid, blk, 0, c->stream>>>(S.n0, S.n1, S.nc, ch.a_begin, a_stored, pair, c->ang.p, (const Fr *)c->w_fr,
                                     c->acc_d.p, c->acc_j.p, c->acc_fe.p);
   check_launch(c);
