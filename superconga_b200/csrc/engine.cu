@@ -510,11 +510,6 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, bool pr
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(pred ? 16 : 0)
                : "memory");
 }
-// The same through L1 (cp.async.ca), for gathers whose neighbours share lines.
-__device__ __forceinline__ void cp_async16_ca(void *smem, const void *gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
@@ -989,48 +984,6 @@ __global__ void __launch_bounds__(256, NC == 1 ? 4 : 3) k_rotate_back(int n0, in
   }
   double jx = acc_j[i], jy = acc_j[nn0 + i], fe = acc_fe[i];
   const int last = (pair ? 2 : 1) * (a_end - a_begin);
-  // FP32 frames (mixed precision, 128-thread blocks): the four corner records
-  // of the next RB_STAGES - 1 angles are copied ahead into shared memory
-  // (cp.async through L1, one stage per angle; each thread waits for its own
-  // copies only), so that the gather latency of several angles overlaps.
-  constexpr bool RING = sizeof(F2) == 8;
-  constexpr int RB_STAGES = 4;
-  __shared__ float4 rbr[RING ? RB_STAGES : 1][RING ? 4 : 1][RING ? 128 : 1];
-  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-  // Corner record indices of step k (the frame origin when the lookup falls
-  // outside, as below).
-  auto corners = [&](int k, size_t *ci) {
-    const int a0 = a_begin + (pair ? k >> 1 : k);
-    const bool mirrored = pair && (k & 1);
-    const AngleParams &P = ang[mirrored ? a0 + pair : a0];
-    Bilinear b;
-    const size_t i00 = rotated_lookup(x, y, n0, n1, P.cB, P.sB, b) ? (size_t)b.i00 : 0;
-    const size_t slot = (size_t)(a0 - a_begin) * nn1;
-    if (!mirrored) {
-      ci[0] = slot + i00;
-      ci[1] = ci[0] + 1;
-      ci[2] = ci[0] + n1;
-      ci[3] = ci[0] + n1 + 1;
-    } else {
-      ci[0] = slot + (nn1 - 1 - i00);
-      ci[1] = ci[0] - 1;
-      ci[2] = ci[0] - n1;
-      ci[3] = ci[0] - n1 - 1;
-    }
-  };
-  auto issue = [&](int k) {
-    if constexpr (RING) {
-      if (k < last) {
-        size_t ci[4];
-        corners(k, ci);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) cp_async16_ca(&rbr[k % RB_STAGES][q][tid], (const float4 *)fr + ci[q]);
-      }
-      cp_async_commit();
-    }
-  };
-  if constexpr (RING)
-    for (int k = 0; k < RB_STAGES - 1; ++k) issue(k);
   for (int k = 0; k < last; ++k) {
     const int a0 = a_begin + (pair ? k >> 1 : k);
     const bool mirrored = pair && (k & 1);
@@ -1046,16 +999,7 @@ __global__ void __launch_bounds__(256, NC == 1 ? 4 : 3) k_rotate_back(int n0, in
     const double pw = inside ? P.w : 0.0, psx = inside ? P.sx : 0.0, psy = inside ? P.sy : 0.0;
     FrameRec r00, r01, r10, r11;
     const size_t slot = (size_t)(a0 - a_begin) * nn1;
-    if constexpr (RING) {
-      issue(k + RB_STAGES - 1);
-      cp_async_wait<RB_STAGES - 1>();
-      const int sl = k % RB_STAGES;
-      const float4 v00 = rbr[sl][0][tid], v01 = rbr[sl][1][tid], v10 = rbr[sl][2][tid], v11 = rbr[sl][3][tid];
-      r00 = FrameRec{make_double2(v00.x, v00.y), make_double2(v00.z, v00.w)};
-      r01 = FrameRec{make_double2(v01.x, v01.y), make_double2(v01.z, v01.w)};
-      r10 = FrameRec{make_double2(v10.x, v10.y), make_double2(v10.z, v10.w)};
-      r11 = FrameRec{make_double2(v11.x, v11.y), make_double2(v11.z, v11.w)};
-    } else if (!mirrored) {
+    if (!mirrored) {
       const size_t base = slot + b.i00;
       r00 = load_rec(fr, base); r01 = load_rec(fr, base + 1); r10 = load_rec(fr, base + n1); r11 = load_rec(fr, base + n1 + 1);
     } else {
@@ -1080,7 +1024,6 @@ __global__ void __launch_bounds__(256, NC == 1 ? 4 : 3) k_rotate_back(int n0, in
     jy += g * psy;
     fe += bilerp(r00.q.y, r01.q.y, r10.q.y, r11.q.y, b.xf, b.yf) * pw;
   }
-  if constexpr (RING) cp_async_wait<0>();
 #pragma unroll
   for (int c = 0; c < nc; ++c) {
     acc_d[(size_t)(2 * c) * nn0 + i] = dr[c];
@@ -2501,8 +2444,7 @@ void frame_to_reference(sc_ctx *c, const Chunk &ch) {
   }
   // A warp covers an 8 x 4 patch of the reference grid (its rotated corners
   // share cache lines of the frame).
-  const int by = sizeof(Fr) == 8 ? 16 : 32;  // FP32 frames: 128-thread blocks (the staging ring)
-  dim3 blk(8, by), grid((S.n0 + 7) / 8, (S.n0 + by - 1) / by);
+  dim3 blk(8, 32), grid((S.n0 + 7) / 8, (S.n0 + 31) / 32);
   ProfScope prof(c, 1);
   auto kern = S.nc == 1 ? k_rotate_back<Fr, 1> : S.nc == 2 ? k_rotate_back<Fr, 2> : k_rotate_back<Fr, 0>;
   kern<<<grid, blk, 0, c->stream>>>(S.n0, S.n1, S.nc, ch.a_begin, a_stored, pair, c->ang.p, (const Fr *)c->w_fr,
