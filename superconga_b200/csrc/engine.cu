@@ -521,8 +521,8 @@ __device__ __forceinline__ void cp_async_wait() {
 // the gammaTilde stored going down), copied asynchronously into shared memory
 // ring[stage][16-byte unit][thread], so that the latency of these loads spans
 // several sites' Riccati steps instead of one.  Used by the packed FP32 sweep
-// with at most four energies per thread (128 threads per block; about 40 KB
-// of shared memory per block).  Measured on B200: C2 mixed sweep 5.69 ->
+// with at most four energies per thread (128 threads per block; at most 40 KB
+// of shared memory per block: 36 KB at four energies per thread, six stages).  Measured on B200: C2 mixed sweep 5.69 ->
 // 5.30 ms, C5 mixed LDOS sweep 79.5 -> 74.9 ms; the FP64 sweep, whose larger
 // records leave room for three stages only, ran 2% (C2) to 18% (C5 LDOS)
 // slower with it and keeps the one-site-ahead register prefetch.
