@@ -77,6 +77,15 @@ __global__ void k_pack_reference(int nc, int nn, const double *__restrict__ x, d
   for (int c = 0; c <= nc; ++c) r[c] = make_double2(x[(size_t)(2 * c) * nn + i], x[(size_t)(2 * c + 1) * nn + i]);
 }
 
+// FP32 copy of the records for the mixed-precision lookups (the FP32 sweep
+// rounds the frame fields to FP32 anyway): half the bytes per gathered corner.
+__global__ void k_round_reference(size_t n, const double2 *__restrict__ rf, float2 *__restrict__ rf32) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double2 v = rf[i];
+  rf32[i] = make_float2((float)v.x, (float)v.y);
+}
+
 // Reference-grid extension of the order parameter (domain_ops.h:11-69):
 // the order parameter everywhere, except label-0 sites next to the grain,
 // which get the mean of their nearest grain sites; written into the records
@@ -165,6 +174,7 @@ struct SweepArgs {
   const Cx<R> *bin_g, *bin_gt;
   Cx<R> *bout_g, *bout_gt;
   const double2 *rf;   // [n0*n0][nc + 1]: extended order parameter per component, then A (k_pack_reference)
+  const float2 *rf32;  // the same records in FP32 (mixed precision: the FP32 sweep's lookups read these)
   const double *e_re, *e_im, *res;
   Cx<R> *scratch;   // [tile][row][energy][item of tile]
   R *scratch2;      // frame-field records [tile][row][item of tile] of (Re D, Im D, energy shift, label), in R
@@ -222,6 +232,24 @@ __device__ __forceinline__ void gauge_potential(int gauge, double b, double area
   }
 }
 
+// Reference records for the frame lookups: FP64 for the FP64 sweep, the FP32
+// copy for the FP32 sweep.  ld_rec01 reads a site's component-0 and
+// vector-potential records of a one-component grain in one load (32 or 16
+// bytes).
+__device__ __forceinline__ void ld_rec01(const SweepArgs<double> &A, size_t site, double2 &d, double2 &a) {
+  ldg_d2x2(A.rf + site * 2, d, a);
+}
+__device__ __forceinline__ void ld_rec01(const SweepArgs<float> &A, size_t site, double2 &d, double2 &a) {
+  const float4 v = __ldg((const float4 *)A.rf32 + site);
+  d = make_double2(v.x, v.y);
+  a = make_double2(v.z, v.w);
+}
+__device__ __forceinline__ double2 ld_rec(const SweepArgs<double> &A, size_t idx) { return __ldg(A.rf + idx); }
+__device__ __forceinline__ double2 ld_rec(const SweepArgs<float> &A, size_t idx) {
+  const float2 v = __ldg(A.rf32 + idx);
+  return make_double2(v.x, v.y);
+}
+
 // Order parameter (OrderParameter::getRotatedGrid) and Doppler shift
 // (computeEnergyShift, RiccatiSolver.h:127-176) at frame site (x, y).
 template <typename R>
@@ -246,7 +274,7 @@ __device__ __forceinline__ void frame_fields(const SweepArgs<R> &A, const AngleP
       const double et = P.eta[0];
       for (int k = 0; k < 4; ++k) {
         double2 v;
-        ldg_d2x2(A.rf + (size_t)off[k] * 2, v, ca[k]);
+        ld_rec01(A, (size_t)off[k], v, ca[k]);
         c_re[k] += v.x * et;
         c_im[k] += v.y * et;
       }
@@ -254,7 +282,7 @@ __device__ __forceinline__ void frame_fields(const SweepArgs<R> &A, const AngleP
       for (int c = 0; c < A.nc; ++c) {
         const double et = P.eta[c];
         for (int k = 0; k < 4; ++k) {
-          const double2 v = __ldg(A.rf + (size_t)off[k] * st + c);
+          const double2 v = ld_rec(A, (size_t)off[k] * st + c);
           c_re[k] += v.x * et;
           c_im[k] += v.y * et;
         }
@@ -281,11 +309,11 @@ __device__ __forceinline__ void frame_fields(const SweepArgs<R> &A, const AngleP
           v10 = ca[2];
           v11 = ca[3];
         } else {
-          const double2 *pa = A.rf + A.nc;
-          v00 = __ldg(pa + (size_t)ba.i00 * st);
-          v01 = __ldg(pa + (size_t)(ba.i00 + 1) * st);
-          v10 = __ldg(pa + (size_t)(ba.i00 + n0) * st);
-          v11 = __ldg(pa + (size_t)(ba.i00 + n0 + 1) * st);
+          const size_t pa = (size_t)A.nc;
+          v00 = ld_rec(A, pa + (size_t)ba.i00 * st);
+          v01 = ld_rec(A, pa + (size_t)(ba.i00 + 1) * st);
+          v10 = ld_rec(A, pa + (size_t)(ba.i00 + n0) * st);
+          v11 = ld_rec(A, pa + (size_t)(ba.i00 + n0 + 1) * st);
         }
         rx = bilerp(v00.x, v01.x, v10.x, v11.x, ba.xf, ba.yf);
         ry = bilerp(v00.y, v01.y, v10.y, v11.y, ba.xf, ba.yf);
@@ -522,10 +550,11 @@ __device__ __forceinline__ void cp_async_wait() {
 // ring[stage][16-byte unit][thread], so that the latency of these loads spans
 // several sites' Riccati steps instead of one.  Used by the packed FP32 sweep
 // with at most four energies per thread (128 threads per block; at most 40 KB
-// of shared memory per block: 36 KB at four energies per thread, six stages).  Measured on B200: C2 mixed sweep 5.69 ->
-// 5.30 ms, C5 mixed LDOS sweep 79.5 -> 74.9 ms; the FP64 sweep, whose larger
-// records leave room for three stages only, ran 2% (C2) to 18% (C5 LDOS)
-// slower with it and keeps the one-site-ahead register prefetch.
+// of shared memory per block: 36 KB at four energies per thread, six stages).
+// Measured on B200: C2 mixed sweep 5.69 -> 5.30 ms, C5 mixed LDOS sweep
+// 79.5 -> 74.9 ms; the FP64 sweep, whose larger records leave room for three
+// stages only, ran 2% (C2) to 18% (C5 LDOS) slower with it and keeps the
+// one-site-ahead register prefetch.
 template <typename R, int EMAX, bool PK>
 struct SweepRing {
   static constexpr bool on = PK && EMAX <= 4;
@@ -1929,6 +1958,7 @@ struct sc_ctx {
 
   // state: x = [delta | avec], g = [delta_new | a_new]
   DevArray<double> xstate, gstate, rfields, j_real;
+  DevArray<double> rfields32;  // FP32 records (mixed precision), allocated as doubles
   std::vector<int4> h_items;  // trajectory columns (angle, x, first row, last row), host copy
   DevArray<double> acc_d, acc_j, acc_fe;
   DevArray<double> bnd;      // boundary storage (4 arrays), R-typed, viewed through pointers
@@ -2066,6 +2096,7 @@ SweepArgs<R> sweep_args(sc_ctx *c, const Chunk *ch, int burn_in) {
   A.bin_gt = (const Cx<R> *)c->bnd_ptr(2);
   A.bout_gt = (Cx<R> *)c->bnd_ptr(3);
   A.rf = (const double2 *)c->rfields.p;
+  A.rf32 = (const float2 *)c->rfields32.p;
   A.e_re = c->e_re.p;
   A.e_im = c->e_im.p;
   A.res = c->res.p;
@@ -2226,6 +2257,12 @@ void extend_reference(sc_ctx *c) {
     dim3 grid(grid1(ns, 128), 2 * S.nc);
     k_extend_reference<<<grid, 128, 0, c->stream>>>(2 * S.nc, nn, ns, S.nc + 1, c->rext_site.p, c->rext_off.p,
                                                     c->rext_src.p, c->xstate.p, c->rfields.p);
+    check_launch(c);
+  }
+  if (c->rfields32.p) {
+    const size_t n = (size_t)(S.nc + 1) * nn;
+    k_round_reference<<<grid1(n, 256), 256, 0, c->stream>>>(n, (const double2 *)c->rfields.p,
+                                                           (float2 *)c->rfields32.p);
     check_launch(c);
   }
 }
@@ -2922,6 +2959,7 @@ void upload_static(sc_ctx *c) {
   c->xstate.zero(s);
   c->gstate.zero(s);
   c->rfields.alloc((size_t)2 * (S.nc + 1) * nn);
+  if (c->mode == SC_MODE_MIXED) c->rfields32.alloc((size_t)(S.nc + 1) * nn + 1);
   c->j_real.alloc(2 * nn);
   c->j_real.zero(s);
   c->acc_d.alloc((size_t)2 * S.nc * nn);
